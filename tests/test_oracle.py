@@ -1,0 +1,224 @@
+"""Pins the CPU oracle (oracle/psb_oracle.c) to the reference's golden vectors
+and, when oracle/_ref has been built from the reference's sources, to the
+reference itself.  CPU only."""
+import math
+import random
+
+import pytest
+
+import oracle as O
+
+SMALL = 4_000_000  # state-count cap for full BFS runs in the CPU suite
+
+
+def n_states(spec):
+    return O.info(spec)["indexes"]
+
+
+def start_index(spec, start):
+    return 0 if start is None else O.parse(spec, start)
+
+
+# --- permutation ranking (PuzzlesTests/PermutationMapTest.cpp) ---------------
+
+def test_permutation_compact(golden):
+    for case in golden["permutation"]["compact"]:
+        assert O.perm_compact(case["perm"]) == case["compact"], case["source"]
+        assert O.perm_uncompact(case["compact"]) == case["perm"], case["source"]
+
+
+def test_permutation_rank(golden):
+    for case in golden["permutation"]["rank"]:
+        assert O.perm_rank(case["perm"]) == case["rank"], case["source"]
+        assert O.perm_unrank(case["rank"], len(case["perm"])) == case["perm"], case["source"]
+
+
+def test_permutation_roundtrip_random():
+    rng = random.Random(1)
+    for n in range(1, 17):
+        for _ in range(50):
+            idx = rng.randrange(math.factorial(n))
+            assert O.perm_rank(O.perm_unrank(idx, n)) == idx
+
+
+# --- expand known-answer tests (PancakeTest, FourPegHanoiTest, SlidingPuzzleTest)
+
+def test_expand_known_answers(golden):
+    for kat in golden["expand_kats"]:
+        spec = kat["puzzle"]
+        parent = 0 if kat["parent"] is None else O.parse(spec, kat["parent"])
+        if kat["parent_index"] is not None:
+            assert parent == kat["parent_index"], kat["source"]
+        if kat["parent"] is not None:
+            assert O.to_string(spec, parent) == kat["parent"], kat["source"]
+        children, ops = O.expand(spec, [parent])
+        got = [O.to_string(spec, c) for c in children]
+        exp = kat["children"]
+        if kat["prefix_only"] and spec[0] == "sliding":
+            # The sliding tests list the children they check; all must be present.
+            assert set(exp) <= set(got), kat["source"]
+            continue
+        # Each test checks the first len(exp) children in order (some list fewer
+        # than the puzzle produces, e.g. FourPegHanoiTest.cpp Opt19_Symmetry).
+        assert got[:len(exp)] == exp, (kat["test"], kat["source"])
+        for o, e in zip(ops, kat["ops"]):
+            if e is not None:
+                assert o == e, (kat["test"], kat["source"])
+
+
+def test_expand_matches_reference_batches(golden):
+    """Seeded batches run through the reference's Puzzle::Expand (oracle/_ref)."""
+    for batch in golden["ref_expand"]:
+        children, ops = O.expand(batch["puzzle"], batch["parents"], batch["opbits"])
+        assert children == batch["children"], batch["puzzle"]
+        assert ops == batch["child_ops"], batch["puzzle"]
+
+
+# --- BFS golden vectors -------------------------------------------------------
+
+ALGOS = ["two_bit", "three_bit", "frontier", "classic"]
+
+
+def _algos_for(spec):
+    return [a for a in ALGOS if a != "frontier" or O.info(spec)["ops"] <= 4]
+
+
+def test_search_vectors(golden):
+    """PuzzlesTests/PuzzleSearchTests.cpp vectors, every in-memory algorithm."""
+    ran = 0
+    for v in golden["search"]:
+        spec = v["puzzle"]
+        if not v["full"] or n_states(spec) > SMALL:
+            continue
+        init = start_index(spec, v["start"])
+        for algo in _algos_for(spec):
+            counts, _ = O.bfs(spec, algo, init)
+            assert counts == v["counts"], (spec, algo, v["source"])
+            ran += 1
+    assert ran >= 12
+
+
+def test_legacy_sliding_vectors(golden):
+    """SlidingPuzzleTests/TestFrontierSearch.cpp: other starts and boards."""
+    ran = 0
+    for v in golden["legacy_sliding"]:
+        spec = v["puzzle"]
+        if not v["full"] or n_states(spec) > SMALL:
+            continue
+        counts, _ = O.bfs(spec, "three_bit", O.parse(spec, v["start"]))
+        assert counts == v["counts"], (spec, v["start"], v["source"])
+        assert len(counts) - 1 == v["radius"]
+        ran += 1
+    assert ran >= 7
+
+
+def test_reference_runs(golden):
+    """Per-depth counts from the reference's own InMemory BFS (oracle/_ref)."""
+    for run in golden["ref_runs"]:
+        spec = run["puzzle"]
+        counts, _ = O.bfs(spec, run["algo"], O.parse(spec, run["start"]))
+        assert counts == run["counts"], (spec, run["algo"], run["start"])
+
+
+def test_sum_invariants():
+    """Every pancake and Hanoi state is reachable; half of the sliding states are."""
+    assert sum(O.bfs(["pancake", 8, 0], "three_bit")[0]) == math.factorial(8)
+    assert sum(O.bfs(["hanoi4", 8, 0], "two_bit")[0]) == 4 ** 8
+    assert sum(O.bfs(["sliding", 3, 3], "two_bit")[0]) == math.factorial(9) // 2
+
+
+def test_final_arrays_consistent():
+    """Final arrays: the 2-bit array holds every reached state as OLD (code 1);
+    three-bit old|cur hold the last two levels."""
+    spec = ["pancake", 7, 0]
+    counts, fin = O.bfs(spec, "two_bit", 0, final=True)
+    N = n_states(spec)
+    old = sum(1 for i in range(N) if (fin[(2 * i) >> 6] >> ((2 * i) & 63)) & 1 == 0 and
+              (fin[(2 * i + 1) >> 6] >> ((2 * i + 1) & 63)) & 1 == 1)
+    assert old == sum(counts) == N
+    counts3, fin3 = O.bfs(spec, "three_bit", 0, final=True)
+    W = (N + 63) // 64
+    popc = [sum(bin(w).count("1") for w in fin3[k * W:(k + 1) * W]) for k in range(3)]
+    assert popc == [counts3[-2], counts3[-1], 0]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_oracle_visits_what_reference_expands():
+    """The set of parents the reference expands equals the oracle's reached set."""
+    for spec, algo in [(["hanoi4", 6, 1], "two_bit"), (["sliding", 3, 2], "three_bit"), (["pancake", 6, 0], "classic")]:
+        start = O.to_string(spec, 0)
+        parents = O.ref_bfs_parents(spec, algo, start, 1 << 22)
+        counts, fin = O.bfs(spec, "two_bit", 0, final=True)
+        reached = [i for i in range(n_states(spec)) if (fin[(2 * i + 1) >> 6] >> ((2 * i + 1) & 63)) & 1]
+        assert sorted(parents) == reached
+        assert len(parents) == sum(counts)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_oracle_vs_reference_random_expand():
+    rng = random.Random(5)
+    for spec in [["sliding", 4, 3], ["sliding", 2, 8], ["pancake", 14, 0], ["hanoi4", 18, 0], ["hanoi4", 12, 1]]:
+        N = n_states(spec)
+        ops_n = O.info(spec)["ops"]
+        parents = [rng.randrange(N) for _ in range(500)]
+        opbits = [rng.randrange(1 << ops_n) if i % 2 else 0 for i in range(500)]
+        assert O.expand(spec, parents, opbits) == O.ref_expand(spec, parents, opbits), spec
+
+
+# --- codecs (CommonTests/StreamVIntTests.cpp, CompressionTests.cpp) -----------
+
+def test_streamvint_tuples(golden):
+    for case in golden["streamvint"]["tuples"]:
+        enc = O.svi_encode_tuple(case["values"])
+        assert len(enc) == case["bytes"], case["source"]
+        dec, n = O.svi_decode_tuple(enc)
+        assert dec == case["values"] and n == case["bytes"]
+
+
+def test_streamvint_tuple_lists(golden):
+    for case in golden["streamvint"]["tuple_lists"]:
+        vals = case["values"]
+        total = sum(len(O.svi_encode_tuple(vals[i:i + 4])) for i in range(0, len(vals), 4))
+        assert total == case["bytes"], case["source"]
+
+
+def test_streamvint_roundtrip():
+    vals = [i * i for i in range(65536)]  # StreamVIntTests.cpp:146-160
+    enc = O.svi_encode(vals)
+    dec, size = O.svi_decode(enc)
+    assert dec == vals and size == len(enc)
+    assert O.svi_encode([]) == b""
+
+
+def test_compression_selection(golden):
+    c = golden["compression"]
+    for key in ("bitmap_stride", "svi_stride"):
+        case = c[key]
+        vals = [i * case["stride"] for i in range(case["count"])]
+        enc = O.fc_encode(vals)
+        assert O.fc_is_bitmap(enc) == case["is_bitmap"], case["source"]
+        dec, size = O.fc_decode(enc, 1024)
+        assert dec == vals and size == len(enc)
+    vals = c["bitmap_small"]["values"]
+    enc = O.fc_encode_bitmap(vals)
+    assert O.fc_decode(enc, 1024)[0] == vals
+    for key in ("out_of_order", "same_begin_end"):
+        assert O.fc_encode_bitmap(c[key]["values"], with_check=True) == -1, c[key]["source"]
+    vals = [i * 7 for i in range(150)] + [700]  # CompressionTests.cpp TestCompression_WithCheck
+    enc = O.fc_encode(vals, with_check=True)
+    assert not O.fc_is_bitmap(enc)
+    assert O.fc_decode(enc, 1024)[0] == vals
+    vals = c["large_range"]["values"]
+    enc = O.fc_encode(vals)
+    assert O.fc_decode(enc, 400)[0] == vals
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_codec_bytes_match_reference():
+    rng = random.Random(3)
+    for trial in range(40):
+        n = rng.choice([1, 3, 8, 129, 200, 1000, 5000])
+        span = rng.choice([n, 2 * n, 10 * n, 1 << 20, 1 << 31])
+        vals = sorted(rng.sample(range(span), n)) if span >= n else list(range(n))
+        for wc in (False, True):
+            assert O.fc_encode(vals, wc) == O.ref_fc_encode(vals, wc), (n, span, wc)
