@@ -1,0 +1,310 @@
+#!/usr/bin/env python3
+"""Benchmark: full in-memory BFS of the 13-pancake puzzle (three-bit arrays) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+One step is one complete BFS from the identity (13! = 6,227,020,800 states,
+16 depths, three bit arrays of 778 MB each, resident in HBM).  The metric
+is BFS states per second: states reached divided by device time.
+`value` times psb_bfs_session_run with the arrays already allocated.  `e2e`
+times the public C-ABI call psb_bfs, which allocates, runs and copies the
+per-depth counts back to the host.
+
+Multi-GPU: the path does not shard across GPUs inside one search (the
+reference has no multi-GPU path), so --gpus N runs N independent replicas,
+one process per GPU under torchrun.  value = total states / max-over-ranks time.
+
+--impl reference times the reference's own CPU path: InMemoryThreeBitBFS
+built from its sources into oracle/_ref.  It runs on a bounded sample (the
+full 11-pancake search) so the run ends in minutes.  The single-threaded
+13-pancake search takes tens of minutes.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+WORKLOADS = {
+    # name: (kind, a, b, algo, description)
+    "pancake13-3bit": ("pancake", 13, 0, "three_bit", "13-pancake in-memory three-bit BFS, full solve from the identity"),
+    "sliding3x4-2bit": ("sliding", 3, 4, "two_bit", "3x4 sliding-tile in-memory two-bit BFS, full solve from the solved state"),
+    "pancake14-2bit": ("pancake", 14, 0, "two_bit", "14-pancake in-memory two-bit BFS, full solve from the identity"),
+    "hanoi18-2bit": ("hanoi4", 18, 0, "two_bit", "18-disk 4-peg Hanoi in-memory two-bit BFS, full solve from all disks on peg 0"),
+}
+REF_SAMPLE = ("pancake", 11, 0, "three_bit")  # CPU baseline sample (reference InMemoryThreeBitBFS)
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != n_gpus:
+        raise SystemExit(f"--gpus {n_gpus} but WORLD_SIZE={world}")
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def cpu_reference_sample(sample=REF_SAMPLE):
+    """Runs the reference's InMemory BFS (oracle/_ref/psbref) on the sample; returns (states, seconds, kind)."""
+    kind, a, b, algo = sample
+    kinds = {"sliding": 1, "pancake": 2, "hanoi4": 3}
+    algos = {"two_bit": 1, "three_bit": 2, "frontier": 3, "classic": 4}
+    exe = os.path.join(REPO, "oracle", "_ref", "psbref")
+    if os.path.exists(exe):
+        out = subprocess.run([exe, str(kinds[kind]), str(a), str(b), str(algos[algo])], capture_output=True,
+                             text=True, check=True).stdout
+        d = json.loads(out.strip().splitlines()[-1])
+        return d["states"], d["seconds"], "reference"
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    t0 = time.perf_counter()
+    counts, _ = O.bfs([kind, a, b], algo, 0)
+    return sum(counts), time.perf_counter() - t0, "port"
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    kind, a, b, algo = REF_SAMPLE
+    for _ in range(args.warmup):
+        cpu_reference_sample()
+    secs, states, ck = 0.0, 0, "reference"
+    for _ in range(args.steps):
+        s, t, ck = cpu_reference_sample()
+        states += s
+        secs += t
+    value = states / secs
+    wl = WORKLOADS[args.workload]
+    line = {
+        "impl": "reference", "metric": f"BFS states/sec ({wl[4]})", "value": value, "unit": "states/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": args.workload, "sample": f"{a}-pancake full {algo} BFS ({math.factorial(a)} states)"},
+        "cpu_baseline": {"value": value, "unit": "states/s", "cores": 1, "kind": ck,
+                         "sample": f"reference InMemoryThreeBitBFS on {a}-pancake (full search, {math.factorial(a)} states), single-threaded as in the reference"},
+        "e2e": {"value": value, "unit": "states/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pancake13-3bit", choices=sorted(WORKLOADS))
+    ap.add_argument("--window-bits", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    import puzzlesearch_b200 as psb
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    kind, a, b, algo, desc = WORKLOADS[args.workload]
+    puzzle = {"pancake": lambda: psb.PancakeSimple(a), "sliding": lambda: psb.SlidingTilePuzzleSimple(a, b),
+              "hanoi4": lambda: psb.FourPegHanoiSimple(a, bool(b))}[kind]()
+    N = puzzle.IndexesCount()
+    stream = torch.cuda.Stream()
+    # Session on torch's stream so the CUDA events below bracket exactly the searches.
+    opts = psb._opts(0, args.window_bits, local, stream.cuda_stream)
+    h = ctypes.c_void_p()
+    psb._check(psb.lib().psb_bfs_session_create(puzzle.handle, psb._algo(algo), ctypes.byref(opts), ctypes.byref(h)))
+    cap = 1 << 16
+    counts = (ctypes.c_uint64 * cap)()
+    nd = ctypes.c_uint32()
+
+    def run_once():
+        st = psb.BfsStats()
+        st.struct_size = ctypes.sizeof(psb.BfsStats)
+        o = psb._opts(0, 0, local, stream.cuda_stream)
+        psb._check(psb.lib().psb_bfs_session_run(h, 0, ctypes.byref(o), counts, cap, ctypes.byref(nd), ctypes.byref(st)))
+        return list(counts[:nd.value]), st
+
+    for _ in range(args.warmup):
+        ref_counts, _ = run_once()
+    assert sum(ref_counts) in (N, N // 2), "search did not reach the whole component"
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    stats = []
+    torch.cuda.synchronize()
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            c, st = run_once()
+            assert c == ref_counts
+            stats.append(st)
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    elapsed_ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([elapsed_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    states_per_step = sum(ref_counts)
+    value = world * args.steps * states_per_step / (elapsed_ms / 1000.0)
+
+    # e2e: the public C-ABI entry point, host in/out, allocation included.
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    levels = 0
+    for _ in range(args.steps):
+        r = psb.bfs(puzzle, algo, 0, device=local)
+        assert r["counts"] == ref_counts
+        levels = r["stats"]["levels"]
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * args.steps * states_per_step / e2e_s
+
+    psb.lib().psb_bfs_session_destroy(h)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    # Roofline of the dominant kernel (the fused level kernel), algorithmic bytes:
+    # per level N/8 bytes of frontier swept + 8 bytes per generated child
+    # (three-bit); two-bit sweeps 2N/8 read + 2N/8 write per level.
+    st = stats[-1]
+    if algo == "three_bit":
+        sweep_bytes = N / 8
+    elif algo == "two_bit":
+        sweep_bytes = 2 * (2 * N / 8)
+    else:
+        sweep_bytes = N / 8
+    alg_bytes = st.levels * sweep_bytes + 8.0 * st.children
+    expand_ms = sum(s.expand_ms for s in stats) / len(stats)
+    achieved = alg_bytes / (expand_ms / 1000.0) / 1e9
+    peak, peak_kind = load_peaks()
+    launches_per_step = st.levels * (2 if algo in ("three_bit", "classic") else 1)
+
+    line = {
+        "metric": f"BFS states/sec ({desc})", "value": value, "unit": "states/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (the puzzle's full state space from its standard start state)",
+        "config": {"workload": args.workload, "states": states_per_step, "depths": len(ref_counts),
+                   "index_space": N, "device_bytes": st.device_bytes, "window_bits": st.window_bits,
+                   "l2": "inputs larger than L2 (bit arrays of %d MB resident in HBM)" % (st.device_bytes >> 20),
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "e2e": {"value": e2e_value, "unit": "states/s", "h2d_bytes_per_step": 8,
+                "d2h_bytes_per_step": 64 * levels + 8 * len(ref_counts)},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "note": f"level kernel, {peak_kind} peak; algorithmic bytes/level = sweep + 8 B/child"},
+        "kernel_ms_per_step": {"level": expand_ms, "finalize": sum(s.finalize_ms for s in stats) / len(stats)},
+        "children_per_step": st.children, "local_child_fraction": st.local_children / max(st.children, 1),
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        s, secs, ck = cpu_reference_sample()
+        line["cpu_baseline"] = {"value": s / secs, "unit": "states/s", "cores": 1, "kind": ck,
+                                "sample": "reference InMemoryThreeBitBFS on 11-pancake (full search, 39,916,800 states), single-threaded as in the reference"}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,160 @@
+/*
+ * psb200.h -- C ABI of puzzlesearch_b200, a B200-native (sm_100a) engine for
+ * complete breadth-first search over ranked puzzle state spaces.
+ *
+ * It is a drop-in for the complete-BFS path of lightln2/PuzzleSearch: the
+ * abstract Puzzle class (Common/Puzzle.h:16-48), its *Simple puzzles
+ * (Puzzles/SlidingTilePuzzleSimple.h, PancakeSimple.h, FourPegHanoiSimple.h)
+ * and the entry points InMemoryClassicBFS / InMemoryTwoBitBFS /
+ * InMemoryThreeBitBFS / InMemoryFrontierSearch (Common/InMemoryBFS.h:5-11).
+ * Indexes, operator codes, per-depth counts and final bit arrays are
+ * identical to the reference's.  include/psb200.hpp wraps this ABI in the
+ * reference's C++ interface.
+ *
+ * Conventions: plain C types only; every function returns int status
+ * (PSB_OK = 0, negative = error; psb_last_error() gives the message of the
+ * calling thread's last error).  No exceptions cross the ABI.  Calls on
+ * distinct puzzle handles may run concurrently from different threads.
+ */
+#ifndef PSB200_H
+#define PSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSB_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+    PSB_OK = 0,
+    PSB_ERR_ARG = -1,         /* bad argument (replaces the reference's ensure()/exit(-1), Common/Util.h:13-15) */
+    PSB_ERR_CUDA = -2,        /* CUDA runtime error (the reference throws std::runtime_error, Puzzles/GPU.cu:5-10) */
+    PSB_ERR_NOMEM = -3,       /* device or host allocation failed */
+    PSB_ERR_CAPACITY = -4,    /* an output buffer is too small */
+    PSB_ERR_UNSUPPORTED = -5, /* combination not supported (e.g. frontier search with > 4 operators) */
+    PSB_ERR_DEVICE = -6,      /* a kernel reported an internal error (index out of range) */
+    PSB_ERR_NO_DEVICE = -7    /* no CUDA device visible */
+};
+
+/* Puzzle kinds (the reference's *Simple classes). */
+enum {
+    PSB_SLIDING = 1, /* SlidingTilePuzzleSimple(width=a, height=b), 2 <= a*b <= 16 */
+    PSB_PANCAKE = 2, /* PancakeSimple(size=a), 2 <= a <= 16 */
+    PSB_HANOI4 = 3   /* FourPegHanoiSimple(disks=a, useSymmetry=b), 1 <= a <= 31 */
+};
+
+/* In-memory search algorithms (Common/InMemoryBFS.h:5-11). */
+enum {
+    PSB_TWO_BIT = 1,   /* InMemoryTwoBitBFS    (Common/InMemoryTwoBitBFS.cpp:24-69)   */
+    PSB_THREE_BIT = 2, /* InMemoryThreeBitBFS  (Common/InMemoryThreeBitBFS.cpp:4-48)  */
+    PSB_FRONTIER = 3,  /* InMemoryFrontierSearch (Common/InMemoryFrontierSearch.cpp:57-112) */
+    PSB_CLASSIC = 4    /* InMemoryClassicBFS   (Common/InMemoryClassicBFS.cpp:4-45)   */
+};
+
+#define PSB_INVALID_INDEX (~(uint64_t)0) /* Puzzle::INVALID_INDEX, Common/Puzzle.h:19 */
+
+typedef struct psb_puzzle psb_puzzle;
+
+const char* psb_version(void);
+/* Copies the calling thread's last error message (NUL-terminated). */
+int psb_last_error(char* buf, int cap);
+/* Number of visible CUDA devices (0 when none). */
+int psb_device_count(int* count);
+
+/* --- Puzzle (Common/Puzzle.h:16-48) --------------------------------------- */
+
+/* Replaces the constructors SlidingTilePuzzleSimple(w,h), PancakeSimple(n),
+ * FourPegHanoiSimple(n, sym).  No device memory is held by a puzzle. */
+int psb_puzzle_create(int kind, int a, int b, psb_puzzle** out);
+int psb_puzzle_destroy(psb_puzzle* p);
+/* Puzzle::IndexesCount, OperatorsCount, BranchingFactor, HasOddLengthCycles. */
+int psb_puzzle_info(const psb_puzzle* p, uint64_t* indexes, int* operators, int* branching, int* odd_cycles);
+/* Puzzle::Name. */
+int psb_puzzle_name(const psb_puzzle* p, char* buf, int cap);
+/* Puzzle::Parse / Puzzle::ToString (host). */
+int psb_parse(const psb_puzzle* p, const char* state, uint64_t* index);
+int psb_to_string(const psb_puzzle* p, uint64_t index, char* buf, int cap);
+
+/* --- Expand (Common/Puzzle.h:32-37; GPU twin of Puzzles/PuzzleGpu.cpp:53-82) */
+
+#define PSB_EXPAND_HOST_POINTERS 1u /* all pointers are host memory (copied in and out) */
+#define PSB_EXPAND_COMPACT 2u       /* drop INVALID slots (host pointers only) */
+#define PSB_EXPAND_USE_OPBITS 4u    /* honour used-operator bits (skip operators whose bit is set) */
+
+/* Expands n parents.  Without PSB_EXPAND_COMPACT the output has
+ * BranchingFactor() slots per parent, the valid children first in the
+ * *Simple classes' order, unused slots = PSB_INVALID_INDEX with operator
+ * (1 << OperatorsCount()) - 1, as the reference's GPU puzzles emit them
+ * (PuzzlesTests/SlidingPuzzleTest.cpp:43-60).  With PSB_EXPAND_COMPACT the
+ * valid children are packed in order and *n_out is their count.  cap is the
+ * capacity of children / child_ops in elements.  Parents must be < IndexesCount().
+ * stream is a cudaStream_t (NULL = the legacy default stream); the call
+ * returns after the results are available. */
+int psb_expand(const psb_puzzle* p, const uint64_t* parents, const uint32_t* opbits, uint64_t n,
+               uint64_t* children, uint32_t* child_ops, uint64_t cap, uint64_t* n_out,
+               uint32_t flags, void* stream);
+
+/* --- In-memory BFS (Common/InMemoryBFS.h:5-11) ----------------------------- */
+
+typedef struct {
+    uint32_t struct_size;  /* sizeof(psb_bfs_opts) */
+    uint32_t max_depth;    /* stop after this depth (0 = until the frontier is empty; PuzzleOptions::maxSteps, Common/DiskBasedBFS.h:10) */
+    int32_t window_bits;   /* log2 states per thread-block window (0 = automatic) */
+    int32_t device;        /* CUDA device ordinal (-1 = current) */
+    void* stream;          /* cudaStream_t (NULL = a stream owned by the call) */
+    uint64_t* final_words; /* optional host buffer: final arrays in the reference's layout (see psb_final_words) */
+    uint64_t final_cap;    /* capacity of final_words in 64-bit words */
+    float* level_ms;       /* optional, counts_cap entries: device ms of each level */
+    uint64_t* level_children; /* optional, counts_cap entries: children generated at each level */
+} psb_bfs_opts;
+
+typedef struct {
+    uint32_t struct_size;     /* sizeof(psb_bfs_stats) */
+    uint32_t levels;          /* level kernels launched */
+    uint32_t window_bits;     /* window used */
+    uint32_t threads;         /* threads per block of the level kernel */
+    double total_ms;          /* device time of the whole search (CUDA events) */
+    double expand_ms;         /* sum over levels of the fused sweep+expand+mark kernel */
+    double finalize_ms;       /* sum over levels of the finalize kernel (three-bit and classic only) */
+    uint64_t expanded;        /* parents expanded */
+    uint64_t children;        /* valid children generated */
+    uint64_t local_children;  /* children marked in the block's shared-memory window */
+    uint64_t expand_launches; /* level-kernel launches (one per level) */
+    uint64_t device_bytes;    /* device memory held by the search */
+} psb_bfs_stats;
+
+/* Size in 64-bit words of the final arrays that psb_bfs copies out:
+ *   PSB_TWO_BIT:   ceil(2N/64)  (vector<bool> layout of InMemoryTwoBitBFS.cpp:6-20: bit 2i = code/2, bit 2i+1 = code%2)
+ *   PSB_THREE_BIT: 3*ceil(N/64) (old, cur, new)
+ *   PSB_CLASSIC:   3*ceil(N/64) (closed, open, newOpen)
+ *   PSB_FRONTIER:  2*ceil(N/16) (current, next; 4 operator bits per state) */
+int psb_final_words(const psb_puzzle* p, int algo, uint64_t* words);
+
+/* Runs the whole search on the GPU from initial_index.  depth_counts[d] =
+ * number of states at distance d, as returned by the reference's InMemory*
+ * functions; *n_depths = number of depths.  The bit arrays stay in device
+ * memory for the whole search; only the per-depth counts (and, on request,
+ * the final arrays) come back.  opts and stats may be NULL. */
+int psb_bfs(const psb_puzzle* p, int algo, uint64_t initial_index, const psb_bfs_opts* opts,
+            uint64_t* depth_counts, uint32_t counts_cap, uint32_t* n_depths, psb_bfs_stats* stats);
+
+/* Device memory the search of psb_bfs would allocate (bytes). */
+int psb_bfs_footprint(const psb_puzzle* p, int algo, uint64_t* bytes);
+
+/* Reusable device state: allocate once, run many searches (benchmarks and
+ * serving keep arrays resident between runs). */
+typedef struct psb_bfs_session psb_bfs_session;
+int psb_bfs_session_create(const psb_puzzle* p, int algo, const psb_bfs_opts* opts, psb_bfs_session** out);
+int psb_bfs_session_run(psb_bfs_session* s, uint64_t initial_index, const psb_bfs_opts* opts,
+                        uint64_t* depth_counts, uint32_t counts_cap, uint32_t* n_depths, psb_bfs_stats* stats);
+int psb_bfs_session_destroy(psb_bfs_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSB200_H */

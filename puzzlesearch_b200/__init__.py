@@ -1,0 +1,326 @@
+"""puzzlesearch_b200 -- Python binding of the C ABI in include/psb200.h.
+
+It mirrors the reference's Puzzle API (Common/Puzzle.h:16-48) and its
+in-memory entry points (Common/InMemoryBFS.h:5-11) under the same names:
+
+    from puzzlesearch_b200 import PancakeSimple, InMemoryThreeBitBFS
+    puzzle = PancakeSimple(13)
+    counts = InMemoryThreeBitBFS(puzzle, puzzle.ToString(0))
+
+All search work runs on the GPU through libpsb200.so (sm_100a).  There is no
+CPU fallback: if the library or a CUDA device is missing, calls raise
+PsbError.
+"""
+import ctypes
+import os
+
+__all__ = [
+    "PsbError", "lib", "SlidingTilePuzzleSimple", "PancakeSimple", "FourPegHanoiSimple",
+    "InMemoryTwoBitBFS", "InMemoryThreeBitBFS", "InMemoryFrontierSearch", "InMemoryClassicBFS",
+    "bfs", "BfsSession", "TWO_BIT", "THREE_BIT", "FRONTIER", "CLASSIC", "INVALID_INDEX",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpsb200.so")
+
+SLIDING, PANCAKE, HANOI4 = 1, 2, 3
+TWO_BIT, THREE_BIT, FRONTIER, CLASSIC = 1, 2, 3, 4
+ALGOS = {"two_bit": TWO_BIT, "three_bit": THREE_BIT, "frontier": FRONTIER, "classic": CLASSIC}
+INVALID_INDEX = (1 << 64) - 1
+EXPAND_HOST_POINTERS, EXPAND_COMPACT, EXPAND_USE_OPBITS = 1, 2, 4
+
+u64p = ctypes.POINTER(ctypes.c_uint64)
+u32p = ctypes.POINTER(ctypes.c_uint32)
+
+
+class PsbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"psb error {code}: {msg}")
+        self.code = code
+
+
+class BfsOpts(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
+                ("window_bits", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("stream", ctypes.c_void_p), ("final_words", u64p), ("final_cap", ctypes.c_uint64),
+                ("level_ms", ctypes.POINTER(ctypes.c_float)), ("level_children", u64p)]
+
+
+class BfsStats(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("levels", ctypes.c_uint32),
+                ("window_bits", ctypes.c_uint32), ("threads", ctypes.c_uint32),
+                ("total_ms", ctypes.c_double), ("expand_ms", ctypes.c_double),
+                ("finalize_ms", ctypes.c_double), ("expanded", ctypes.c_uint64),
+                ("children", ctypes.c_uint64), ("local_children", ctypes.c_uint64),
+                ("expand_launches", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}
+
+
+_lib = None
+
+
+def lib():
+    """Loads libpsb200.so; raises PsbError when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PsbError(-5, f"{LIB_PATH} is missing: build it with python -m puzzlesearch_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        L.psb_version.restype = ctypes.c_char_p
+        L.psb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        L.psb_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
+        L.psb_puzzle_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
+        L.psb_puzzle_destroy.argtypes = [P]
+        L.psb_puzzle_info.argtypes = [P, u64p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int)]
+        L.psb_puzzle_name.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
+        L.psb_parse.argtypes = [P, ctypes.c_char_p, u64p]
+        L.psb_to_string.argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_int]
+        L.psb_expand.argtypes = [P, u64p, u32p, ctypes.c_uint64, u64p, u32p, ctypes.c_uint64, u64p,
+                                 ctypes.c_uint32, ctypes.c_void_p]
+        L.psb_final_words.argtypes = [P, ctypes.c_int, u64p]
+        L.psb_bfs.argtypes = [P, ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(BfsOpts), u64p, ctypes.c_uint32,
+                              u32p, ctypes.POINTER(BfsStats)]
+        L.psb_bfs_footprint.argtypes = [P, ctypes.c_int, u64p]
+        L.psb_bfs_session_create.argtypes = [P, ctypes.c_int, ctypes.POINTER(BfsOpts), ctypes.POINTER(P)]
+        L.psb_bfs_session_run.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(BfsOpts), u64p, ctypes.c_uint32,
+                                          u32p, ctypes.POINTER(BfsStats)]
+        L.psb_bfs_session_destroy.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc < 0:
+        buf = ctypes.create_string_buffer(512)
+        lib().psb_last_error(buf, 512)
+        raise PsbError(rc, buf.value.decode(errors="replace"))
+    return rc
+
+
+def device_count():
+    c = ctypes.c_int()
+    _check(lib().psb_device_count(ctypes.byref(c)))
+    return c.value
+
+
+class Puzzle:
+    """Common/Puzzle.h:16-48, backed by a psb_puzzle handle."""
+    MAX_INDEXES_BUFFER = 2 * 1024 * 1024   # Common/Puzzle.h:18
+    INVALID_INDEX = INVALID_INDEX           # Common/Puzzle.h:19
+
+    def __init__(self, kind, a, b=0):
+        h = ctypes.c_void_p()
+        _check(lib().psb_puzzle_create(kind, a, b, ctypes.byref(h)))
+        self._h = h
+        self.kind, self.a, self.b = kind, a, b
+        n = ctypes.c_uint64()
+        ops, br, odd = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().psb_puzzle_info(h, ctypes.byref(n), ctypes.byref(ops), ctypes.byref(br), ctypes.byref(odd)))
+        self._info = (n.value, ops.value, br.value, bool(odd.value))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.psb_puzzle_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def Name(self):
+        buf = ctypes.create_string_buffer(256)
+        _check(lib().psb_puzzle_name(self._h, buf, 256))
+        return buf.value.decode()
+
+    def IndexesCount(self):
+        return self._info[0]
+
+    def OperatorsCount(self):
+        return self._info[1]
+
+    def BranchingFactor(self):
+        return self._info[2]
+
+    def HasOddLengthCycles(self):
+        return self._info[3]
+
+    def Parse(self, state):
+        out = ctypes.c_uint64()
+        _check(lib().psb_parse(self._h, state.encode(), ctypes.byref(out)))
+        return out.value
+
+    def ToString(self, index):
+        buf = ctypes.create_string_buffer(512)
+        _check(lib().psb_to_string(self._h, index, buf, 512))
+        return buf.value.decode()
+
+    def Expand(self, indexes, usedOperatorBits=None, compact=True):
+        """Puzzle::Expand: returns (expandedIndexes, expandedOperators).
+
+        compact=True drops INVALID_INDEX slots (what ExpandBuffer does,
+        Common/Puzzle.h:95-101); compact=False returns BranchingFactor() slots
+        per parent like the reference's GPU puzzles."""
+        n = len(indexes)
+        br = self.BranchingFactor()
+        P = (ctypes.c_uint64 * max(n, 1))(*indexes)
+        flags = EXPAND_HOST_POINTERS | (EXPAND_COMPACT if compact else 0)
+        O = None
+        if usedOperatorBits is not None:
+            O = (ctypes.c_uint32 * max(n, 1))(*usedOperatorBits)
+            flags |= EXPAND_USE_OPBITS
+        cap = max(n * br, 1)
+        C = (ctypes.c_uint64 * cap)()
+        CO = (ctypes.c_uint32 * cap)()
+        n_out = ctypes.c_uint64()
+        _check(lib().psb_expand(self._h, P, O, n, C, CO, cap, ctypes.byref(n_out), flags, None))
+        k = n_out.value
+        return list(C[:k]), list(CO[:k])
+
+    def expand_device(self, parents_ptr, opbits_ptr, n, children_ptr, ops_ptr, stream=None):
+        """Expand with device pointers (ints); BranchingFactor() slots per parent."""
+        n_out = ctypes.c_uint64()
+        flags = EXPAND_USE_OPBITS if opbits_ptr else 0
+        _check(lib().psb_expand(self._h, ctypes.cast(parents_ptr, u64p), ctypes.cast(opbits_ptr or 0, u32p), n,
+                                ctypes.cast(children_ptr, u64p), ctypes.cast(ops_ptr, u32p),
+                                n * self.BranchingFactor(), ctypes.byref(n_out), flags, stream))
+        return n_out.value
+
+    def footprint(self, algo):
+        b = ctypes.c_uint64()
+        _check(lib().psb_bfs_footprint(self._h, _algo(algo), ctypes.byref(b)))
+        return b.value
+
+    def final_words(self, algo):
+        w = ctypes.c_uint64()
+        _check(lib().psb_final_words(self._h, _algo(algo), ctypes.byref(w)))
+        return w.value
+
+
+class SlidingTilePuzzleSimple(Puzzle):
+    """Puzzles/SlidingTilePuzzleSimple.h: index = permutation rank over width*height cells."""
+
+    def __init__(self, width, height):
+        super().__init__(SLIDING, width, height)
+
+
+class PancakeSimple(Puzzle):
+    """Puzzles/PancakeSimple.h: operator k reverses the last k+2 values."""
+
+    def __init__(self, size):
+        super().__init__(PANCAKE, size, 0)
+
+
+class FourPegHanoiSimple(Puzzle):
+    """Puzzles/FourPegHanoiSimple.h: 2 bits per disk; optional peg symmetry."""
+
+    def __init__(self, size, useSymmetry=False):
+        super().__init__(HANOI4, size, 1 if useSymmetry else 0)
+
+
+def _algo(algo):
+    return ALGOS[algo] if isinstance(algo, str) else int(algo)
+
+
+def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_ms=None, level_children=None):
+    o = BfsOpts()
+    o.struct_size = ctypes.sizeof(BfsOpts)
+    o.max_depth = max_depth
+    o.window_bits = window_bits
+    o.device = device
+    o.stream = stream
+    if final is not None:
+        o.final_words = ctypes.cast(final, u64p)
+        o.final_cap = len(final)
+    if level_ms is not None:
+        o.level_ms = level_ms
+    if level_children is not None:
+        o.level_children = level_children
+    return o
+
+
+def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels=False, device=-1):
+    """Runs psb_bfs.  Returns a dict with counts, stats and optionally the final
+    arrays (list of 64-bit words in the reference's layout) and per-level data."""
+    if isinstance(initial, str):
+        initial = puzzle.Parse(initial)
+    cap = 1 << 16
+    counts = (ctypes.c_uint64 * cap)()
+    nd = ctypes.c_uint32()
+    fin = None
+    if final:
+        fin = (ctypes.c_uint64 * puzzle.final_words(algo))()
+    lm = (ctypes.c_float * cap)() if levels else None
+    lc = (ctypes.c_uint64 * cap)() if levels else None
+    o = _opts(max_depth, window_bits, device, None, fin, lm, lc)
+    st = BfsStats()
+    st.struct_size = ctypes.sizeof(BfsStats)
+    _check(lib().psb_bfs(puzzle.handle, _algo(algo), initial, ctypes.byref(o), counts, cap, ctypes.byref(nd),
+                         ctypes.byref(st)))
+    out = {"counts": list(counts[:nd.value]), "stats": st.as_dict()}
+    if final:
+        out["final"] = list(fin)
+    if levels:
+        out["level_ms"] = list(lm[:nd.value])
+        out["level_children"] = list(lc[:nd.value])
+    return out
+
+
+class BfsSession:
+    """psb_bfs_session: device arrays allocated once, reused by run()."""
+
+    def __init__(self, puzzle, algo, window_bits=0, device=-1):
+        self.puzzle = puzzle
+        self.algo = _algo(algo)
+        h = ctypes.c_void_p()
+        o = _opts(0, window_bits, device)
+        _check(lib().psb_bfs_session_create(puzzle.handle, self.algo, ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self._cap = 1 << 16
+        self._counts = (ctypes.c_uint64 * self._cap)()
+
+    def run(self, initial=0, max_depth=0):
+        nd = ctypes.c_uint32()
+        st = BfsStats()
+        st.struct_size = ctypes.sizeof(BfsStats)
+        o = _opts(max_depth)
+        _check(lib().psb_bfs_session_run(self._h, initial, ctypes.byref(o), self._counts, self._cap,
+                                         ctypes.byref(nd), ctypes.byref(st)))
+        return list(self._counts[:nd.value]), st.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().psb_bfs_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+
+def _run(puzzle, algo, initialState):
+    return bfs(puzzle, algo, puzzle.Parse(initialState))["counts"]
+
+
+def InMemoryClassicBFS(puzzle, initialState):
+    """Common/InMemoryClassicBFS.cpp:4-45 on the GPU."""
+    return _run(puzzle, CLASSIC, initialState)
+
+
+def InMemoryTwoBitBFS(puzzle, initialState):
+    """Common/InMemoryTwoBitBFS.cpp:24-69 on the GPU."""
+    return _run(puzzle, TWO_BIT, initialState)
+
+
+def InMemoryThreeBitBFS(puzzle, initialState):
+    """Common/InMemoryThreeBitBFS.cpp:4-48 on the GPU."""
+    return _run(puzzle, THREE_BIT, initialState)
+
+
+def InMemoryFrontierSearch(puzzle, initialState):
+    """Common/InMemoryFrontierSearch.cpp:57-112 on the GPU."""
+    return _run(puzzle, FRONTIER, initialState)

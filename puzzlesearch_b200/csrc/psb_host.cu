@@ -1,0 +1,742 @@
+// psb_host.cu -- host side of the C ABI declared in include/psb200.h:
+// puzzle handles, Parse/ToString, batched Expand and the in-memory search
+// drivers that keep every bit array in device memory and launch one fused
+// level kernel (plus a finalize pass for three-bit and classic) per BFS level.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/psb200.h"
+#include "psb_kernels.cuh"
+
+using psb::LevelArgs;
+using psb::PuzzleArgs;
+using psb::PuzzleKernels;
+
+struct psb_puzzle {
+    int kind, a, b;
+    int cells;  // permutation size (sliding, pancake)
+    uint64_t n_states;
+    int ops, branching, odd;
+    PuzzleKernels k;
+    PuzzleArgs pz;
+};
+
+namespace psb {
+
+// Three-bit level end (InMemoryThreeBitBFS.cpp:31-42):
+//   if odd cycles: new &= ~cur;  count = popcount(new &= ~old);  optionally old = 0.
+__global__ void __launch_bounds__(kThreads) finalize_three_bit(const ulonglong2* __restrict__ cur,
+                                                              ulonglong2* __restrict__ nw,
+                                                              ulonglong2* __restrict__ old, uint64_t n2,
+                                                              int odd, int zero_old,
+                                                              unsigned long long* count) {
+    uint32_t c = 0;
+    for (uint64_t i = blockIdx.x * uint64_t(kThreads) + threadIdx.x; i < n2; i += uint64_t(gridDim.x) * kThreads) {
+        ulonglong2 n = nw[i];
+        const ulonglong2 o = old[i];
+        n.x &= ~o.x;
+        n.y &= ~o.y;
+        if (odd) {
+            const ulonglong2 k = cur[i];
+            n.x &= ~k.x;
+            n.y &= ~k.y;
+        }
+        nw[i] = n;
+        if (zero_old) old[i] = make_ulonglong2(0, 0);
+        c += __popcll(n.x) + __popcll(n.y);
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// Classic level end (InMemoryClassicBFS.cpp:36-37):
+//   count = popcount(newOpen &= ~closed);  closed |= newOpen.
+__global__ void __launch_bounds__(kThreads) finalize_classic(ulonglong2* __restrict__ nw,
+                                                            ulonglong2* __restrict__ closed, uint64_t n2,
+                                                            unsigned long long* count) {
+    uint32_t c = 0;
+    for (uint64_t i = blockIdx.x * uint64_t(kThreads) + threadIdx.x; i < n2; i += uint64_t(gridDim.x) * kThreads) {
+        ulonglong2 n = nw[i];
+        ulonglong2 k = closed[i];
+        n.x &= ~k.x;
+        n.y &= ~k.y;
+        nw[i] = n;
+        k.x |= n.x;
+        k.y |= n.y;
+        closed[i] = k;
+        c += __popcll(n.x) + __popcll(n.y);
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+}  // namespace psb
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+#define PSB_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? PSB_ERR_NOMEM : PSB_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                        \
+    } while (0)
+
+uint64_t factorial(int n) {
+    uint64_t r = 1;
+    for (int i = 2; i <= n; i++) r *= uint64_t(i);
+    return r;
+}
+
+// Permutation index of the reference (Puzzles/PermutationMap.cpp:39-58), host side.
+uint64_t rank_host(const int* v, int n) {
+    uint64_t index = 0;
+    unsigned seen = 0;
+    for (int i = 0; i < n; i++) {
+        const int digit = v[i] - __builtin_popcount(seen & ((1u << v[i]) - 1u));
+        seen |= 1u << v[i];
+        index = index * uint64_t(n - i) + uint64_t(digit);
+    }
+    return index;
+}
+
+void unrank_host(uint64_t index, int* v, int n) {
+    int d[16];
+    for (int i = n - 1; i >= 0; i--) {
+        d[i] = int(index % uint64_t(n - i));
+        index /= uint64_t(n - i);
+    }
+    unsigned used = 0;
+    for (int i = 0; i < n; i++) {
+        int k = d[i], val = 0;
+        for (;; val++) {
+            if (used & (1u << val)) continue;
+            if (k-- == 0) break;
+        }
+        v[i] = val;
+        used |= 1u << val;
+    }
+}
+
+bool read_ints(const char* s, std::vector<int>& out) {
+    std::istringstream in(s);
+    std::string tok;
+    while (in >> tok) {
+        char* end = nullptr;
+        long v = strtol(tok.c_str(), &end, 10);
+        if (!end || *end) return false;
+        out.push_back(int(v));
+    }
+    return true;
+}
+
+int ensure_device(int device) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return fail(PSB_ERR_NO_DEVICE, "no CUDA device visible");
+    if (device >= 0) {
+        if (device >= count) return fail(PSB_ERR_ARG, "device %d out of range (%d visible)", device, count);
+        PSB_CUDA(cudaSetDevice(device));
+    }
+    return PSB_OK;
+}
+
+// Scratch device buffers of psb_expand, one set per host thread.
+struct ExpandPool {
+    int device = -1;
+    uint64_t cap = 0, out_cap = 0;
+    uint64_t* d_par = nullptr;
+    uint32_t* d_ops_in = nullptr;
+    uint64_t* d_out = nullptr;
+    uint32_t* d_ops = nullptr;
+    unsigned long long* d_err = nullptr;
+    cudaStream_t stream = nullptr;
+    void release() {
+        cudaFree(d_par); cudaFree(d_ops_in); cudaFree(d_out); cudaFree(d_ops); cudaFree(d_err);
+        if (stream) cudaStreamDestroy(stream);
+        *this = ExpandPool();
+    }
+    ~ExpandPool() { if (device >= 0) release(); }
+};
+thread_local ExpandPool g_pool;
+
+constexpr uint64_t kExpandChunk = 2 * 1024 * 1024;  // Puzzle::MAX_INDEXES_BUFFER, Common/Puzzle.h:18
+
+int pool_reserve(int branching) {
+    int dev = 0;
+    PSB_CUDA(cudaGetDevice(&dev));
+    const uint64_t out_cap = kExpandChunk * uint64_t(branching);
+    if (g_pool.device == dev && g_pool.out_cap >= out_cap) return PSB_OK;
+    if (g_pool.device >= 0) g_pool.release();
+    g_pool.device = dev;
+    PSB_CUDA(cudaMalloc(&g_pool.d_par, kExpandChunk * 8));
+    PSB_CUDA(cudaMalloc(&g_pool.d_ops_in, kExpandChunk * 4));
+    PSB_CUDA(cudaMalloc(&g_pool.d_out, out_cap * 8));
+    PSB_CUDA(cudaMalloc(&g_pool.d_ops, out_cap * 4));
+    PSB_CUDA(cudaMalloc(&g_pool.d_err, 8));
+    PSB_CUDA(cudaStreamCreateWithFlags(&g_pool.stream, cudaStreamNonBlocking));
+    g_pool.cap = kExpandChunk;
+    g_pool.out_cap = out_cap;
+    return PSB_OK;
+}
+
+int mode_of(int algo) {
+    switch (algo) {
+    case PSB_THREE_BIT: return psb::kThreeBit;
+    case PSB_CLASSIC: return psb::kClassic;
+    case PSB_TWO_BIT: return psb::kTwoBit;
+    case PSB_FRONTIER: return psb::kFrontier;
+    }
+    return -1;
+}
+
+uint64_t words_for(uint64_t bits) { return (bits + 63) / 64; }
+uint64_t padded(uint64_t words) { return (words + 31) / 32 * 32; }  // 256-byte multiples for 128-bit sweeps
+
+}  // namespace
+
+extern "C" {
+
+const char* psb_version(void) { return "puzzlesearch_b200 1.0 (sm_100a)"; }
+
+int psb_last_error(char* buf, int cap) {
+    if (!buf || cap <= 0) return PSB_ERR_ARG;
+    snprintf(buf, size_t(cap), "%s", g_error.c_str());
+    return PSB_OK;
+}
+
+int psb_device_count(int* count) {
+    if (!count) return PSB_ERR_ARG;
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) c = 0;
+    *count = c;
+    return PSB_OK;
+}
+
+int psb_puzzle_create(int kind, int a, int b, psb_puzzle** out) {
+    if (!out) return fail(PSB_ERR_ARG, "out is NULL");
+    auto p = std::make_unique<psb_puzzle>();
+    p->kind = kind; p->a = a; p->b = b;
+    p->pz = PuzzleArgs{0, 0, 0};
+    bool ok = false;
+    switch (kind) {
+    case PSB_SLIDING:  // SlidingTilePuzzleSimple.h:13-19, .cpp:35-39
+        if (a < 1 || b < 1 || a * b < 2 || a * b > 16) return fail(PSB_ERR_ARG, "sliding tile %dx%d: need 2 <= w*h <= 16", a, b);
+        p->cells = a * b; p->n_states = factorial(a * b); p->ops = 4; p->branching = 4; p->odd = 0;
+        p->pz.width = a;
+        ok = psb::sliding_kernels(a * b, &p->k);
+        break;
+    case PSB_PANCAKE:  // PancakeSimple.h:13-19, .cpp:26,36-40
+        if (a < 2 || a > 16) return fail(PSB_ERR_ARG, "pancake size %d: need 2..16", a);
+        p->cells = a; p->n_states = factorial(a); p->ops = a - 1; p->branching = a - 1; p->odd = 1;
+        ok = psb::pancake_kernels(a, &p->k);
+        break;
+    case PSB_HANOI4:  // FourPegHanoiSimple.h:14-20, .cpp:141-143
+        if (a < 1 || a > 31) return fail(PSB_ERR_ARG, "hanoi disks %d: need 1..31", a);
+        p->cells = 0; p->n_states = uint64_t(1) << (2 * a); p->ops = 4; p->branching = 6; p->odd = 1;
+        p->pz.disks = a; p->pz.sym = b ? 1 : 0;
+        ok = psb::hanoi_kernels(&p->k);
+        break;
+    default:
+        return fail(PSB_ERR_ARG, "unknown puzzle kind %d", kind);
+    }
+    if (!ok) return fail(PSB_ERR_UNSUPPORTED, "no kernels for this puzzle");
+    *out = p.release();
+    return PSB_OK;
+}
+
+int psb_puzzle_destroy(psb_puzzle* p) {
+    delete p;
+    return PSB_OK;
+}
+
+int psb_puzzle_info(const psb_puzzle* p, uint64_t* indexes, int* operators, int* branching, int* odd) {
+    if (!p) return fail(PSB_ERR_ARG, "puzzle is NULL");
+    if (indexes) *indexes = p->n_states;
+    if (operators) *operators = p->ops;
+    if (branching) *branching = p->branching;
+    if (odd) *odd = p->odd;
+    return PSB_OK;
+}
+
+int psb_puzzle_name(const psb_puzzle* p, char* buf, int cap) {
+    if (!p || !buf || cap <= 0) return fail(PSB_ERR_ARG, "bad argument");
+    std::ostringstream s;
+    switch (p->kind) {
+    case PSB_SLIDING: s << "Sliding-Tile simple: " << p->a << " x " << p->b; break;   // SlidingTilePuzzleSimple.cpp:27-32
+    case PSB_PANCAKE: s << "Pancake simple, size: " << p->a; break;                   // PancakeSimple.cpp:29-33
+    case PSB_HANOI4: s << "Four-Peg Hanoi Towers, size=" << p->a << "; symmetry=" << (p->b ? 1 : 0); break;  // FourPegHanoiSimple.cpp:129-135
+    }
+    const std::string str = s.str();
+    if (int(str.size()) + 1 > cap) return fail(PSB_ERR_CAPACITY, "name buffer too small");
+    memcpy(buf, str.c_str(), str.size() + 1);
+    return int(str.size());
+}
+
+int psb_parse(const psb_puzzle* p, const char* state, uint64_t* index) {
+    if (!p || !state || !index) return fail(PSB_ERR_ARG, "bad argument");
+    std::vector<int> v;
+    if (!read_ints(state, v)) return fail(PSB_ERR_ARG, "cannot parse state '%s'", state);
+    if (p->kind != PSB_HANOI4) {
+        // SlidingTilePuzzleSimple.cpp:52-59, PancakeSimple.cpp:53-60: a permutation of 0..n-1.
+        if (int(v.size()) != p->cells) return fail(PSB_ERR_ARG, "state '%s' needs %d values", state, p->cells);
+        unsigned seen = 0;
+        for (int x : v) {
+            if (x < 0 || x >= p->cells || (seen >> x) & 1u) return fail(PSB_ERR_ARG, "state '%s' is not a permutation", state);
+            seen |= 1u << x;
+        }
+        *index = rank_host(v.data(), p->cells);
+        return PSB_OK;
+    }
+    // FourPegHanoiSimple.cpp:85-113: disks (1-based) listed peg by peg, a 0 between pegs.
+    uint64_t idx = 0;
+    int peg = 0;
+    for (int x : v) {
+        if (x == 0) { peg++; continue; }
+        if (peg > 3 || x < 1 || x > p->a) return fail(PSB_ERR_ARG, "bad Hanoi state '%s'", state);
+        idx |= uint64_t(peg) << (2 * (x - 1));
+    }
+    *index = idx;
+    return PSB_OK;
+}
+
+int psb_to_string(const psb_puzzle* p, uint64_t index, char* buf, int cap) {
+    if (!p || !buf || cap <= 0) return fail(PSB_ERR_ARG, "bad argument");
+    if (index >= p->n_states) return fail(PSB_ERR_ARG, "index out of range");
+    std::ostringstream s;
+    if (p->kind != PSB_HANOI4) {
+        int v[16];
+        unrank_host(index, v, p->cells);
+        for (int i = 0; i < p->cells; i++) s << (i ? " " : "") << v[i];
+    } else {
+        // FourPegHanoiSimple.cpp:71-83: each peg top-down (1-based), then "0 ", last " 0 " dropped.
+        std::string str;
+        for (int peg = 0; peg < 4; peg++) {
+            for (int d = 0; d < p->a; d++)
+                if (int((index >> (2 * d)) & 3) == peg) str += std::to_string(d + 1) + " ";
+            str += "0 ";
+        }
+        s << str.substr(0, str.size() - 3);
+    }
+    const std::string str = s.str();
+    if (int(str.size()) + 1 > cap) return fail(PSB_ERR_CAPACITY, "string buffer too small");
+    memcpy(buf, str.c_str(), str.size() + 1);
+    return int(str.size());
+}
+
+int psb_expand(const psb_puzzle* p, const uint64_t* parents, const uint32_t* opbits, uint64_t n, uint64_t* children,
+               uint32_t* child_ops, uint64_t cap, uint64_t* n_out, uint32_t flags, void* stream) {
+    if (!p || !n_out || (n && (!parents || !children || !child_ops)))
+        return fail(PSB_ERR_ARG, "bad argument");
+    const bool host = flags & PSB_EXPAND_HOST_POINTERS;
+    const bool compact = flags & PSB_EXPAND_COMPACT;
+    const bool use_ob = (flags & PSB_EXPAND_USE_OPBITS) && opbits;
+    const uint64_t br = uint64_t(p->branching);
+    if (compact && !host) return fail(PSB_ERR_ARG, "PSB_EXPAND_COMPACT needs host pointers");
+    if (!compact && cap < n * br) return fail(PSB_ERR_CAPACITY, "need %llu output slots", (unsigned long long)(n * br));
+    *n_out = 0;
+    if (n == 0) return PSB_OK;
+    if (int rc = ensure_device(-1)) return rc;
+    if (int rc = pool_reserve(p->branching)) return rc;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g_pool.stream;
+    PSB_CUDA(cudaMemsetAsync(g_pool.d_err, 0, 8, s));
+    if (!host) {
+        // Device pointers: one launch per chunk, slots written in place.
+        for (uint64_t off = 0; off < n; off += kExpandChunk) {
+            const uint64_t m = std::min(kExpandChunk, n - off);
+            PSB_CUDA(p->k.expand(parents + off, use_ob ? opbits + off : nullptr, m, p->n_states, children + off * br,
+                                 child_ops + off * br, p->pz, g_pool.d_err, use_ob, s));
+        }
+        unsigned long long err = 0;
+        PSB_CUDA(cudaMemcpyAsync(&err, g_pool.d_err, 8, cudaMemcpyDeviceToHost, s));
+        PSB_CUDA(cudaStreamSynchronize(s));
+        if (err) return fail(PSB_ERR_ARG, "a parent index is >= IndexesCount()");
+        *n_out = n * br;
+        return PSB_OK;
+    }
+    for (uint64_t i = 0; i < n; i++)
+        if (parents[i] >= p->n_states) return fail(PSB_ERR_ARG, "parent %llu >= IndexesCount()", (unsigned long long)parents[i]);
+    std::vector<uint64_t> hbuf;
+    std::vector<uint32_t> obuf;
+    uint64_t written = 0;
+    for (uint64_t off = 0; off < n; off += kExpandChunk) {
+        const uint64_t m = std::min(kExpandChunk, n - off);
+        PSB_CUDA(cudaMemcpyAsync(g_pool.d_par, parents + off, m * 8, cudaMemcpyHostToDevice, s));
+        if (use_ob) PSB_CUDA(cudaMemcpyAsync(g_pool.d_ops_in, opbits + off, m * 4, cudaMemcpyHostToDevice, s));
+        PSB_CUDA(p->k.expand(g_pool.d_par, g_pool.d_ops_in, m, p->n_states, g_pool.d_out, g_pool.d_ops, p->pz,
+                             g_pool.d_err, use_ob, s));
+        uint64_t* dst = children + off * br;
+        uint32_t* dop = child_ops + off * br;
+        if (compact) {
+            hbuf.resize(m * br);
+            obuf.resize(m * br);
+            dst = hbuf.data();
+            dop = obuf.data();
+        }
+        PSB_CUDA(cudaMemcpyAsync(dst, g_pool.d_out, m * br * 8, cudaMemcpyDeviceToHost, s));
+        PSB_CUDA(cudaMemcpyAsync(dop, g_pool.d_ops, m * br * 4, cudaMemcpyDeviceToHost, s));
+        PSB_CUDA(cudaStreamSynchronize(s));
+        if (compact) {
+            for (uint64_t j = 0; j < m * br; j++) {
+                if (hbuf[j] == PSB_INVALID_INDEX) continue;  // ExpandBuffer filters these (Common/Puzzle.h:98)
+                if (written >= cap) return fail(PSB_ERR_CAPACITY, "compacted output exceeds cap");
+                children[written] = hbuf[j];
+                child_ops[written] = obuf[j];
+                written++;
+            }
+        } else {
+            written += m * br;
+        }
+    }
+    *n_out = written;
+    return PSB_OK;
+}
+
+int psb_final_words(const psb_puzzle* p, int algo, uint64_t* words) {
+    if (!p || !words) return fail(PSB_ERR_ARG, "bad argument");
+    const uint64_t N = p->n_states;
+    switch (algo) {
+    case PSB_TWO_BIT: *words = words_for(2 * N); return PSB_OK;
+    case PSB_THREE_BIT: case PSB_CLASSIC: *words = 3 * words_for(N); return PSB_OK;
+    case PSB_FRONTIER: *words = 2 * ((N + 15) / 16); return PSB_OK;
+    }
+    return fail(PSB_ERR_ARG, "unknown algorithm %d", algo);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// In-memory search session.
+// ---------------------------------------------------------------------------
+struct psb_bfs_session {
+    psb_puzzle p;
+    int algo = 0, mode = 0, device = -1, window_bits = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint64_t* arr[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t words[4] = {0, 0, 0, 0};  // padded sizes
+    int n_arr = 0;
+    unsigned long long* d_stats = nullptr;
+    unsigned long long* h_stats = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t bytes = 0;
+
+    ~psb_bfs_session() {
+        for (auto* a : arr) if (a) cudaFree(a);
+        if (d_stats) cudaFree(d_stats);
+        if (h_stats) cudaFreeHost(h_stats);
+        for (auto& e : ev) if (e) cudaEventDestroy(e);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int layout(const psb_puzzle* p, int algo, uint64_t* words, int* n_arr) {
+    const uint64_t N = p->n_states;
+    switch (algo) {
+    case PSB_THREE_BIT: case PSB_CLASSIC:
+        *n_arr = 3;
+        words[0] = words[1] = words[2] = padded(words_for(N));
+        return PSB_OK;
+    case PSB_TWO_BIT:
+        *n_arr = 1;
+        words[0] = padded(words_for(2 * N));
+        return PSB_OK;
+    case PSB_FRONTIER:
+        if (p->ops > 4) return fail(PSB_ERR_UNSUPPORTED, "frontier search keeps 4 operator bits per state; this puzzle has %d operators", p->ops);
+        *n_arr = p->odd ? 4 : 2;
+        words[0] = words[1] = padded((N + 15) / 16);
+        if (p->odd) words[2] = words[3] = padded(words_for(N));
+        return PSB_OK;
+    }
+    return fail(PSB_ERR_ARG, "unknown algorithm %d", algo);
+}
+
+int auto_window_bits(const psb_puzzle* p, int algo) {
+    int lg = 0;
+    while (lg < 63 && (uint64_t(1) << (lg + 1)) <= p->n_states) lg++;
+    int wb = std::max(10, std::min(18, lg - 10));
+    if (algo == PSB_FRONTIER) wb = std::min(wb, 16);  // 4 mark bits per state
+    return wb;
+}
+
+size_t smem_bytes(int mode, int wb) {
+    const size_t W = size_t(1) << wb;
+    switch (mode) {
+    case psb::kFrontier: return W / 2 + size_t(psb::kThreads) * 64 * 4;
+    case psb::kTwoBit: return W / 8 + size_t(psb::kThreads) * 32 * 2;
+    default: return W / 8 + size_t(psb::kThreads) * 64 * 2;
+    }
+}
+
+int set_bit(uint64_t* d_word_base, uint64_t bit, cudaStream_t s) {
+    // OR one bit into a freshly cleared array: the whole 64-bit word is written.
+    static thread_local uint64_t word;  // pageable host source, copied before return
+    word = uint64_t(1) << (bit & 63);
+    PSB_CUDA(cudaMemcpyAsync(d_word_base + (bit >> 6), &word, 8, cudaMemcpyHostToDevice, s));
+    PSB_CUDA(cudaStreamSynchronize(s));
+    return PSB_OK;
+}
+
+int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, uint64_t* counts, uint32_t cap,
+                uint32_t* n_depths, psb_bfs_stats* stats) {
+    const psb_puzzle& P = S->p;
+    const uint64_t N = P.n_states;
+    if (initial >= N) return fail(PSB_ERR_ARG, "initial index %llu >= IndexesCount()", (unsigned long long)initial);
+    if (!counts || !n_depths || cap == 0) return fail(PSB_ERR_ARG, "counts buffer missing");
+    const uint32_t max_depth = opts ? opts->max_depth : 0;
+    cudaStream_t s = S->stream;
+    if (S->device >= 0) PSB_CUDA(cudaSetDevice(S->device));
+    for (int i = 0; i < S->n_arr; i++) PSB_CUDA(cudaMemsetAsync(S->arr[i], 0, S->words[i] * 8, s));
+    PSB_CUDA(cudaEventRecord(S->ev[0], s));
+
+    const uint64_t W1 = words_for(N), W2 = words_for(2 * N), W4 = (N + 15) / 16;
+    const unsigned grid = unsigned((N + (uint64_t(1) << S->window_bits) - 1) >> S->window_bits);
+    const size_t smem = smem_bytes(S->mode, S->window_bits);
+    LevelArgs a{};
+    a.n_states = N;
+    a.window_bits = S->window_bits;
+    a.odd = P.odd;
+    a.pz = P.pz;
+    a.stats = S->d_stats;
+
+    uint64_t *old_ = S->arr[0], *cur = S->arr[1], *nw = S->arr[2];       // three-bit
+    uint64_t *closed = S->arr[0], *open = S->arr[1], *nopen = S->arr[2]; // classic
+    uint64_t *codes = S->arr[0];                                         // two-bit
+    uint64_t *fcur = S->arr[0], *fnext = S->arr[1], *cex = S->arr[2], *nex = S->arr[3];  // frontier
+    uint32_t cur_code = 2;
+
+    switch (S->algo) {
+    case PSB_THREE_BIT: if (int rc = set_bit(cur, initial, s)) return rc; break;
+    case PSB_CLASSIC:
+        if (int rc = set_bit(open, initial, s)) return rc;
+        if (int rc = set_bit(closed, initial, s)) return rc;
+        break;
+    case PSB_TWO_BIT: if (int rc = set_bit(codes, 2 * initial, s)) return rc; break;  // code CUR = 2: bit 2i
+    default: break;
+    }
+
+    std::vector<uint64_t> res;
+    double expand_ms = 0, finalize_ms = 0;
+    uint64_t expanded = 0, children = 0, local = 0, launches = 0;
+    const bool want_final = opts && opts->final_words;
+    bool first = true;
+    for (;;) {
+        if (max_depth && res.size() >= size_t(max_depth) + 1) break;
+        PSB_CUDA(cudaMemsetAsync(S->d_stats, 0, 8 * sizeof(unsigned long long), s));
+        PSB_CUDA(cudaEventRecord(S->ev[1], s));
+        uint64_t count = 0;
+        if (S->algo == PSB_FRONTIER && first) {
+            a.marks = fnext; a.excl_next = nex; a.mark_words = W4;
+            PSB_CUDA(P.k.seed(a, initial, s));
+        } else {
+            switch (S->algo) {
+            case PSB_THREE_BIT: a.front = cur; a.marks = nw; a.front_words = W1; a.mark_words = W1; break;
+            case PSB_CLASSIC: a.front = open; a.marks = nopen; a.front_words = W1; a.mark_words = W1; break;
+            case PSB_TWO_BIT: a.front = codes; a.marks = codes; a.front_words = W2; a.mark_words = W2; a.cur_code = cur_code; break;
+            case PSB_FRONTIER:
+                a.front = fcur; a.marks = fnext; a.excl_cur = cex; a.excl_next = nex;
+                a.front_words = W4; a.mark_words = W4;
+                break;
+            }
+            PSB_CUDA(P.k.level[S->mode](a, grid, smem, s));
+            launches++;
+        }
+        PSB_CUDA(cudaEventRecord(S->ev[2], s));
+        if (S->algo == PSB_THREE_BIT || S->algo == PSB_CLASSIC) {
+            const unsigned fgrid = 148 * 8;
+            const uint64_t n2 = (W1 + 1) / 2;
+            if (S->algo == PSB_THREE_BIT)
+                psb::finalize_three_bit<<<fgrid, psb::kThreads, 0, s>>>(
+                    reinterpret_cast<const ulonglong2*>(cur), reinterpret_cast<ulonglong2*>(nw),
+                    reinterpret_cast<ulonglong2*>(old_), n2, P.odd, want_final ? 0 : 1, S->d_stats + 4);
+            else
+                psb::finalize_classic<<<fgrid, psb::kThreads, 0, s>>>(
+                    reinterpret_cast<ulonglong2*>(nopen), reinterpret_cast<ulonglong2*>(closed), n2, S->d_stats + 4);
+            PSB_CUDA(cudaGetLastError());
+        }
+        PSB_CUDA(cudaEventRecord(S->ev[3], s));
+        PSB_CUDA(cudaMemcpyAsync(S->h_stats, S->d_stats, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        PSB_CUDA(cudaStreamSynchronize(s));
+        if (S->h_stats[3]) return fail(PSB_ERR_DEVICE, "level kernel produced a child index >= IndexesCount()");
+        float t_exp = 0, t_fin = 0;
+        PSB_CUDA(cudaEventElapsedTime(&t_exp, S->ev[1], S->ev[2]));
+        PSB_CUDA(cudaEventElapsedTime(&t_fin, S->ev[2], S->ev[3]));
+        expand_ms += t_exp;
+        finalize_ms += t_fin;
+        expanded += (S->algo == PSB_FRONTIER && first) ? 1 : S->h_stats[0];
+        children += S->h_stats[1];
+        local += S->h_stats[2];
+        const size_t lvl = res.size();
+        if (opts && opts->level_ms && lvl < cap) opts->level_ms[lvl] = t_exp + t_fin;
+        if (opts && opts->level_children && lvl < cap) opts->level_children[lvl] = S->h_stats[1];
+
+        switch (S->algo) {
+        case PSB_THREE_BIT:
+            count = S->h_stats[4];
+            if (first) { res.push_back(1); }
+            if (count == 0) goto done;
+            res.push_back(count);
+            { uint64_t* t = old_; old_ = cur; cur = nw; nw = t; }  // old<-cur, cur<-new, new<-old
+            if (want_final) PSB_CUDA(cudaMemsetAsync(nw, 0, W1 * 8, s));
+            break;
+        case PSB_CLASSIC:
+            count = S->h_stats[4];
+            if (first) { res.push_back(1); }
+            if (count == 0) goto done;
+            res.push_back(count);
+            std::swap(open, nopen);
+            break;
+        case PSB_TWO_BIT:
+            count = S->h_stats[0];  // states found with code CUR = states at this depth
+            if (count == 0) goto done;
+            res.push_back(count);
+            cur_code = 5 - cur_code;
+            break;
+        case PSB_FRONTIER:
+            count = first ? 1 : S->h_stats[0];
+            if (count == 0) goto done;
+            res.push_back(count);
+            std::swap(fcur, fnext);
+            if (P.odd) {
+                std::swap(cex, nex);
+                PSB_CUDA(cudaMemsetAsync(nex, 0, W1 * 8, s));
+            }
+            break;
+        }
+        first = false;
+        if (res.size() > cap) return fail(PSB_ERR_CAPACITY, "more than %u depths", cap);
+    }
+done:
+    PSB_CUDA(cudaEventRecord(S->ev[3], s));
+    PSB_CUDA(cudaEventSynchronize(S->ev[3]));
+    float total = 0;
+    PSB_CUDA(cudaEventElapsedTime(&total, S->ev[0], S->ev[3]));
+    if (res.size() > cap) return fail(PSB_ERR_CAPACITY, "more than %u depths", cap);
+    std::copy(res.begin(), res.end(), counts);
+    *n_depths = uint32_t(res.size());
+
+    if (want_final) {
+        uint64_t need = 0;
+        psb_final_words(&P, S->algo, &need);
+        if (opts->final_cap < need) return fail(PSB_ERR_CAPACITY, "final_words needs %llu words", (unsigned long long)need);
+        uint64_t* out = opts->final_words;
+        auto copy = [&](const uint64_t* src, uint64_t w) -> int {
+            PSB_CUDA(cudaMemcpyAsync(out, src, w * 8, cudaMemcpyDeviceToHost, s));
+            out += w;
+            return PSB_OK;
+        };
+        int rc = PSB_OK;
+        switch (S->algo) {
+        case PSB_THREE_BIT: rc = copy(old_, W1); if (!rc) rc = copy(cur, W1); if (!rc) rc = copy(nw, W1); break;
+        case PSB_CLASSIC: rc = copy(closed, W1); if (!rc) rc = copy(open, W1); if (!rc) rc = copy(nopen, W1); break;
+        case PSB_TWO_BIT: rc = copy(codes, W2); break;
+        case PSB_FRONTIER: rc = copy(fcur, W4); if (!rc) rc = copy(fnext, W4); break;
+        }
+        if (rc) return rc;
+        PSB_CUDA(cudaStreamSynchronize(s));
+    }
+    if (stats && stats->struct_size >= sizeof(psb_bfs_stats)) {
+        stats->levels = uint32_t(launches);
+        stats->window_bits = uint32_t(S->window_bits);
+        stats->threads = uint32_t(psb::kThreads);
+        stats->total_ms = total;
+        stats->expand_ms = expand_ms;
+        stats->finalize_ms = finalize_ms;
+        stats->expanded = expanded;
+        stats->children = children;
+        stats->local_children = local;
+        stats->expand_launches = launches;
+        stats->device_bytes = S->bytes;
+    }
+    return PSB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psb_bfs_footprint(const psb_puzzle* p, int algo, uint64_t* bytes) {
+    if (!p || !bytes) return fail(PSB_ERR_ARG, "bad argument");
+    uint64_t w[4] = {0, 0, 0, 0};
+    int n = 0;
+    if (int rc = layout(p, algo, w, &n)) return rc;
+    *bytes = (w[0] + w[1] + w[2] + w[3]) * 8 + 64;
+    return PSB_OK;
+}
+
+int psb_bfs_session_create(const psb_puzzle* p, int algo, const psb_bfs_opts* opts, psb_bfs_session** out) {
+    if (!p || !out) return fail(PSB_ERR_ARG, "bad argument");
+    if (opts && opts->struct_size != sizeof(psb_bfs_opts)) return fail(PSB_ERR_ARG, "psb_bfs_opts.struct_size mismatch");
+    auto S = std::make_unique<psb_bfs_session>();
+    S->p = *p;
+    S->algo = algo;
+    S->mode = mode_of(algo);
+    if (S->mode < 0) return fail(PSB_ERR_ARG, "unknown algorithm %d", algo);
+    if (int rc = layout(p, algo, S->words, &S->n_arr)) return rc;
+    S->device = opts ? opts->device : -1;
+    if (int rc = ensure_device(S->device)) return rc;
+    if (S->device < 0) PSB_CUDA(cudaGetDevice(&S->device));
+    S->window_bits = (opts && opts->window_bits) ? opts->window_bits : auto_window_bits(p, algo);
+    if (S->window_bits < 10 || S->window_bits > 20 || (algo == PSB_FRONTIER && S->window_bits > 18))
+        return fail(PSB_ERR_ARG, "window_bits %d out of range", S->window_bits);
+    if (((p->n_states + (uint64_t(1) << S->window_bits) - 1) >> S->window_bits) > 0x7FFFFFFFull)
+        return fail(PSB_ERR_ARG, "too many windows");
+    if (opts && opts->stream) S->stream = static_cast<cudaStream_t>(opts->stream);
+    else {
+        PSB_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+        S->own_stream = true;
+    }
+    for (int i = 0; i < S->n_arr; i++) {
+        PSB_CUDA(cudaMalloc(&S->arr[i], S->words[i] * 8));
+        S->bytes += S->words[i] * 8;
+    }
+    PSB_CUDA(cudaMalloc(&S->d_stats, 8 * sizeof(unsigned long long)));
+    PSB_CUDA(cudaMallocHost(&S->h_stats, 8 * sizeof(unsigned long long)));
+    for (auto& e : S->ev) PSB_CUDA(cudaEventCreate(&e));
+    *out = S.release();
+    return PSB_OK;
+}
+
+int psb_bfs_session_run(psb_bfs_session* s, uint64_t initial, const psb_bfs_opts* opts, uint64_t* counts,
+                        uint32_t cap, uint32_t* n_depths, psb_bfs_stats* stats) {
+    if (!s) return fail(PSB_ERR_ARG, "session is NULL");
+    if (opts && opts->struct_size != sizeof(psb_bfs_opts)) return fail(PSB_ERR_ARG, "psb_bfs_opts.struct_size mismatch");
+    return session_run(s, initial, opts, counts, cap, n_depths, stats);
+}
+
+int psb_bfs_session_destroy(psb_bfs_session* s) {
+    delete s;
+    return PSB_OK;
+}
+
+int psb_bfs(const psb_puzzle* p, int algo, uint64_t initial, const psb_bfs_opts* opts, uint64_t* counts,
+            uint32_t cap, uint32_t* n_depths, psb_bfs_stats* stats) {
+    psb_bfs_session* s = nullptr;
+    if (int rc = psb_bfs_session_create(p, algo, opts, &s)) return rc;
+    std::unique_ptr<psb_bfs_session> guard(s);
+    return session_run(s, initial, opts, counts, cap, n_depths, stats);
+}
+
+}  // extern "C"

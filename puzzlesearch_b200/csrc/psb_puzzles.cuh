@@ -1,0 +1,247 @@
+// psb_puzzles.cuh -- device-side state codecs and expanders for the three
+// puzzles of the reference (lightln2/PuzzleSearch), in the index spaces of its
+// *Simple classes, so that every index, child and operator code is identical
+// to the reference's CPU path.
+//
+//   sliding tile : Puzzles/SlidingTilePuzzleSimple.cpp  (n! permutation index)
+//   pancake      : Puzzles/PancakeSimple.cpp            (n! permutation index, suffix reversal)
+//   4-peg Hanoi  : Puzzles/FourPegHanoiSimple.cpp       (2 bits per disk)
+//
+// Permutation index (Puzzles/PermutationMap.cpp:39-58): position 0 is the
+// most significant digit; digit i equals the number of later values smaller
+// than the value at i; index = sum_i d_i * (n-1-i)!.  Everything is
+// templated on n so all radices and factorial weights are compile-time
+// constants: divisions become multiply-high sequences and the value arrays
+// stay in registers.
+#pragma once
+
+#include <cstdint>
+
+namespace psb {
+
+constexpr uint64_t kInvalidIndex = ~uint64_t(0);  // Common/Puzzle.h:19
+
+__host__ __device__ constexpr uint64_t fact(int k) { return k <= 1 ? 1 : uint64_t(k) * fact(k - 1); }
+constexpr uint32_t kF12 = 479001600u;  // 12!
+
+// Lehmer digits of a permutation index.  Digits with weight < 12! come from
+// the low 32-bit part; the (at most four) top digits of n > 12 from the quotient.
+template <int N>
+__device__ __forceinline__ void perm_digits(uint64_t index, uint32_t (&d)[N]) {
+    uint32_t lo, hi = 0;
+    if constexpr (N <= 12) {
+        lo = uint32_t(index);
+    } else {
+        hi = uint32_t(index / kF12);
+        lo = uint32_t(index - uint64_t(hi) * kF12);
+    }
+#pragma unroll
+    for (int i = N - 1; i >= 0; --i) {
+        const uint32_t radix = uint32_t(N - i);
+        if (N - 1 - i < 12) {
+            d[i] = lo % radix;
+            lo /= radix;
+        } else {
+            d[i] = hi % radix;
+            hi /= radix;
+        }
+    }
+}
+
+// PermutationUncompact (PermutationMap.cpp:21-37): digit k picks the k-th
+// unused value from a nibble list.
+template <int N>
+__device__ __forceinline__ void perm_values(const uint32_t (&d)[N], uint32_t (&v)[N]) {
+    uint64_t tiles = 0xFEDCBA9876543210ull;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const uint32_t s = 4u * d[i];
+        v[i] = uint32_t(tiles >> s) & 15u;
+        const uint64_t lo = tiles & ((uint64_t(1) << s) - 1);
+        const uint64_t hi = ((tiles >> s) >> 4) << s;
+        tiles = hi | lo;
+    }
+}
+
+// PermutationRank via "smaller values to the right" counts.
+template <int N>
+__device__ __forceinline__ uint64_t perm_rank(const uint32_t (&v)[N]) {
+    uint32_t seen = 0, lo = 0, hi = 0;
+#pragma unroll
+    for (int i = N - 1; i >= 0; --i) {
+        const uint32_t dig = __popc(seen & ((1u << v[i]) - 1u));
+        seen |= 1u << v[i];
+        const int w = N - 1 - i;
+        if (w < 12) lo += dig * uint32_t(fact(w));
+        else hi += dig * uint32_t(fact(w) / kF12);
+    }
+    return uint64_t(hi) * kF12 + lo;
+}
+
+// Rank of a nibble-packed permutation (nibble i = value at position i).
+template <int N>
+__device__ __forceinline__ uint64_t perm_rank_packed(uint64_t p) {
+    uint32_t v[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = uint32_t(p >> (4 * i)) & 15u;
+    return perm_rank<N>(v);
+}
+
+// --------------------------------------------------------------------------
+// Pancake (PancakeSimple.cpp:12-20,62-73): operator k reverses the LAST k+2
+// values; the child's operator code is k.  Only the last m = k+2 Lehmer
+// digits change, so child = parent - low_m(parent) + low_m(child), where
+// low_m(child) = sum_{q<m} q! * #(earlier values of the parent suffix that
+// are smaller than the parent value at position n-m+q).
+// --------------------------------------------------------------------------
+template <int N>
+struct Pancake {
+    static constexpr int kBranch = N - 1;
+    static constexpr int kOps = N - 1;
+
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, Emit& emit) {
+        uint32_t d[N], v[N];
+        perm_digits<N>(index, d);
+        perm_values<N>(d, v);
+        uint32_t below[N], bit[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) { bit[i] = 1u << v[i]; below[i] = bit[i] - 1u; }
+        uint64_t low = d[N - 1];  // low_1 = d_{n-1} * 0! (always 0)
+#pragma unroll
+        for (int m = 2; m <= N; ++m) {
+            low += uint64_t(d[N - m]) * fact(m - 1);
+            const int op = m - 2;
+            if (kOpBits && (opbits >> op) & 1u) continue;
+            uint32_t seen = bit[N - m];
+            uint64_t s;
+            if (m <= 12) {  // m is a compile-time constant after unrolling; low_m < m! <= 12! < 2^32
+                uint32_t s32 = 0;
+#pragma unroll
+                for (int q = 1; q < m; ++q) {
+                    s32 += uint32_t(fact(q)) * __popc(seen & below[N - m + q]);
+                    seen |= bit[N - m + q];
+                }
+                s = s32;
+            } else {
+                uint32_t s32 = 0, t = 0;
+#pragma unroll
+                for (int q = 1; q < m; ++q) {
+                    const uint32_t c = __popc(seen & below[N - m + q]);
+                    if (q < 12) s32 += uint32_t(fact(q)) * c;
+                    else t += uint32_t(fact(q) / kF12) * c;
+                    seen |= bit[N - m + q];
+                }
+                s = uint64_t(t) * kF12 + s32;
+            }
+            emit(index - low + s, uint32_t(op));
+        }
+    }
+};
+
+// --------------------------------------------------------------------------
+// Sliding tile (SlidingTilePuzzleSimple.cpp:8,61-99): operators UP=0, LEFT=1,
+// RIGHT=2, DOWN=3; children in the order up, down, left, right; each child
+// carries the operator that moves the blank back.
+// --------------------------------------------------------------------------
+template <int N>
+struct Sliding {
+    static constexpr int kBranch = 4;
+    static constexpr int kOps = 4;
+
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, int width, Emit& emit) {
+        uint32_t d[N], v[N];
+        perm_digits<N>(index, d);
+        perm_values<N>(d, v);
+        uint64_t packed = 0;
+        int blank = 0;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            packed |= uint64_t(v[i]) << (4 * i);
+            if (v[i] == 0) blank = i;
+        }
+        const int col = blank % width;
+        auto child = [&](int t) -> uint64_t {
+            const uint64_t tile = (packed >> (4 * t)) & 15u;
+            const uint64_t p = packed + (tile << (4 * blank)) - (tile << (4 * t));
+            return perm_rank_packed<N>(p);
+        };
+        if (blank >= width && !(kOpBits && (opbits & 1u))) emit(child(blank - width), 3u);
+        if (blank < N - width && !(kOpBits && (opbits & 8u))) emit(child(blank + width), 0u);
+        if (col > 0 && !(kOpBits && (opbits & 2u))) emit(child(blank - 1), 2u);
+        if (col < width - 1 && !(kOpBits && (opbits & 4u))) emit(child(blank + 1), 1u);
+    }
+};
+
+// --------------------------------------------------------------------------
+// Four-peg Towers of Hanoi (FourPegHanoiSimple.cpp:104-124,156-174): disk d
+// (0 = smallest) sits on peg (index >> 2d) & 3.  For each peg pair a<b the
+// smaller of the two top disks moves; the operator bit tested is the source
+// peg and the child's operator is the destination peg.  With symmetry on,
+// pegs 1..3 are relabelled after the move so that their bottom disks are in
+// descending order, using the compare-exchange sequence (2,3),(1,2),(2,3)
+// of FourPegHanoiSimple.cpp:51-69, and the child's operator is the
+// destination's new label.
+// --------------------------------------------------------------------------
+struct Hanoi {
+    static constexpr int kBranch = 6;
+    static constexpr int kOps = 4;
+
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, int disks, bool sym,
+                                                  Emit& emit) {
+        const uint64_t even = disks >= 32 ? 0x5555555555555555ull
+                                          : (0x5555555555555555ull & ((uint64_t(1) << (2 * disks)) - 1));
+        const uint64_t L = index & even, H = (index >> 1) & even;
+        uint64_t m[4];
+        m[0] = ~H & ~L & even;
+        m[1] = ~H & L;
+        m[2] = H & ~L;
+        m[3] = H & L;
+        int top[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) top[p] = m[p] ? __ffsll((long long)m[p]) - 1 : 64;  // even bit position
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+#pragma unroll
+            for (int b = a + 1; b < 4; ++b) {
+                if (top[a] == 64 && top[b] == 64) continue;
+                const bool a_src = top[a] < top[b];
+                const int src = a_src ? a : b, dst = a_src ? b : a;
+                const int pos = a_src ? top[a] : top[b];
+                if (kOpBits && ((opbits >> src) & 1u)) continue;
+                uint64_t child = index ^ (uint64_t(src ^ dst) << pos);
+                uint32_t op = uint32_t(dst);
+                if (sym) {
+                    uint64_t mm[4] = {m[0], m[1], m[2], m[3]};
+                    const uint64_t bitpos = uint64_t(1) << pos;
+                    mm[src] &= ~bitpos;
+                    mm[dst] |= bitpos;
+                    int bottom[4], lab[4] = {0, 1, 2, 3};
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) bottom[p] = mm[p] ? 63 - __clzll((long long)mm[p]) : -1;
+                    // compare-exchange (2,3), (1,2), (2,3): swap when bottom[i] < bottom[j]
+                    auto cx = [&](int i, int j) {
+                        if (bottom[i] < bottom[j]) {
+                            int t = bottom[i]; bottom[i] = bottom[j]; bottom[j] = t;
+                            uint64_t u = mm[i]; mm[i] = mm[j]; mm[j] = u;
+                            t = lab[i]; lab[i] = lab[j]; lab[j] = t;
+                        }
+                    };
+                    cx(2, 3); cx(1, 2); cx(2, 3);
+                    // position k now holds original peg lab[k]: index bits of disks on it = k
+                    const uint64_t nl = mm[1] | mm[3], nh = mm[2] | mm[3];
+                    child = nl | (nh << 1);
+                    uint32_t inv = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) if (lab[k] == dst) inv = uint32_t(k);
+                    op = inv;
+                }
+                emit(child, op);
+            }
+        }
+    }
+};
+
+}  // namespace psb

@@ -1,0 +1,133 @@
+"""CPU tests of the C ABI (include/psb200.h): the library loads, exports every
+declared function, and its host-side logic (puzzle info, Parse, ToString,
+argument checks) matches the oracle.  No kernels are launched."""
+import math
+import os
+import random
+import re
+import subprocess
+
+import pytest
+
+import oracle as O
+import puzzlesearch_b200 as psb
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SPECS = [["sliding", 3, 2], ["sliding", 4, 4], ["sliding", 3, 4], ["sliding", 2, 8], ["sliding", 1, 2],
+         ["pancake", 2, 0], ["pancake", 9, 0], ["pancake", 13, 0], ["pancake", 16, 0],
+         ["hanoi4", 1, 0], ["hanoi4", 7, 1], ["hanoi4", 18, 0], ["hanoi4", 31, 0]]
+
+
+def make(spec):
+    kind, a, b = spec
+    if kind == "sliding":
+        return psb.SlidingTilePuzzleSimple(a, b)
+    if kind == "pancake":
+        return psb.PancakeSimple(a)
+    return psb.FourPegHanoiSimple(a, bool(b))
+
+
+def declared_functions():
+    text = open(os.path.join(REPO, "include", "psb200.h")).read()
+    return sorted(set(re.findall(r"^(?:int|const char\*)\s+(psb_\w+)\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = psb.lib()
+    names = declared_functions()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", psb.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (psb_\w+)", out))
+    assert set(names) <= exported
+
+
+def test_library_is_sm100a():
+    out = subprocess.run(["cuobjdump", "--list-elf", psb.LIB_PATH], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
+
+
+def test_version():
+    assert b"sm_100a" in psb.lib().psb_version()
+
+
+@pytest.mark.parametrize("spec", SPECS, ids=lambda s: f"{s[0]}{s[1]}x{s[2]}")
+def test_info_matches_oracle(spec):
+    p = make(spec)
+    info = O.info(spec)
+    assert p.IndexesCount() == info["indexes"]
+    assert p.OperatorsCount() == info["ops"]
+    assert p.BranchingFactor() == info["branching"]
+    assert p.HasOddLengthCycles() == info["odd_cycles"]
+
+
+@pytest.mark.parametrize("spec", SPECS, ids=lambda s: f"{s[0]}{s[1]}x{s[2]}")
+def test_parse_to_string_match_oracle(spec):
+    p = make(spec)
+    rng = random.Random(11)
+    N = p.IndexesCount()
+    for idx in [0, N - 1] + [rng.randrange(N) for _ in range(200)]:
+        s = p.ToString(idx)
+        assert s == O.to_string(spec, idx)
+        assert p.Parse(s) == idx
+
+
+def test_names():
+    assert psb.SlidingTilePuzzleSimple(3, 4).Name() == "Sliding-Tile simple: 3 x 4"
+    assert psb.PancakeSimple(13).Name() == "Pancake simple, size: 13"
+    assert psb.FourPegHanoiSimple(18).Name() == "Four-Peg Hanoi Towers, size=18; symmetry=0"
+
+
+def test_known_answer_parse(golden):
+    for kat in golden["expand_kats"]:
+        if kat["parent"] is None:
+            continue
+        p = make(kat["puzzle"])
+        idx = p.Parse(kat["parent"])
+        assert p.ToString(idx) == kat["parent"]
+        if kat["parent_index"] is not None:
+            assert idx == kat["parent_index"]
+
+
+def test_argument_errors():
+    with pytest.raises(psb.PsbError) as e:
+        psb.PancakeSimple(17)
+    assert e.value.code == -1
+    with pytest.raises(psb.PsbError):
+        psb.SlidingTilePuzzleSimple(5, 4)
+    with pytest.raises(psb.PsbError):
+        psb.FourPegHanoiSimple(0)
+    p = psb.PancakeSimple(5)
+    with pytest.raises(psb.PsbError):
+        p.Parse("0 1 2 3")          # too short
+    with pytest.raises(psb.PsbError):
+        p.Parse("0 1 2 3 3")        # not a permutation
+    with pytest.raises(psb.PsbError):
+        p.ToString(math.factorial(5))
+    with pytest.raises(psb.PsbError):
+        psb.bfs(psb.PancakeSimple(5), "no_such_algo" if False else 9)
+
+
+def test_frontier_search_rejects_more_than_four_operators():
+    # FourBitArray keeps 4 operator bits per state (InMemoryFrontierSearch.cpp:8-53).
+    with pytest.raises(psb.PsbError) as e:
+        psb.bfs(psb.PancakeSimple(6), "frontier")
+    assert e.value.code in (-5, -7)
+
+
+def test_footprint():
+    assert psb.PancakeSimple(13).footprint("three_bit") >= 3 * math.factorial(13) // 8
+    assert psb.PancakeSimple(14).footprint("two_bit") >= 2 * math.factorial(14) // 8
+    assert psb.FourPegHanoiSimple(18).footprint("two_bit") >= 2 * 4 ** 18 // 8
+    assert psb.PancakeSimple(9).final_words("three_bit") == 3 * ((math.factorial(9) + 63) // 64)
+
+
+def test_no_device_error_without_gpu():
+    if psb.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    with pytest.raises(psb.PsbError) as e:
+        psb.bfs(psb.PancakeSimple(5), "three_bit")
+    assert e.value.code == -7
