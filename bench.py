@@ -39,6 +39,9 @@ WORKLOADS = {
     "sliding3x4-2bit": ("sliding", 3, 4, "two_bit", "3x4 sliding-tile in-memory two-bit BFS, full solve from the solved state"),
     "pancake14-2bit": ("pancake", 14, 0, "two_bit", "14-pancake in-memory two-bit BFS, full solve from the identity"),
     "hanoi18-2bit": ("hanoi4", 18, 0, "two_bit", "18-disk 4-peg Hanoi in-memory two-bit BFS, full solve from all disks on peg 0"),
+    # smaller cases of the same kernels, sized for ncu captures (arrays above L2, a few GB at most)
+    "hanoi15-2bit": ("hanoi4", 15, 0, "two_bit", "15-disk 4-peg Hanoi in-memory two-bit BFS (profiling case)"),
+    "pancake12-3bit": ("pancake", 12, 0, "three_bit", "12-pancake in-memory three-bit BFS (profiling case)"),
 }
 REF_SAMPLE = ("pancake", 11, 0, "three_bit")  # CPU baseline sample (reference InMemoryThreeBitBFS)
 
@@ -168,6 +171,20 @@ def run_reference_arm(args):
     return 0
 
 
+def profile_once(args):
+    """One search with per-level device times (the command ncu wraps)."""
+    import puzzlesearch_b200 as psb
+
+    kind, a, b, algo, desc = WORKLOADS[args.workload]
+    puzzle = {"pancake": lambda: psb.PancakeSimple(a), "sliding": lambda: psb.SlidingTilePuzzleSimple(a, b),
+              "hanoi4": lambda: psb.FourPegHanoiSimple(a, bool(b))}[kind]()
+    r = psb.bfs(puzzle, algo, 0, max_depth=args.max_depth, window_bits=args.window_bits, levels=True)
+    out = {"workload": args.workload, "counts": r["counts"], "level_ms": [round(x, 3) for x in r["level_ms"]],
+           "level_children": r["level_children"], "stats": r["stats"]}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -177,7 +194,12 @@ def main():
     ap.add_argument("--workload", default="pancake13-3bit", choices=sorted(WORKLOADS))
     ap.add_argument("--window-bits", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-once", action="store_true",
+                    help="run ONE search (no warm-up, no e2e, no CPU baseline) and print per-level times; for ncu")
+    ap.add_argument("--max-depth", type=int, default=0, help="with --profile-once: stop after this depth")
     args = ap.parse_args()
+    if args.profile_once:
+        return profile_once(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -108,8 +108,9 @@ typedef struct {
     void* stream;          /* cudaStream_t (NULL = a stream owned by the call) */
     uint64_t* final_words; /* optional host buffer: final arrays in the reference's layout (see psb_final_words) */
     uint64_t final_cap;    /* capacity of final_words in 64-bit words */
-    float* level_ms;       /* optional, counts_cap entries: device ms of each level */
-    uint64_t* level_children; /* optional, counts_cap entries: children generated at each level */
+    float* level_ms;       /* optional, counts_cap entries: entry d = device ms of the level that expanded depth d */
+    uint64_t* level_children; /* optional, counts_cap entries: entry d = children generated from depth d
+                              (two-bit writes one more entry, for its final empty sweep, when it fits) */
 } psb_bfs_opts;
 
 typedef struct {

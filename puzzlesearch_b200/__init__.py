@@ -21,7 +21,7 @@ __all__ = [
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libpsb200.so")
+LIB_PATH = os.environ.get("PSB_LIB") or os.path.join(HERE, "libpsb200.so")
 
 SLIDING, PANCAKE, HANOI4 = 1, 2, 3
 TWO_BIT, THREE_BIT, FRONTIER, CLASSIC = 1, 2, 3, 4

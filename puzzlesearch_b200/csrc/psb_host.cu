@@ -438,12 +438,15 @@ struct psb_bfs_session {
     int n_arr = 0;
     unsigned long long* d_stats = nullptr;
     unsigned long long* h_stats = nullptr;
+    uint8_t* wflags[2] = {nullptr, nullptr};  // active-window flags (1 byte per window), double-buffered
+    uint64_t n_windows = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t bytes = 0;
 
     ~psb_bfs_session() {
         for (auto* a : arr) if (a) cudaFree(a);
         if (d_stats) cudaFree(d_stats);
+        for (auto* f : wflags) if (f) cudaFree(f);
         if (h_stats) cudaFreeHost(h_stats);
         for (auto& e : ev) if (e) cudaEventDestroy(e);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -473,21 +476,24 @@ int layout(const psb_puzzle* p, int algo, uint64_t* words, int* n_arr) {
     return fail(PSB_ERR_ARG, "unknown algorithm %d", algo);
 }
 
+// Window of 2^16 states for the permutation puzzles and 2^17 for Hanoi
+// (window sweeps on B200: 13-pancake three-bit 353 ms at 2^15..2^16 vs 374 ms
+// at 2^17; 18-disk Hanoi two-bit 1.64 s at 2^17 vs 1.76 s at 2^16), smaller
+// for small puzzles so that every SM gets windows.
 int auto_window_bits(const psb_puzzle* p, int algo) {
     int lg = 0;
     while (lg < 63 && (uint64_t(1) << (lg + 1)) <= p->n_states) lg++;
-    int wb = std::max(10, std::min(18, lg - 10));
+    const int cap = p->kind == PSB_HANOI4 ? 17 : 16;
+    int wb = std::max(10, std::min(cap, lg - 10));
     if (algo == PSB_FRONTIER) wb = std::min(wb, 16);  // 4 mark bits per state
     return wb;
 }
 
 size_t smem_bytes(int mode, int wb) {
+    // window marks + one list of a warp chunk's states per warp (see level_kernel)
     const size_t W = size_t(1) << wb;
-    switch (mode) {
-    case psb::kFrontier: return W / 2 + size_t(psb::kThreads) * 64 * 4;
-    case psb::kTwoBit: return W / 8 + size_t(psb::kThreads) * 32 * 2;
-    default: return W / 8 + size_t(psb::kThreads) * 64 * 2;
-    }
+    const size_t warps = size_t(psb::level_threads(mode)) / 32;
+    return psb::mark_bytes(mode, W) + warps * 32 * psb::states_per_unit(mode) * psb::list_entry_bytes(mode);
 }
 
 int set_bit(uint64_t* d_word_base, uint64_t bit, cudaStream_t s) {
@@ -537,14 +543,37 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     default: break;
     }
 
+    // Active-window flags: a level whose frontier is sparse (estimate below
+    // N/64) records every window it marks; the next level then sweeps only
+    // those windows.  Flags are a superset of the windows holding frontier
+    // states, so skipping the others is exact.
+    int flags_valid = -1;          // index of the flag array valid for this level, -1 = sweep every window
+    uint64_t estimate = 1;         // last known frontier size
+    const uint64_t sparse_limit = N / 64;
+    if (S->algo != PSB_FRONTIER) {
+        // Level 0 sweeps only the window of the initial state.
+        static thread_local uint8_t one;
+        one = 1;
+        PSB_CUDA(cudaMemsetAsync(S->wflags[0], 0, S->n_windows, s));
+        PSB_CUDA(cudaMemcpyAsync(S->wflags[0] + (initial >> S->window_bits), &one, 1, cudaMemcpyHostToDevice, s));
+        PSB_CUDA(cudaStreamSynchronize(s));
+        flags_valid = 0;
+    }
+
     std::vector<uint64_t> res;
     double expand_ms = 0, finalize_ms = 0;
     uint64_t expanded = 0, children = 0, local = 0, launches = 0;
     const bool want_final = opts && opts->final_words;
     bool first = true;
+    uint32_t iteration = 0;
     for (;;) {
         if (max_depth && res.size() >= size_t(max_depth) + 1) break;
         PSB_CUDA(cudaMemsetAsync(S->d_stats, 0, 8 * sizeof(unsigned long long), s));
+        const bool produce = estimate < sparse_limit;
+        const int flags_next = flags_valid < 0 ? 0 : 1 - flags_valid;
+        if (produce) PSB_CUDA(cudaMemsetAsync(S->wflags[flags_next], 0, S->n_windows, s));
+        a.wflag_cur = flags_valid >= 0 ? S->wflags[flags_valid] : nullptr;
+        a.wflag_next = produce ? S->wflags[flags_next] : nullptr;
         PSB_CUDA(cudaEventRecord(S->ev[1], s));
         uint64_t count = 0;
         if (S->algo == PSB_FRONTIER && first) {
@@ -588,7 +617,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         expanded += (S->algo == PSB_FRONTIER && first) ? 1 : S->h_stats[0];
         children += S->h_stats[1];
         local += S->h_stats[2];
-        const size_t lvl = res.size();
+        const size_t lvl = size_t(iteration++);  // the depth this level kernel expanded
         if (opts && opts->level_ms && lvl < cap) opts->level_ms[lvl] = t_exp + t_fin;
         if (opts && opts->level_children && lvl < cap) opts->level_children[lvl] = S->h_stats[1];
 
@@ -626,6 +655,8 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             break;
         }
         first = false;
+        flags_valid = produce ? flags_next : -1;
+        estimate = count;
         if (res.size() > cap) return fail(PSB_ERR_CAPACITY, "more than %u depths", cap);
     }
 done:
@@ -660,7 +691,7 @@ done:
     if (stats && stats->struct_size >= sizeof(psb_bfs_stats)) {
         stats->levels = uint32_t(launches);
         stats->window_bits = uint32_t(S->window_bits);
-        stats->threads = uint32_t(psb::kThreads);
+        stats->threads = uint32_t(psb::level_threads(S->mode));
         stats->total_ms = total;
         stats->expand_ms = expand_ms;
         stats->finalize_ms = finalize_ms;
@@ -711,6 +742,11 @@ int psb_bfs_session_create(const psb_puzzle* p, int algo, const psb_bfs_opts* op
     for (int i = 0; i < S->n_arr; i++) {
         PSB_CUDA(cudaMalloc(&S->arr[i], S->words[i] * 8));
         S->bytes += S->words[i] * 8;
+    }
+    S->n_windows = (p->n_states + (uint64_t(1) << S->window_bits) - 1) >> S->window_bits;
+    for (auto& f : S->wflags) {
+        PSB_CUDA(cudaMalloc(&f, S->n_windows));
+        S->bytes += S->n_windows;
     }
     PSB_CUDA(cudaMalloc(&S->d_stats, 8 * sizeof(unsigned long long)));
     PSB_CUDA(cudaMallocHost(&S->h_stats, 8 * sizeof(unsigned long long)));

@@ -30,14 +30,41 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "psb_puzzles.cuh"
 
 namespace psb {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;  // finalize and batched-expand kernels
 
 enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
+
+// Block shape of the level kernel per mode, chosen by a sweep on B200:
+// two-bit reads the target's code before each long-range mark, so it wants
+// more resident warps (four 256-thread blocks per SM); three-bit's marks are
+// fire-and-forget, and it runs fastest without a register cap.
+// PSB_THREADS / PSB_MIN_BLOCKS override every mode (tuning builds only).
+template <int MODE>
+struct Shape {
+#ifdef PSB_THREADS
+    static constexpr int threads = PSB_THREADS;
+#else
+    static constexpr int threads = 256;
+#endif
+#ifdef PSB_MIN_BLOCKS
+    static constexpr int min_blocks = PSB_MIN_BLOCKS;
+#else
+    static constexpr int min_blocks = MODE == kTwoBit ? 4 : MODE == kFrontier ? 2 : 1;
+#endif
+};
+
+__host__ __device__ constexpr int level_threads(int mode) {
+    return mode == kThreeBit ? Shape<kThreeBit>::threads
+         : mode == kClassic  ? Shape<kClassic>::threads
+         : mode == kTwoBit   ? Shape<kTwoBit>::threads
+                             : Shape<kFrontier>::threads;
+}
 
 struct PuzzleArgs {
     int width;  // sliding tile: board width
@@ -86,6 +113,8 @@ struct LevelArgs {
     int odd;                   // frontier search: exclusion bitsets in use
     PuzzleArgs pz;
     unsigned long long* stats;  // [0] frontier states, [1] children, [2] local children, [3] error flag
+    const uint8_t* wflag_cur;   // optional: 1 byte per window, non-zero if the window may hold frontier states
+    uint8_t* wflag_next;        // optional: set for every window that receives a mark this level
 };
 
 constexpr uint64_t kEven = 0x5555555555555555ull;
@@ -122,31 +151,22 @@ __device__ __forceinline__ uint32_t nibble_flags(uint64_t x) {
     return uint32_t(t);
 }
 
-// Block-wide exclusive prefix sum (kThreads threads); also returns the total.
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* s_warp, uint32_t& total) {
-    constexpr int kWarps = kThreads / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t incl = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = lane < kWarps ? s_warp[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < kWarps; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < kWarps) s_warp[lane] = w;
-    }
-    __syncthreads();
-    total = s_warp[kWarps - 1];
-    return (warp ? s_warp[warp - 1] : 0) + incl - x;
+// Shared-memory marks: one bit per state (1-bit modes) or four operator bits
+// per state (frontier search).  PSB_BYTE_MARKS (tuning builds) keeps one byte
+// per state for the 1-bit modes and marks with plain stores instead of atomics.
+#ifdef PSB_BYTE_MARKS
+constexpr bool kByteMarks = true;
+#else
+constexpr bool kByteMarks = false;
+#endif
+
+__host__ __device__ constexpr size_t mark_bytes(int mode, size_t window_states) {
+    return mode == kFrontier ? window_states / 2 : kByteMarks ? window_states : window_states / 8;
 }
+
+// Warp chunk: 32 lanes x one unit each (64 states; 32 for two-bit codes).
+__host__ __device__ constexpr uint32_t states_per_unit(int mode) { return mode == kTwoBit ? 32 : 64; }
+__host__ __device__ constexpr size_t list_entry_bytes(int mode) { return mode == kFrontier ? 4 : 2; }
 
 template <int MODE>
 struct Emitter {
@@ -156,6 +176,8 @@ struct Emitter {
     uint64_t* gmarks;     // global mark array
     uint64_t n_states;
     uint32_t next_pat;    // two-bit: bits of the NEXT code (hi at bit 0, lo at bit 1)
+    uint8_t* wflag_next;  // optional active-window flags of the next level
+    int window_bits;
     uint32_t children = 0, local = 0, bad = 0;
 
     __device__ __forceinline__ void operator()(uint64_t c, uint32_t op) {
@@ -164,72 +186,113 @@ struct Emitter {
         const uint64_t o = c - base;
         if (o < span) {
             ++local;
-            if constexpr (MODE == kFrontier) atomicOr(&smarks[o >> 3], 1u << (4 * (uint32_t(o) & 7u) + op));
-            else atomicOr(&smarks[o >> 5], 1u << (uint32_t(o) & 31u));
+            if constexpr (MODE == kFrontier) {
+                atomicOr(&smarks[o >> 3], 1u << (4 * (uint32_t(o) & 7u) + op));
+            } else if constexpr (kByteMarks) {
+                reinterpret_cast<uint8_t*>(smarks)[o] = 1;
+            } else {
+                atomicOr(&smarks[o >> 5], 1u << (uint32_t(o) & 31u));
+            }
         } else if constexpr (MODE == kFrontier) {
+            if (wflag_next) wflag_next[c >> window_bits] = 1;
             atomicOr(reinterpret_cast<unsigned int*>(gmarks) + (c >> 3), 1u << (4 * (uint32_t(c) & 7u) + op));
         } else if constexpr (MODE == kTwoBit) {
             unsigned long long* w = reinterpret_cast<unsigned long long*>(gmarks) + (c >> 5);
             const uint32_t sh = 2u * (uint32_t(c) & 31u);
             const uint64_t v = __ldcg(reinterpret_cast<const unsigned long long*>(w));
-            if (((v >> sh) & 3u) == 0) atomicOr(w, (unsigned long long)next_pat << sh);  // UNVISITED -> NEXT
+            if (((v >> sh) & 3u) == 0) {  // UNVISITED -> NEXT
+                if (wflag_next) wflag_next[c >> window_bits] = 1;
+                atomicOr(w, (unsigned long long)next_pat << sh);
+            }
         } else {
+            if (wflag_next) wflag_next[c >> window_bits] = 1;
             atomicOr(reinterpret_cast<unsigned int*>(gmarks) + (c >> 5), 1u << (uint32_t(c) & 31u));
         }
     }
 };
 
+// 32 marks held as bytes (0/1) -> 32-bit mask.
+__device__ __forceinline__ uint32_t bytes_to_bits(const uint32_t* b8) {
+    uint32_t r = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r |= (((b8[k] & 0x01010101u) * 0x01020408u) >> 24 & 15u) << (4 * k);
+    return r;
+}
+
 template <class PZ, int MODE>
-__global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs a) {
+__global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks) level_kernel(LevelArgs a) {
+    constexpr int kThreads = Shape<MODE>::threads;
+    constexpr int kWarps = kThreads / 32;
+    constexpr uint32_t kSPU = states_per_unit(MODE);
+    constexpr uint32_t kChunk = 32 * kSPU;           // states per warp chunk
+    constexpr int kWPU = MODE == kFrontier ? 4 : 1;  // 64-bit frontier words per unit
     extern __shared__ __align__(16) unsigned long long smem64[];
-    __shared__ uint32_t s_warp[kThreads / 32];
-    const int tid = threadIdx.x;
+    __shared__ uint32_t s_any;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t W = 1u << a.window_bits;
     const uint64_t base = uint64_t(blockIdx.x) << a.window_bits;
     if (base >= a.n_states) return;
+    if (a.wflag_cur && !a.wflag_cur[blockIdx.x]) return;  // no frontier state can be in this window
     const uint64_t remaining = a.n_states - base;
     const uint32_t span = remaining < W ? uint32_t(remaining) : W;
-    constexpr uint32_t kSPU = MODE == kTwoBit ? 32 : 64;  // states per thread unit
     const uint32_t units = (span + kSPU - 1) / kSPU;
-    constexpr uint32_t kMarkBits = MODE == kFrontier ? 4 : 1;
-    const uint32_t mark_u32 = (W * kMarkBits) / 32;
+    const uint32_t chunks = (units + 31) / 32;
+    const uint32_t mbytes = uint32_t(mark_bytes(MODE, W));
     uint32_t* smarks = reinterpret_cast<uint32_t*>(smem64);
-    uint16_t* list16 = reinterpret_cast<uint16_t*>(smarks + mark_u32);
-    uint32_t* list32 = smarks + mark_u32;
+    using Entry = typename std::conditional<MODE == kFrontier, uint32_t, uint16_t>::type;
+    Entry* wlist = reinterpret_cast<Entry*>(reinterpret_cast<char*>(smem64) + mbytes) + size_t(warp) * kChunk;
 
-    for (uint32_t i = tid; i < mark_u32; i += kThreads) smarks[i] = 0;
+    for (uint32_t i = tid; i < mbytes / 16; i += kThreads) reinterpret_cast<uint4*>(smem64)[i] = make_uint4(0, 0, 0, 0);
+    if (tid == 0) s_any = 0;
     __syncthreads();
 
-    Emitter<MODE> em{base, W, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u)};
+    Emitter<MODE> em{base, W, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u), a.wflag_next,
+                     a.window_bits};
     uint32_t found = 0;
 
-    for (uint32_t u0 = 0; u0 < units; u0 += kThreads) {
-        const uint32_t u = u0 + tid;
+    // Each warp walks its chunks (warp, warp + kWarps, ...) on its own: lane
+    // l sweeps unit 32*chunk + l, the warp compacts the frontier states into
+    // its shared-memory list with a shuffle scan and expands them, while the
+    // next chunk's words are already in flight.  No block barrier until the flush.
+    auto load = [&](uint32_t ch, uint64_t (&w)[kWPU]) {
+        const uint32_t u = ch * 32 + uint32_t(lane);
+#pragma unroll
+        for (int q = 0; q < kWPU; ++q) {
+            const uint64_t wi = MODE == kFrontier ? (base >> 4) + 4ull * u + q
+                              : MODE == kTwoBit   ? (base >> 5) + u
+                                                  : (base >> 6) + u;
+            w[q] = (ch < chunks && u < units && wi < a.front_words) ? a.front[wi] : 0;
+        }
+    };
+    uint64_t cw[kWPU], nw[kWPU];
+    uint32_t ch = uint32_t(warp);
+    load(ch, cw);
+    while (ch < chunks) {  // uniform within the warp
+        const uint32_t nch = ch + kWarps;
+        load(nch, nw);
+        const uint32_t u = ch * 32 + uint32_t(lane);
         uint64_t pmask = 0;
-        uint64_t nib0 = 0, nib1 = 0, nib2 = 0, nib3 = 0;
         if (u < units) {
             if constexpr (MODE == kThreeBit) {
-                pmask = a.front[(base >> 6) + u];
+                pmask = cw[0];
             } else if constexpr (MODE == kClassic) {
-                uint64_t* p = a.front + (base >> 6) + u;
-                pmask = *p;
-                if (pmask) *p = 0;  // BitArray::ScanBitsAndClear
+                pmask = cw[0];
+                if (pmask) a.front[(base >> 6) + u] = 0;  // BitArray::ScanBitsAndClear
             } else if constexpr (MODE == kTwoBit) {
-                unsigned long long* p = reinterpret_cast<unsigned long long*>(a.front) + (base >> 5) + u;
-                const uint64_t w = *p;
+                const uint64_t w = cw[0];
                 const uint64_t hi = w & kEven, lo = (w >> 1) & kEven;
                 const uint64_t cur = hi & (a.cur_code == 3 ? lo : ~lo);
-                if (cur) atomicXor(p, (unsigned long long)(cur | (a.cur_code == 2 ? (cur << 1) : 0)));  // CUR -> OLD (1)
+                if (cur)  // CUR -> OLD (code 1); only this block changes this window's CUR codes
+                    atomicXor(reinterpret_cast<unsigned long long*>(a.front) + (base >> 5) + u,
+                              (unsigned long long)(cur | (a.cur_code == 2 ? (cur << 1) : 0)));
                 pmask = gather_even(cur);
             } else {
                 const uint64_t w0 = (base >> 4) + 4ull * u;
-                uint64_t* p = a.front + w0;
-                if (w0 + 0 < a.front_words) { nib0 = p[0]; if (nib0) p[0] = 0; }
-                if (w0 + 1 < a.front_words) { nib1 = p[1]; if (nib1) p[1] = 0; }
-                if (w0 + 2 < a.front_words) { nib2 = p[2]; if (nib2) p[2] = 0; }
-                if (w0 + 3 < a.front_words) { nib3 = p[3]; if (nib3) p[3] = 0; }
-                pmask = uint64_t(nibble_flags(nib0)) | (uint64_t(nibble_flags(nib1)) << 16) |
-                        (uint64_t(nibble_flags(nib2)) << 32) | (uint64_t(nibble_flags(nib3)) << 48);
+#pragma unroll
+                for (int q = 0; q < kWPU; ++q) {
+                    if (cw[q]) a.front[w0 + q] = 0;  // FourBitArray::ScanAndClear
+                    pmask |= uint64_t(nibble_flags(cw[q])) << (16 * q);
+                }
                 if (a.odd) {
                     const uint64_t ex = a.excl_cur[(base >> 6) + u];
                     pmask &= ~ex;
@@ -239,60 +302,82 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs a) {
         }
         const uint32_t cnt = __popcll(pmask);
         found += cnt;
-        uint32_t total;
-        uint32_t off = block_exclusive_scan(cnt, s_warp, total);
-        const uint32_t ub = uint32_t(tid) * kSPU;
-        while (pmask) {
-            const uint32_t j = __ffsll((long long)pmask) - 1;
-            pmask &= pmask - 1;
-            if constexpr (MODE == kFrontier) {
-                const uint64_t nw = j < 16 ? nib0 : j < 32 ? nib1 : j < 48 ? nib2 : nib3;
-                const uint32_t bits = uint32_t(nw >> (4 * (j & 15))) & 15u;
-                list32[off++] = (ub + j) | (bits << 16);
-            } else {
-                list16[off++] = uint16_t(ub + j);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        if (total) {
+            uint32_t off = incl - cnt;
+            const uint32_t ub = uint32_t(lane) * kSPU;
+            while (pmask) {
+                const uint32_t j = __ffsll((long long)pmask) - 1;
+                pmask &= pmask - 1;
+                if constexpr (MODE == kFrontier) {
+                    const uint64_t word = j < 16 ? cw[0 % kWPU] : j < 32 ? cw[1 % kWPU] : j < 48 ? cw[2 % kWPU] : cw[3 % kWPU];
+                    const uint32_t bits = uint32_t(word >> (4 * (j & 15))) & 15u;
+                    wlist[off++] = Entry((ub + j) | (bits << 16));
+                } else {
+                    wlist[off++] = Entry(ub + j);
+                }
+            }
+            __syncwarp();
+            const uint64_t cbase = base + uint64_t(ch) * kChunk;
+            for (uint32_t e = uint32_t(lane); e < total; e += 32) {
+                if constexpr (MODE == kFrontier) {
+                    const uint32_t v = wlist[e];
+                    PZ::template expand<true>(cbase + (v & 0xFFFFu), v >> 16, a.pz, em);
+                } else {
+                    PZ::template expand<false>(cbase + wlist[e], 0u, a.pz, em);
+                }
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int q = 0; q < kWPU; ++q) cw[q] = nw[q];
+        ch = nch;
+    }
+    if (found) s_any = 1;
+    __syncthreads();
+
+    // Flush the window's shared-memory marks (only if it had frontier states).
+    if (s_any) {
+        if (a.wflag_next && tid == 0) a.wflag_next[blockIdx.x] = 1;
+        if constexpr (MODE == kTwoBit) {
+            const uint32_t next_pat = em.next_pat;
+            unsigned long long* codes = reinterpret_cast<unsigned long long*>(a.marks) + (base >> 5);
+            for (uint32_t i = tid; i < W / 32; i += kThreads) {
+                const uint32_t v = kByteMarks ? bytes_to_bits(smarks + 8 * i) : smarks[i];
+                if (!v || (base >> 5) + i >= a.mark_words) continue;
+                const uint64_t w = __ldcg(codes + i);
+                const uint64_t unvisited = ~(w | (w >> 1)) & kEven;
+                const uint64_t m = spread_even(v) & unvisited;
+                if (m) atomicOr(codes + i, (unsigned long long)(m | ((next_pat & 2u) ? (m << 1) : 0)));
+            }
+        } else {
+            constexpr uint32_t kShift = MODE == kFrontier ? 4 : 6;  // states per 64-bit word: 16 or 64
+            unsigned long long* g = reinterpret_cast<unsigned long long*>(a.marks) + (base >> kShift);
+            const uint32_t words = MODE == kFrontier ? W / 16 : W / 64;
+            for (uint32_t i = tid; i < words; i += kThreads) {
+                unsigned long long v;
+                if constexpr (MODE != kFrontier && kByteMarks)
+                    v = (unsigned long long)bytes_to_bits(smarks + 16 * i) |
+                        ((unsigned long long)bytes_to_bits(smarks + 16 * i + 8) << 32);
+                else
+                    v = smem64[i];
+                if (v && (base >> kShift) + i < a.mark_words) atomicOr(g + i, v);
             }
         }
-        __syncthreads();
-        const uint64_t batch_base = base + uint64_t(u0) * kSPU;
-        for (uint32_t k = tid; k < total; k += kThreads) {
-            if constexpr (MODE == kFrontier) {
-                const uint32_t e = list32[k];
-                PZ::template expand<true>(batch_base + (e & 0xFFFFu), e >> 16, a.pz, em);
-            } else {
-                PZ::template expand<false>(batch_base + list16[k], 0u, a.pz, em);
-            }
-        }
-        __syncthreads();
     }
 
-    // Flush the window's shared-memory marks.
-    if constexpr (MODE == kTwoBit) {
-        const uint32_t next_pat = em.next_pat;
-        unsigned long long* codes = reinterpret_cast<unsigned long long*>(a.marks) + (base >> 5);
-        for (uint32_t i = tid; i < mark_u32; i += kThreads) {
-            const uint32_t v = smarks[i];
-            if (!v || (base >> 5) + i >= a.mark_words) continue;
-            const uint64_t w = __ldcg(codes + i);
-            const uint64_t unvisited = ~(w | (w >> 1)) & kEven;
-            const uint64_t m = spread_even(v) & unvisited;
-            if (m) atomicOr(codes + i, (unsigned long long)(m | ((next_pat & 2u) ? (m << 1) : 0)));
-        }
-    } else {
-        constexpr uint32_t kShift = MODE == kFrontier ? 4 : 6;  // states per 64-bit word: 16 or 64
-        unsigned long long* g = reinterpret_cast<unsigned long long*>(a.marks) + (base >> kShift);
-        for (uint32_t i = tid; i < mark_u32 / 2; i += kThreads) {
-            const unsigned long long v = smem64[i];
-            if (v && (base >> kShift) + i < a.mark_words) atomicOr(g + i, v);
-        }
-    }
-
-    // Counters: one atomic per block and counter.
+    // Counters: one atomic per warp and counter.
     uint32_t c0 = __reduce_add_sync(0xFFFFFFFFu, found);
     uint32_t c1 = __reduce_add_sync(0xFFFFFFFFu, em.children);
     uint32_t c2 = __reduce_add_sync(0xFFFFFFFFu, em.local);
     uint32_t c3 = __reduce_or_sync(0xFFFFFFFFu, em.bad);
-    if ((tid & 31) == 0) {
+    if (lane == 0) {
         if (c0) atomicAdd(&a.stats[0], (unsigned long long)c0);
         if (c1) atomicAdd(&a.stats[1], (unsigned long long)c1);
         if (c2) atomicAdd(&a.stats[2], (unsigned long long)c2);
@@ -305,7 +390,7 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs a) {
 template <class PZ>
 __global__ void seed_kernel(LevelArgs a, uint64_t initial) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Emitter<kFrontier> em{~uint64_t(0), 0, nullptr, a.marks, a.n_states, 0};
+    Emitter<kFrontier> em{~uint64_t(0), 0, nullptr, a.marks, a.n_states, 0, a.wflag_next, a.window_bits};
     PZ::template expand<true>(initial, 0u, a.pz, em);
     if (a.odd) a.excl_next[initial >> 6] |= 1ull << (initial & 63);
     a.stats[1] += em.children;
@@ -375,7 +460,7 @@ cudaError_t launch_level(const LevelArgs& a, unsigned grid, size_t smem, cudaStr
     cudaError_t e = cudaFuncSetAttribute(level_kernel<PZ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(smem));
     if (e != cudaSuccess) return e;
-    level_kernel<PZ, MODE><<<grid, kThreads, smem, s>>>(a);
+    level_kernel<PZ, MODE><<<grid, Shape<MODE>::threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 

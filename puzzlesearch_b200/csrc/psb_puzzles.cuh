@@ -214,10 +214,10 @@ struct Hanoi {
                 uint64_t child = index ^ (uint64_t(src ^ dst) << pos);
                 uint32_t op = uint32_t(dst);
                 if (sym) {
-                    uint64_t mm[4] = {m[0], m[1], m[2], m[3]};
                     const uint64_t bitpos = uint64_t(1) << pos;
-                    mm[src] &= ~bitpos;
-                    mm[dst] |= bitpos;
+                    uint64_t mm[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) mm[q] = m[q] ^ ((q == src || q == dst) ? bitpos : 0);
                     int bottom[4], lab[4] = {0, 1, 2, 3};
 #pragma unroll
                     for (int p = 0; p < 4; ++p) bottom[p] = mm[p] ? 63 - __clzll((long long)mm[p]) : -1;
