@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks)
     constexpr int kWPU = MODE == kFrontier ? 4 : 1;  // 64-bit frontier words per unit
     extern __shared__ __align__(16) unsigned long long smem64[];
     __shared__ uint32_t s_any;
+    __shared__ uint32_t s_next_chunk;  // chunks are handed out dynamically so warps finish together
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t W = 1u << a.window_bits;
     const uint64_t base = uint64_t(blockIdx.x) << a.window_bits;
@@ -243,17 +244,21 @@ __global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks)
     Entry* wlist = reinterpret_cast<Entry*>(reinterpret_cast<char*>(smem64) + mbytes) + size_t(warp) * kChunk;
 
     for (uint32_t i = tid; i < mbytes / 16; i += kThreads) reinterpret_cast<uint4*>(smem64)[i] = make_uint4(0, 0, 0, 0);
-    if (tid == 0) s_any = 0;
+    if (tid == 0) {
+        s_any = 0;
+        s_next_chunk = kWarps;  // chunks 0 .. kWarps-1 go to warps 0 .. kWarps-1
+    }
     __syncthreads();
 
     Emitter<MODE> em{base, W, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u), a.wflag_next,
                      a.window_bits};
     uint32_t found = 0;
 
-    // Each warp walks its chunks (warp, warp + kWarps, ...) on its own: lane
-    // l sweeps unit 32*chunk + l, the warp compacts the frontier states into
-    // its shared-memory list with a shuffle scan and expands them, while the
-    // next chunk's words are already in flight.  No block barrier until the flush.
+    // Each warp takes chunks on its own (its first chunk is its warp index,
+    // later ones come from a shared counter): lane l sweeps unit 32*chunk + l,
+    // the warp compacts the frontier states into its shared-memory list with a
+    // shuffle scan and expands them, while the next chunk's words are already
+    // in flight.  No block barrier until the flush.
     auto load = [&](uint32_t ch, uint64_t (&w)[kWPU]) {
         const uint32_t u = ch * 32 + uint32_t(lane);
 #pragma unroll
@@ -268,7 +273,9 @@ __global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks)
     uint32_t ch = uint32_t(warp);
     load(ch, cw);
     while (ch < chunks) {  // uniform within the warp
-        const uint32_t nch = ch + kWarps;
+        uint32_t nch = 0;
+        if (lane == 0) nch = atomicAdd(&s_next_chunk, 1u);
+        nch = __shfl_sync(0xFFFFFFFFu, nch, 0);
         load(nch, nw);
         const uint32_t u = ch * 32 + uint32_t(lane);
         uint64_t pmask = 0;

@@ -1,0 +1,67 @@
+"""The C++ adapter (include/psb200.hpp) used the way the reference's own tests
+use its classes: PuzzleSearchTests-style searches and Pancake/Hanoi Expand
+known-answer tests, through tests/cpp/psb200_driver.cpp."""
+import os
+import subprocess
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(REPO, "tests", "cpp", "psb200_driver")
+
+
+def build_driver():
+    src = os.path.join(REPO, "tests", "cpp", "psb200_driver.cpp")
+    if os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(
+            os.path.getmtime(src), os.path.getmtime(os.path.join(REPO, "include", "psb200.hpp"))):
+        return DRIVER
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I" + os.path.join(REPO, "include"), src, "-o", DRIVER,
+                           "-L" + os.path.join(REPO, "puzzlesearch_b200"), "-lpsb200",
+                           "-Wl,-rpath,$ORIGIN/../../puzzlesearch_b200"])
+    return DRIVER
+
+
+def run(lines):
+    out = subprocess.run([build_driver()], input="\n".join(lines) + "\n", capture_output=True, text=True,
+                         timeout=600, check=True).stdout
+    return out.strip().split("\n")
+
+
+def test_driver_compiles():
+    assert os.path.exists(build_driver())
+
+
+@pytest.mark.gpu
+def test_search_vectors_through_adapter(golden):
+    cases = []
+    for v in golden["search"]:
+        kind, a, b = v["puzzle"]
+        if not v["full"] or (kind == "sliding" and a * b > 10):
+            continue
+        algos = ["classic", "two_bit", "three_bit"] + (["frontier"] if kind != "pancake" else [])
+        for algo in algos:
+            cases.append((f"bfs {kind} {a} {b} {algo} {v['start'] or ''}".rstrip(), v["counts"]))
+    got = run([c for c, _ in cases])
+    assert len(got) == len(cases)
+    for (cmd, exp), line in zip(cases, got):
+        assert [int(x) for x in line.split()] == exp, cmd
+
+
+@pytest.mark.gpu
+def test_expand_known_answers_through_adapter(golden):
+    kats = [k for k in golden["expand_kats"] if k["puzzle"][0] != "sliding"]
+    cmds = [f"expand {k['puzzle'][0]} {k['puzzle'][1]} {k['puzzle'][2]} {k['parent'] or ''}".rstrip() for k in kats]
+    got = run(cmds)
+    for k, line in zip(kats, got):
+        items = [x.split("|") for x in line.split(";")]
+        states = [s for s, _ in items]
+        assert states[:len(k["children"])] == k["children"], k["test"]
+        for (s, op), e in zip(items, k["ops"]):
+            if e is not None:
+                assert int(op) == e, k["test"]
+
+
+@pytest.mark.gpu
+def test_error_path_through_adapter():
+    got = run(["bfs pancake 6 0 frontier"])
+    assert got[0].startswith("ERROR -5")
