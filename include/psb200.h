@@ -154,6 +154,25 @@ int psb_bfs_session_run(psb_bfs_session* s, uint64_t initial_index, const psb_bf
                         uint64_t* depth_counts, uint32_t counts_cap, uint32_t* n_depths, psb_bfs_stats* stats);
 int psb_bfs_session_destroy(psb_bfs_session* s);
 
+/* --- Search without device allocation --------------------------------------
+ * No counterpart in the reference.  For callers that may not call cudaMalloc
+ * (all device memory is owned by another allocator or a pre-reserved arena):
+ * the same search as psb_bfs, but the caller passes the bit arrays in
+ * d_arrays (device memory of at least psb_bfs_footprint() bytes, given in
+ * 64-bit words as d_array_words) and the function allocates nothing: no
+ * cudaMalloc/cudaFree, no pinned host memory, no stream or event.  Its few
+ * bytes of scratch (level counters and active-window flags) sit in a static
+ * device array of 4 MiB + 256 bytes that every GPU loading the library holds
+ * until exit; searches needing more than 2^21 windows (more than ~1.4e11
+ * states) return PSB_ERR_CAPACITY.  All calls share that array: calls whose
+ * GPU work overlaps race, so run them one after the other.  The first call on
+ * a device looks the array's address up; make it before any stream capture.
+ * For PSB_TWO_BIT the final code array is d_arrays[0 .. ceil(2N/64)) on
+ * return, in the reference's layout. */
+int psb_bfs_noalloc(const psb_puzzle* p, int algo, uint64_t initial_index, uint64_t* d_arrays,
+                    uint64_t d_array_words, uint32_t max_depth, void* stream, uint64_t* depth_counts,
+                    uint32_t counts_cap, uint32_t* n_depths);
+
 #ifdef __cplusplus
 }
 #endif

@@ -89,6 +89,8 @@ def lib():
         L.psb_bfs_session_run.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(BfsOpts), u64p, ctypes.c_uint32,
                                           u32p, ctypes.POINTER(BfsStats)]
         L.psb_bfs_session_destroy.argtypes = [P]
+        L.psb_bfs_noalloc.argtypes = [P, ctypes.c_int, ctypes.c_uint64, u64p, ctypes.c_uint64, ctypes.c_uint32,
+                                      ctypes.c_void_p, u64p, ctypes.c_uint32, u32p]
         _lib = L
     return _lib
 

@@ -14,20 +14,13 @@
 #include <vector>
 
 #include "../../include/psb200.h"
+#include "psb_internal.h"
 #include "psb_kernels.cuh"
 
 using psb::LevelArgs;
 using psb::PuzzleArgs;
 using psb::PuzzleKernels;
 
-struct psb_puzzle {
-    int kind, a, b;
-    int cells;  // permutation size (sliding, pancake)
-    uint64_t n_states;
-    int ops, branching, odd;
-    PuzzleKernels k;
-    PuzzleArgs pz;
-};
 
 namespace psb {
 
@@ -214,6 +207,8 @@ uint64_t words_for(uint64_t bits) { return (bits + 63) / 64; }
 uint64_t padded(uint64_t words) { return (words + 31) / 32 * 32; }  // 256-byte multiples for 128-bit sweeps
 
 }  // namespace
+
+int psb_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
 extern "C" {
 

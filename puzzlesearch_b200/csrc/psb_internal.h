@@ -1,0 +1,30 @@
+// psb_internal.h -- definitions shared by the host-side translation units of
+// libpsb200 (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "psb_kernels.cuh"
+
+struct psb_puzzle {
+    int kind, a, b;
+    int cells;  // permutation size (sliding, pancake)
+    uint64_t n_states;
+    int ops, branching, odd;
+    psb::PuzzleKernels k;
+    psb::PuzzleArgs pz;
+};
+
+// Records the calling thread's last error for psb_last_error(); returns code.
+int psb_set_error(int code, const char* msg);
+
+namespace psb {
+// Level-end kernels, defined in psb_host.cu.
+__global__ void finalize_three_bit(const ulonglong2* __restrict__ cur, ulonglong2* __restrict__ nw,
+                                   ulonglong2* __restrict__ old, uint64_t n2, int odd, int zero_old,
+                                   unsigned long long* count);
+__global__ void finalize_classic(ulonglong2* __restrict__ nw, ulonglong2* __restrict__ closed, uint64_t n2,
+                                 unsigned long long* count);
+}  // namespace psb
