@@ -154,6 +154,41 @@ int psb_bfs_session_run(psb_bfs_session* s, uint64_t initial_index, const psb_bf
                         uint64_t* depth_counts, uint32_t counts_cap, uint32_t* n_depths, psb_bfs_stats* stats);
 int psb_bfs_session_destroy(psb_bfs_session* s);
 
+/* --- Frontier compression (Common/FrontierCompression.cpp, StreamVInt.cpp,
+ *     CompressedFrontier.cpp) -------------------------------------------------
+ * A segment's frontier -- the set bits of a bitmap range of at most 2^32
+ * states, as ascending u32 offsets -- in the reference's segment stream:
+ * blocks of up to 262,144 offsets (StreamVInt::MAX_INDEXES_COUNT), each
+ * FrontierCompression::Encode'd (bitmap block when count > 128 and it is
+ * smaller than 10 bits per offset, else StreamVInt), concatenated as
+ * CompressedSegmentWriter does (Common/CompressedFrontier.cpp:103-140).
+ * The stream bytes are identical to the reference's. */
+typedef struct {
+    uint64_t offset;    /* byte offset of the block in the stream */
+    uint32_t count;     /* offsets in the block */
+    uint32_t bytes;     /* encoded size */
+    uint32_t first;     /* first offset (bitmap blocks; first delta for StreamVInt) */
+    uint32_t is_bitmap;
+} psb_codec_block;
+
+/* Encodes the set bits of d_bits[first_bit .. first_bit + n_bits) (device
+ * memory; first_bit a multiple of 64; n_bits <= 2^32) into d_out (device).
+ * *out_bytes receives the stream size; if d_out is NULL or out_cap is too
+ * small the call returns PSB_ERR_CAPACITY with *out_bytes set (ask, then
+ * encode).  blocks (host, optional) receives the block table used by
+ * psb_frontier_decode. */
+int psb_frontier_encode(const uint64_t* d_bits, uint64_t first_bit, uint64_t n_bits, uint8_t* d_out,
+                        uint64_t out_cap, uint64_t* out_bytes, psb_codec_block* blocks, uint32_t blocks_cap,
+                        uint32_t* n_blocks, void* stream);
+/* Builds the block table of a stream held in host memory (the reference's
+ * own streams included): walks the block headers and StreamVInt descriptors. */
+int psb_frontier_index(const uint8_t* stream, uint64_t stream_bytes, psb_codec_block* blocks, uint32_t cap,
+                       uint32_t* n_blocks);
+/* ORs the offsets of a device-resident stream into d_bits[first_bit ..
+ * first_bit + n_bits) (bit first_bit + offset); blocks is the host table. */
+int psb_frontier_decode(const uint8_t* d_stream, const psb_codec_block* blocks, uint32_t n_blocks,
+                        uint64_t* d_bits, uint64_t first_bit, uint64_t n_bits, void* stream);
+
 /* --- Search without device allocation --------------------------------------
  * No counterpart in the reference.  For callers that may not call cudaMalloc
  * (all device memory is owned by another allocator or a pre-reserved arena):

@@ -289,3 +289,23 @@ def ref_svi_encode_bounds(values, bounds):
     out = (ctypes.c_uint8 * cap)()
     k = ref().ref_svi_encode_bounds(n, idx, bd, out, cap)
     return bytes(out[:k])
+
+
+def segment_stream(offsets):
+    """The reference's segment stream for ascending u32 offsets: blocks of
+    262,144 FrontierCompression::Encode'd and concatenated
+    (Common/CompressedFrontier.cpp:103-140).  offsets: numpy uint32 array."""
+    import numpy as np
+    out = []
+    B = 256 * 1024
+    for s in range(0, len(offsets), B):
+        blk = np.ascontiguousarray(offsets[s:s + B], dtype=np.uint32)
+        n = len(blk)
+        idx = np.zeros((n + 7) // 8 * 8 + 8, dtype=np.uint32)
+        idx[:n] = blk
+        span = int(blk[-1]) - int(blk[0])
+        cap = 17 * ((n + 7) // 8 * 2) + 64 + span // 8 + 64
+        buf = (ctypes.c_uint8 * cap)()
+        k = lib().orc_fc_encode(n, idx.ctypes.data_as(u32p), buf)
+        out.append(bytes(buf[:k]))
+    return b"".join(out)

@@ -58,6 +58,12 @@ class BfsStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}
 
 
+class CodecBlock(ctypes.Structure):
+    """psb_codec_block: one block of a compressed frontier stream."""
+    _fields_ = [("offset", ctypes.c_uint64), ("count", ctypes.c_uint32), ("bytes", ctypes.c_uint32),
+                ("first", ctypes.c_uint32), ("is_bitmap", ctypes.c_uint32)]
+
+
 _lib = None
 
 
@@ -89,6 +95,12 @@ def lib():
         L.psb_bfs_session_run.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(BfsOpts), u64p, ctypes.c_uint32,
                                           u32p, ctypes.POINTER(BfsStats)]
         L.psb_bfs_session_destroy.argtypes = [P]
+        L.psb_frontier_encode.argtypes = [u64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
+                                          u64p, ctypes.POINTER(CodecBlock), ctypes.c_uint32, u32p, ctypes.c_void_p]
+        L.psb_frontier_index.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(CodecBlock),
+                                         ctypes.c_uint32, u32p]
+        L.psb_frontier_decode.argtypes = [ctypes.c_void_p, ctypes.POINTER(CodecBlock), ctypes.c_uint32, u64p,
+                                          ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
         L.psb_bfs_noalloc.argtypes = [P, ctypes.c_int, ctypes.c_uint64, u64p, ctypes.c_uint64, ctypes.c_uint32,
                                       ctypes.c_void_p, u64p, ctypes.c_uint32, u32p]
         _lib = L
@@ -302,6 +314,38 @@ class BfsSession:
     def __del__(self):
         if _lib is not None:
             self.close()
+
+
+def frontier_index(data):
+    """Block table of a compressed frontier stream held in host memory (bytes)."""
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    n = ctypes.c_uint32()
+    _check(lib().psb_frontier_index(buf, len(data), None, 0, ctypes.byref(n)))
+    blocks = (CodecBlock * max(n.value, 1))()
+    _check(lib().psb_frontier_index(buf, len(data), blocks, n.value, ctypes.byref(n)))
+    return blocks, n.value
+
+
+def frontier_encode(d_bits, first_bit, n_bits, d_out=None, out_cap=0, stream=None):
+    """Encodes a device bitmap range (device pointers as ints).  Returns
+    (stream_bytes, block_table, n_blocks); with d_out=None only sizes it."""
+    nbytes = ctypes.c_uint64()
+    nb = ctypes.c_uint32()
+    rc = lib().psb_frontier_encode(ctypes.cast(d_bits, u64p), first_bit, n_bits, d_out, out_cap,
+                                   ctypes.byref(nbytes), None, 0, ctypes.byref(nb), stream)
+    if d_out is None:
+        if rc not in (0, -4):
+            _check(rc)
+        return nbytes.value, None, nb.value
+    blocks = (CodecBlock * max(nb.value, 1))()
+    _check(lib().psb_frontier_encode(ctypes.cast(d_bits, u64p), first_bit, n_bits, d_out, out_cap,
+                                     ctypes.byref(nbytes), blocks, nb.value, ctypes.byref(nb), stream))
+    return nbytes.value, blocks, nb.value
+
+
+def frontier_decode(d_stream, blocks, n_blocks, d_bits, first_bit, n_bits, stream=None):
+    _check(lib().psb_frontier_decode(d_stream, blocks, n_blocks, ctypes.cast(d_bits, u64p), first_bit, n_bits,
+                                     stream))
 
 
 def _run(puzzle, algo, initialState):
