@@ -171,6 +171,85 @@ def run_reference_arm(args):
     return 0
 
 
+BATCH_TYPES = [("sliding", 2, 3), ("sliding", 2, 4), ("sliding", 3, 3), ("sliding", 2, 5),
+               ("pancake", 7, 0), ("pancake", 8, 0), ("pancake", 9, 0), ("pancake", 10, 0), ("pancake", 11, 0)]
+
+
+def _make(psb, kind, a, b):
+    return {"pancake": lambda: psb.PancakeSimple(a), "sliding": lambda: psb.SlidingTilePuzzleSimple(a, b),
+            "hanoi4": lambda: psb.FourPegHanoiSimple(a, bool(b))}[kind]()
+
+
+def solvable_start(rng, kind, a, b, puzzle):
+    """Uniformly random start in the start state's component: any permutation
+    for pancake; for the sliding tile, permutation parity must equal the
+    parity of the blank's taxicab distance from cell 0."""
+    if kind != "sliding":
+        return rng.randrange(puzzle.IndexesCount())
+    while True:
+        p = list(range(a * b))
+        rng.shuffle(p)
+        inv = sum(1 for i in range(len(p)) for j in range(i + 1, len(p)) if p[i] > p[j])
+        z = p.index(0)
+        if inv % 2 == (z // a + z % a) % 2:
+            return puzzle.Parse(" ".join(map(str, p)))
+
+
+def batch_bench(args):
+    """4096 independent two-bit searches drawn from a seed,
+    uniform over sliding 2x3/2x4/3x3/2x5 and pancake 7..11, from random
+    solvable starts; batched engine vs one search per launch, counts equal."""
+    import random
+
+    import puzzlesearch_b200 as psb
+    rng = random.Random(4096)
+    puzzles = {t: _make(psb, *t) for t in BATCH_TYPES}
+    items = []
+    for i in range(args.instances):
+        t = BATCH_TYPES[rng.randrange(len(BATCH_TYPES))]
+        items.append((i, t, solvable_start(rng, *t, puzzles[t])))
+    total_states = sum(puzzles[t].IndexesCount() // (2 if t[0] == "sliding" else 1) for _, t, _ in items)
+
+    def run_batched():
+        eng = psb.Engine(max_instances=args.instances, max_depths=128, pool_bytes=24 << 30)
+        t0 = time.perf_counter()
+        for i, t, st in items:
+            assert eng.add(puzzles[t], st, i)
+        res = {}
+        while len(res) < len(items):
+            eng.step(8)
+            res.update(eng.poll())
+        dt = time.perf_counter() - t0
+        levels = eng.info()["levels_run"]
+        eng.close()
+        return res, dt, levels
+
+    sessions = {t: psb.BfsSession(puzzles[t], "two_bit") for t in BATCH_TYPES}
+
+    def run_plain():
+        t0 = time.perf_counter()
+        res = {i: sessions[t].run(st)[0] for i, t, st in items}
+        return res, time.perf_counter() - t0
+
+    for _ in range(max(1, args.warmup - 2)):
+        run_batched()
+        run_plain()
+    b_res, b_dt, levels = run_batched()
+    p_res, p_dt = run_plain()
+    assert b_res == p_res, "batched counts differ from the single-instance path"
+    line = {"metric": "batched solves/s (config 4: 4096 two-bit searches, sliding 2x3/2x4/3x3/2x5 + pancake 7..11)",
+            "value": len(items) / b_dt, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "u64", "data": "seeded random solvable starts",
+            "config": {"workload": "batch4096", "instances": len(items), "states": total_states,
+                       "engine_levels": levels},
+            "batched": {"seconds": b_dt, "solves_per_s": len(items) / b_dt, "states_per_s": total_states / b_dt},
+            "plain_one_per_launch": {"seconds": p_dt, "solves_per_s": len(items) / p_dt,
+                                     "states_per_s": total_states / p_dt},
+            "speedup_vs_plain": p_dt / b_dt, "counts_equal": True}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def profile_once(args):
     """One search with per-level device times (the command ncu wraps)."""
     import puzzlesearch_b200 as psb
@@ -191,15 +270,18 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pancake13-3bit", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="pancake13-3bit", choices=sorted(WORKLOADS) + ["batch4096"])
     ap.add_argument("--window-bits", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-once", action="store_true",
                     help="run ONE search (no warm-up, no e2e, no CPU baseline) and print per-level times; for ncu")
     ap.add_argument("--max-depth", type=int, default=0, help="with --profile-once: stop after this depth")
+    ap.add_argument("--instances", type=int, default=4096, help="--workload batch4096: number of searches")
     args = ap.parse_args()
     if args.profile_once:
         return profile_once(args)
+    if args.workload == "batch4096":
+        return batch_bench(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -189,6 +189,41 @@ int psb_frontier_index(const uint8_t* stream, uint64_t stream_bytes, psb_codec_b
 int psb_frontier_decode(const uint8_t* d_stream, const psb_codec_block* blocks, uint32_t n_blocks,
                         uint64_t* d_bits, uint64_t first_bit, uint64_t n_bits, void* stream);
 
+/* --- Batched and served solves -----------------------------------------------
+ * No single counterpart in the reference (one InMemoryTwoBitBFS per call).
+ * An engine keeps many independent two-bit searches on the GPU at once, each
+ * with its own array in the reference's layout (InMemoryTwoBitBFS.cpp:6-20),
+ * packed back to back in one device pool.  psb_engine_step advances every
+ * active search by one level: one persistent kernel over an
+ * (instance, window) work queue, captured once as a CUDA graph.  Searches
+ * may be added between steps (continuous batching); finished ones are
+ * collected with psb_engine_poll.  Per-depth counts equal psb_bfs's.
+ * Puzzles: sliding tile with 6, 8, 9, 10 or 12 cells, pancake 7..12,
+ * 4-peg Hanoi up to 16 disks. */
+typedef struct psb_engine psb_engine;
+typedef struct {
+    uint32_t struct_size;   /* sizeof(psb_engine_opts) */
+    uint32_t max_instances; /* instance slots */
+    uint32_t max_depths;    /* per-depth counts kept per instance */
+    int32_t device;         /* CUDA device (-1 = current) */
+    uint64_t pool_bytes;    /* device pool for the instances' two-bit arrays (admission limit) */
+    int32_t blocks_per_sm;  /* persistent blocks per SM (0 = 2) */
+    int32_t use_graph;      /* 1 = replay each step as a CUDA graph */
+} psb_engine_opts;
+int psb_engine_create(const psb_engine_opts* opts, psb_engine** out);
+int psb_engine_destroy(psb_engine* e);
+/* Device bytes one instance takes in the pool (2 bits per state, padded). */
+int psb_engine_footprint(int kind, int a, int b, uint64_t* bytes);
+/* Admits one search; PSB_ERR_CAPACITY when no slot or pool space is free. */
+int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial_index, uint64_t tag, uint32_t* slot);
+/* Advances all active searches by `levels` levels (returns after the GPU is done). */
+int psb_engine_step(psb_engine* e, uint32_t levels);
+/* Collects up to cap finished searches: their tags, depth counts and per-depth
+ * counts (row i of counts holds max_depths entries); frees their slots. */
+int psb_engine_poll(psb_engine* e, uint64_t* tags, uint32_t* n_depths, uint64_t* counts, uint32_t cap, uint32_t* n);
+/* Active searches, largest free pool extent, levels stepped so far. */
+int psb_engine_info(psb_engine* e, uint32_t* active, uint64_t* largest_free_bytes, uint64_t* levels_run);
+
 /* --- Search without device allocation --------------------------------------
  * No counterpart in the reference.  For callers that may not call cudaMalloc
  * (all device memory is owned by another allocator or a pre-reserved arena):

@@ -58,6 +58,12 @@ class BfsStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}
 
 
+class EngineOpts(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("max_instances", ctypes.c_uint32),
+                ("max_depths", ctypes.c_uint32), ("device", ctypes.c_int32), ("pool_bytes", ctypes.c_uint64),
+                ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
+
+
 class CodecBlock(ctypes.Structure):
     """psb_codec_block: one block of a compressed frontier stream."""
     _fields_ = [("offset", ctypes.c_uint64), ("count", ctypes.c_uint32), ("bytes", ctypes.c_uint32),
@@ -101,6 +107,14 @@ def lib():
                                          ctypes.c_uint32, u32p]
         L.psb_frontier_decode.argtypes = [ctypes.c_void_p, ctypes.POINTER(CodecBlock), ctypes.c_uint32, u64p,
                                           ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+        L.psb_engine_create.argtypes = [ctypes.POINTER(EngineOpts), ctypes.POINTER(P)]
+        L.psb_engine_destroy.argtypes = [P]
+        L.psb_engine_footprint.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, u64p]
+        L.psb_engine_add.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
+                                     u32p]
+        L.psb_engine_step.argtypes = [P, ctypes.c_uint32]
+        L.psb_engine_poll.argtypes = [P, u64p, u32p, u64p, ctypes.c_uint32, u32p]
+        L.psb_engine_info.argtypes = [P, u32p, u64p, u64p]
         L.psb_bfs_noalloc.argtypes = [P, ctypes.c_int, ctypes.c_uint64, u64p, ctypes.c_uint64, ctypes.c_uint32,
                                       ctypes.c_void_p, u64p, ctypes.c_uint32, u32p]
         _lib = L
@@ -309,6 +323,73 @@ class BfsSession:
     def close(self):
         if getattr(self, "_h", None):
             lib().psb_bfs_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+
+class Engine:
+    """psb_engine: many two-bit searches advanced level by level together
+    (batched solves, and continuous batching for serving)."""
+
+    def __init__(self, max_instances=4096, max_depths=128, pool_bytes=8 << 30, blocks_per_sm=0, use_graph=True,
+                 device=-1):
+        o = EngineOpts()
+        o.struct_size = ctypes.sizeof(EngineOpts)
+        o.max_instances = max_instances
+        o.max_depths = max_depths
+        o.device = device
+        o.pool_bytes = pool_bytes
+        o.blocks_per_sm = blocks_per_sm
+        o.use_graph = 1 if use_graph else 0
+        h = ctypes.c_void_p()
+        _check(lib().psb_engine_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.max_depths = max_depths
+        self.max_instances = max_instances
+
+    @staticmethod
+    def footprint(puzzle):
+        b = ctypes.c_uint64()
+        _check(lib().psb_engine_footprint(puzzle.kind, puzzle.a, puzzle.b, ctypes.byref(b)))
+        return b.value
+
+    def add(self, puzzle, initial, tag):
+        """Admits a search; returns False when the engine is full (no slot or pool space)."""
+        slot = ctypes.c_uint32()
+        rc = lib().psb_engine_add(self._h, puzzle.kind, puzzle.a, puzzle.b, initial, tag, ctypes.byref(slot))
+        if rc == -4:
+            return False
+        _check(rc)
+        return True
+
+    def step(self, levels=1):
+        _check(lib().psb_engine_step(self._h, levels))
+
+    def poll(self, cap=None):
+        """Finished searches as {tag: per-depth counts}."""
+        cap = cap or self.max_instances
+        tags = (ctypes.c_uint64 * cap)()
+        nd = (ctypes.c_uint32 * cap)()
+        counts = (ctypes.c_uint64 * (cap * self.max_depths))()
+        n = ctypes.c_uint32()
+        _check(lib().psb_engine_poll(self._h, tags, nd, counts, cap, ctypes.byref(n)))
+        out = {}
+        for i in range(n.value):
+            row = i * self.max_depths
+            out[tags[i]] = list(counts[row:row + nd[i]])
+        return out
+
+    def info(self):
+        a, f, l = ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().psb_engine_info(self._h, ctypes.byref(a), ctypes.byref(f), ctypes.byref(l)))
+        return {"active": a.value, "largest_free_bytes": f.value, "levels_run": l.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().psb_engine_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -1,0 +1,500 @@
+// psb_engine.cu -- many independent two-bit searches at once.
+//
+// Batched and served solves (no single counterpart in the reference, which
+// runs one InMemoryTwoBitBFS per call, Common/InMemoryTwoBitBFS.cpp:24-69):
+// every instance keeps its own two-bit array, identical in codes and layout
+// to InMemoryTwoBitBFS's, in one device pool, back to back.  One engine step
+// advances every active instance by one BFS level:
+//
+//   build_queue  (1 block): exclusive scan of the active instances' window
+//                counts -> the level's (instance, window) work queue
+//   batch_level  (persistent, #SM x k blocks): blocks pull work items and run
+//                the same per-window level pass as psb_bfs (level_window)
+//   epilogue     (1 block): each instance's count of CUR states becomes its
+//                next per-depth count; an instance whose count is 0 is done
+//                and its slot id is appended to a completion list
+//
+// The three launches are captured once as a CUDA graph and replayed; all
+// per-level state lives in device tables, so instances added between
+// replays (continuous batching) simply appear in the next queue.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/psb200.h"
+#include "psb_internal.h"
+
+namespace psb {
+
+// Puzzle shapes the engine compiles in (one level_window instantiation each).
+enum EngineType : uint32_t {
+    kE_S6 = 0, kE_S8, kE_S9, kE_S10, kE_S12,
+    kE_P7, kE_P8, kE_P9, kE_P10, kE_P11, kE_P12,
+    kE_H,
+    kE_Types
+};
+
+constexpr int kEThreads = 256;
+constexpr int kEMinBlocks = 2;
+constexpr uint32_t kEWindowBitsMax = 16;
+
+struct EngineSlot {
+    LevelArgs args;   // per-instance level arguments (front = marks = its codes)
+    uint32_t type;    // EngineType
+    uint32_t state;   // 0 free, 1 active, 2 done (waiting for the host to collect)
+    uint32_t depth;   // counts recorded so far
+    uint32_t windows; // windows of this instance
+};
+
+struct EngineDev {
+    EngineSlot* slots;
+    unsigned long long* stats;   // 8 per slot
+    unsigned long long* counts;  // max_depths per slot
+    uint32_t* item_start;        // n_slots + 1
+    uint32_t* queue_head;
+    uint32_t* n_items;
+    uint32_t* done_list;         // slot ids, ring of n_slots
+    uint32_t* done_count;        // monotonically increasing
+    uint32_t* n_active;
+    unsigned long long* err;
+    uint32_t n_slots;
+    uint32_t max_depths;
+};
+
+__global__ void __launch_bounds__(1024) engine_build_queue(EngineDev d) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    uint32_t active = 0;
+    for (uint32_t base = 0; base < d.n_slots; base += 1024) {
+        const uint32_t s = base + threadIdx.x;
+        uint32_t w = 0;
+        if (s < d.n_slots && d.slots[s].state == 1) { w = d.slots[s].windows; active++; }
+        uint32_t incl = w;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t t = warp_tot[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + (warp ? warp_tot[warp - 1] : 0) + incl - w;
+        if (s < d.n_slots) d.item_start[s] = excl;
+        const uint32_t block_total = warp_tot[31];
+        __syncthreads();
+        if (threadIdx.x == 0) carry += block_total;
+        __syncthreads();
+    }
+    (void)active;
+    if (threadIdx.x == 0) {
+        d.item_start[d.n_slots] = carry;
+        *d.n_items = carry;
+        *d.queue_head = 0;
+    }
+}
+
+template <int T>
+__device__ __forceinline__ void engine_window(const LevelArgs& a, uint64_t window, unsigned long long* smem,
+                                              WindowShared& sh) {
+    if constexpr (T == kE_S6) level_window<SlidingK<6>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_S8) level_window<SlidingK<8>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_S9) level_window<SlidingK<9>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_S10) level_window<SlidingK<10>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_S12) level_window<SlidingK<12>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_P7) level_window<PancakeK<7>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_P8) level_window<PancakeK<8>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_P9) level_window<PancakeK<9>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_P10) level_window<PancakeK<10>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_P11) level_window<PancakeK<11>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_P12) level_window<PancakeK<12>, kTwoBit, kEThreads>(a, window, smem, sh);
+    if constexpr (T == kE_H) level_window<HanoiK, kTwoBit, kEThreads>(a, window, smem, sh);
+}
+
+__global__ void __launch_bounds__(kEThreads, kEMinBlocks) engine_level(EngineDev d) {
+    extern __shared__ __align__(16) unsigned long long smem64[];
+    __shared__ WindowShared sh;
+    __shared__ uint32_t s_item;
+    const uint32_t n_items = *d.n_items;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(d.queue_head, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        __syncthreads();  // every thread read s_item before thread 0 may overwrite it
+        if (item >= n_items) break;
+        // instance owning this item: last s with item_start[s] <= item
+        uint32_t lo = 0, hi = d.n_slots;  // item_start[lo] <= item < item_start[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (d.item_start[mid] <= item) lo = mid; else hi = mid;
+        }
+        const LevelArgs la = d.slots[lo].args;  // uniform loads: one copy per thread, broadcast by L1
+        const uint32_t type = d.slots[lo].type;
+        const uint64_t window = item - d.item_start[lo];
+        switch (type) {
+        case kE_S6: engine_window<kE_S6>(la, window, smem64, sh); break;
+        case kE_S8: engine_window<kE_S8>(la, window, smem64, sh); break;
+        case kE_S9: engine_window<kE_S9>(la, window, smem64, sh); break;
+        case kE_S10: engine_window<kE_S10>(la, window, smem64, sh); break;
+        case kE_S12: engine_window<kE_S12>(la, window, smem64, sh); break;
+        case kE_P7: engine_window<kE_P7>(la, window, smem64, sh); break;
+        case kE_P8: engine_window<kE_P8>(la, window, smem64, sh); break;
+        case kE_P9: engine_window<kE_P9>(la, window, smem64, sh); break;
+        case kE_P10: engine_window<kE_P10>(la, window, smem64, sh); break;
+        case kE_P11: engine_window<kE_P11>(la, window, smem64, sh); break;
+        case kE_P12: engine_window<kE_P12>(la, window, smem64, sh); break;
+        default: engine_window<kE_H>(la, window, smem64, sh); break;
+        }
+    }
+}
+
+// Records each active instance's count of this level (InMemoryTwoBitBFS.cpp:42-65:
+// a level with no new state ends the search) and rotates its CUR/NEXT codes.
+__global__ void __launch_bounds__(1024) engine_epilogue(EngineDev d) {
+    for (uint32_t s = threadIdx.x; s < d.n_slots; s += 1024) {
+        EngineSlot& slot = d.slots[s];
+        if (slot.state != 1) continue;
+        unsigned long long* st = d.stats + 8ull * s;
+        if (st[3]) atomicOr(d.err, 1ull);
+        const unsigned long long count = st[0];
+        for (int k = 0; k < 8; k++) st[k] = 0;
+        if (count == 0 || slot.depth >= d.max_depths) {
+            if (count != 0) atomicOr(d.err, 2ull);  // more depths than the engine records
+            slot.state = 2;
+            const uint32_t pos = atomicAdd(d.done_count, 1u);
+            d.done_list[pos % d.n_slots] = s;
+            continue;
+        }
+        d.counts[uint64_t(s) * d.max_depths + slot.depth] = count;
+        slot.depth++;
+        slot.args.cur_code = 5u - slot.args.cur_code;
+    }
+}
+
+// Frees the slots the host has collected.
+__global__ void engine_release(EngineDev d, const uint32_t* slots, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) d.slots[slots[i]].state = 0;
+}
+
+}  // namespace psb
+
+struct psb_engine {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    uint32_t n_slots = 0, max_depths = 0;
+    uint64_t pool_words = 0;
+    uint64_t* pool = nullptr;
+    psb::EngineDev d{};
+    std::vector<psb::EngineSlot> host_slots;
+    std::vector<uint64_t> slot_off, slot_words, slot_tag;
+    std::vector<uint32_t> free_slots;
+    std::map<uint64_t, uint64_t> free_space;  // offset -> words (first fit)
+    uint32_t done_seen = 0;
+    uint32_t active = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool use_graph = true;
+    unsigned grid = 0;
+    size_t smem = 0;
+    uint64_t levels_run = 0;
+    uint32_t* h_done_count = nullptr;  // pinned
+
+    ~psb_engine() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        cudaFree(pool);
+        cudaFree(d.slots);
+        cudaFree(d.stats);
+        cudaFree(d.counts);
+        cudaFree(d.item_start);
+        cudaFree(d.err);
+        if (h_done_count) cudaFreeHost(h_done_count);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+#define EN_CUDA(call)                                                                           \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return psb_set_error(e_ == cudaErrorMemoryAllocation ? PSB_ERR_NOMEM : PSB_ERR_CUDA, \
+                                 (std::string(#call) + ": " + cudaGetErrorString(e_)).c_str());  \
+    } while (0)
+
+int engine_type(int kind, int a, int b, uint32_t* type) {
+    if (kind == PSB_SLIDING) {
+        switch (a * b) {
+        case 6: *type = psb::kE_S6; return PSB_OK;
+        case 8: *type = psb::kE_S8; return PSB_OK;
+        case 9: *type = psb::kE_S9; return PSB_OK;
+        case 10: *type = psb::kE_S10; return PSB_OK;
+        case 12: *type = psb::kE_S12; return PSB_OK;
+        }
+    } else if (kind == PSB_PANCAKE) {
+        if (a >= 7 && a <= 12) { *type = psb::kE_P7 + uint32_t(a - 7); return PSB_OK; }
+    } else if (kind == PSB_HANOI4) {
+        if (a >= 1 && a <= 16) { *type = psb::kE_H; return PSB_OK; }
+    }
+    return psb_set_error(PSB_ERR_UNSUPPORTED,
+                         "engine puzzles: sliding tile with 6, 8, 9, 10 or 12 cells, pancake 7..12, Hanoi up to 16 disks");
+}
+
+int engine_window_bits(uint64_t n) {
+    int lg = 0;
+    while (lg < 63 && (uint64_t(1) << (lg + 1)) <= n) lg++;
+    return std::max(10, std::min(int(psb::kEWindowBitsMax), lg - 6));
+}
+
+uint64_t two_bit_words(uint64_t n) { return ((2 * n + 63) / 64 + 31) / 32 * 32; }
+
+int alloc_space(psb_engine* e, uint64_t words, uint64_t* off) {
+    for (auto it = e->free_space.begin(); it != e->free_space.end(); ++it) {
+        if (it->second >= words) {
+            *off = it->first;
+            const uint64_t rest = it->second - words;
+            const uint64_t at = it->first + words;
+            e->free_space.erase(it);
+            if (rest) e->free_space[at] = rest;
+            return PSB_OK;
+        }
+    }
+    return psb_set_error(PSB_ERR_CAPACITY, "engine pool is full");
+}
+
+void free_space(psb_engine* e, uint64_t off, uint64_t words) {
+    auto it = e->free_space.emplace(off, words).first;
+    auto next = std::next(it);
+    if (next != e->free_space.end() && it->first + it->second == next->first) {
+        it->second += next->second;
+        e->free_space.erase(next);
+    }
+    if (it != e->free_space.begin()) {
+        auto prev = std::prev(it);
+        if (prev->first + prev->second == it->first) {
+            prev->second += it->second;
+            e->free_space.erase(it);
+        }
+    }
+}
+
+int record_step(psb_engine* e) {
+    cudaStream_t s = e->stream;
+    psb::engine_build_queue<<<1, 1024, 0, s>>>(e->d);
+    psb::engine_level<<<e->grid, psb::kEThreads, e->smem, s>>>(e->d);
+    psb::engine_epilogue<<<1, 1024, 0, s>>>(e->d);
+    EN_CUDA(cudaGetLastError());
+    return PSB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psb_engine_create(const psb_engine_opts* opts, psb_engine** out) {
+    if (!opts || !out || opts->struct_size != sizeof(psb_engine_opts)) return psb_set_error(PSB_ERR_ARG, "bad options");
+    if (opts->max_instances == 0 || opts->max_depths == 0 || opts->pool_bytes < 256)
+        return psb_set_error(PSB_ERR_ARG, "max_instances, max_depths and pool_bytes must be positive");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return psb_set_error(PSB_ERR_NO_DEVICE, "no CUDA device visible");
+    auto e = std::make_unique<psb_engine>();
+    if (opts->device >= 0) EN_CUDA(cudaSetDevice(opts->device));
+    EN_CUDA(cudaGetDevice(&e->device));
+    e->n_slots = opts->max_instances;
+    e->max_depths = opts->max_depths;
+    e->pool_words = opts->pool_bytes / 8;
+    e->use_graph = opts->use_graph != 0;
+    EN_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    EN_CUDA(cudaMalloc(&e->pool, e->pool_words * 8));
+    e->free_space[0] = e->pool_words;
+    EN_CUDA(cudaMalloc(&e->d.slots, sizeof(psb::EngineSlot) * e->n_slots));
+    EN_CUDA(cudaMalloc(&e->d.stats, 8 * 8ull * e->n_slots));
+    EN_CUDA(cudaMalloc(&e->d.counts, 8ull * e->n_slots * e->max_depths));
+    // small counters in one allocation
+    const size_t ints = size_t(e->n_slots + 1) + 4 + 2 * size_t(e->n_slots) + 2;  // + release scratch
+    uint32_t* ib = nullptr;
+    EN_CUDA(cudaMalloc(&ib, ints * 4 + 16));
+    e->d.item_start = ib;
+    e->d.queue_head = ib + e->n_slots + 1;
+    e->d.n_items = e->d.queue_head + 1;
+    e->d.done_count = e->d.n_items + 1;
+    e->d.n_active = e->d.done_count + 1;
+    e->d.done_list = e->d.n_active + 1;
+    EN_CUDA(cudaMalloc(&e->d.err, 8));
+    EN_CUDA(cudaMemsetAsync(e->d.err, 0, 8, e->stream));
+    e->d.n_slots = e->n_slots;
+    e->d.max_depths = e->max_depths;
+    EN_CUDA(cudaMemsetAsync(e->d.slots, 0, sizeof(psb::EngineSlot) * e->n_slots, e->stream));
+    EN_CUDA(cudaMemsetAsync(e->d.stats, 0, 8 * 8ull * e->n_slots, e->stream));
+    EN_CUDA(cudaMemsetAsync(ib, 0, ints * 4 + 16, e->stream));
+    EN_CUDA(cudaMallocHost(&e->h_done_count, 4));
+    e->host_slots.assign(e->n_slots, psb::EngineSlot{});
+    e->slot_off.assign(e->n_slots, 0);
+    e->slot_words.assign(e->n_slots, 0);
+    e->slot_tag.assign(e->n_slots, 0);
+    for (uint32_t i = e->n_slots; i > 0; i--) e->free_slots.push_back(i - 1);
+    int sms = 0;
+    EN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+    const int per_sm = opts->blocks_per_sm > 0 ? opts->blocks_per_sm : psb::kEMinBlocks;
+    e->grid = unsigned(sms * per_sm);
+    e->smem = psb::mark_bytes(psb::kTwoBit, size_t(1) << psb::kEWindowBitsMax) +
+              size_t(psb::kEThreads) / 32 * 32 * psb::states_per_unit(psb::kTwoBit) * psb::list_entry_bytes(psb::kTwoBit);
+    EN_CUDA(cudaFuncSetAttribute(psb::engine_level, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->smem)));
+    EN_CUDA(cudaStreamSynchronize(e->stream));
+    if (e->use_graph) {
+        EN_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = record_step(e.get());
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        EN_CUDA(ce);
+        e->graph = g;
+        EN_CUDA(cudaGraphInstantiate(&e->exec, e->graph, 0));
+    }
+    *out = e.release();
+    return PSB_OK;
+}
+
+int psb_engine_destroy(psb_engine* e) {
+    delete e;
+    return PSB_OK;
+}
+
+int psb_engine_footprint(int kind, int a, int b, uint64_t* bytes) {
+    psb_puzzle* p = nullptr;
+    if (int rc = psb_puzzle_create(kind, a, b, &p)) return rc;
+    *bytes = two_bit_words(p->n_states) * 8;
+    psb_puzzle_destroy(p);
+    return PSB_OK;
+}
+
+int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial, uint64_t tag, uint32_t* slot_out) {
+    if (!e) return psb_set_error(PSB_ERR_ARG, "engine is NULL");
+    uint32_t type = 0;
+    if (int rc = engine_type(kind, a, b, &type)) return rc;
+    psb_puzzle* p = nullptr;
+    if (int rc = psb_puzzle_create(kind, a, b, &p)) return rc;
+    std::unique_ptr<psb_puzzle, int (*)(psb_puzzle*)> guard(p, psb_puzzle_destroy);
+    if (initial >= p->n_states) return psb_set_error(PSB_ERR_ARG, "initial index >= IndexesCount()");
+    if (e->free_slots.empty()) return psb_set_error(PSB_ERR_CAPACITY, "no free instance slot");
+    const uint64_t words = two_bit_words(p->n_states);
+    uint64_t off = 0;
+    if (int rc = alloc_space(e, words, &off)) return rc;
+    const uint32_t s = e->free_slots.back();
+    e->free_slots.pop_back();
+    e->slot_off[s] = off;
+    e->slot_words[s] = words;
+    e->slot_tag[s] = tag;
+    psb::EngineSlot slot{};
+    slot.type = type;
+    slot.state = 1;
+    slot.depth = 0;
+    const int wb = engine_window_bits(p->n_states);
+    slot.windows = uint32_t((p->n_states + (uint64_t(1) << wb) - 1) >> wb);
+    psb::LevelArgs& la = slot.args;
+    la.front = la.marks = e->pool + off;
+    la.n_states = p->n_states;
+    la.front_words = la.mark_words = (2 * p->n_states + 63) / 64;
+    la.window_bits = wb;
+    la.cur_code = 2;
+    la.odd = p->odd;
+    la.pz = p->pz;
+    la.stats = e->d.stats + 8ull * s;
+    la.wflag_cur = nullptr;
+    la.wflag_next = nullptr;
+    cudaStream_t st = e->stream;
+    EN_CUDA(cudaMemsetAsync(e->pool + off, 0, words * 8, st));
+    static thread_local uint64_t word;
+    word = uint64_t(1) << ((2 * initial) & 63);  // code CUR = 2 at the initial state: bit 2i
+    EN_CUDA(cudaMemcpyAsync(e->pool + off + (2 * initial) / 64, &word, 8, cudaMemcpyHostToDevice, st));
+    EN_CUDA(cudaMemsetAsync(e->d.stats + 8ull * s, 0, 64, st));
+    e->host_slots[s] = slot;
+    EN_CUDA(cudaMemcpyAsync(e->d.slots + s, &e->host_slots[s], sizeof(psb::EngineSlot), cudaMemcpyHostToDevice, st));
+    EN_CUDA(cudaStreamSynchronize(st));
+    e->active++;
+    *slot_out = s;
+    return PSB_OK;
+}
+
+int psb_engine_step(psb_engine* e, uint32_t levels) {
+    if (!e) return psb_set_error(PSB_ERR_ARG, "engine is NULL");
+    for (uint32_t l = 0; l < levels; l++) {
+        if (e->use_graph) EN_CUDA(cudaGraphLaunch(e->exec, e->stream));
+        else if (int rc = record_step(e)) return rc;
+        e->levels_run++;
+    }
+    EN_CUDA(cudaStreamSynchronize(e->stream));
+    unsigned long long err = 0;
+    EN_CUDA(cudaMemcpy(&err, e->d.err, 8, cudaMemcpyDeviceToHost));
+    if (err & 1) return psb_set_error(PSB_ERR_DEVICE, "a level produced a child index >= IndexesCount()");
+    if (err & 2) return psb_set_error(PSB_ERR_CAPACITY, "an instance has more depths than max_depths");
+    return PSB_OK;
+}
+
+int psb_engine_poll(psb_engine* e, uint64_t* tags, uint32_t* n_depths, uint64_t* counts, uint32_t cap, uint32_t* n) {
+    if (!e || !n || (cap && (!tags || !n_depths || !counts))) return psb_set_error(PSB_ERR_ARG, "bad argument");
+    *n = 0;
+    cudaStream_t st = e->stream;
+    EN_CUDA(cudaMemcpyAsync(e->h_done_count, e->d.done_count, 4, cudaMemcpyDeviceToHost, st));
+    EN_CUDA(cudaStreamSynchronize(st));
+    const uint32_t done = *e->h_done_count;
+    const uint32_t k = std::min(cap, done - e->done_seen);
+    if (k == 0) return PSB_OK;
+    std::vector<uint32_t> ring(e->n_slots);
+    EN_CUDA(cudaMemcpyAsync(ring.data(), e->d.done_list, 4ull * e->n_slots, cudaMemcpyDeviceToHost, st));
+    std::vector<psb::EngineSlot> slots(e->n_slots);
+    EN_CUDA(cudaMemcpyAsync(slots.data(), e->d.slots, sizeof(psb::EngineSlot) * e->n_slots, cudaMemcpyDeviceToHost, st));
+    std::vector<uint64_t> all(uint64_t(e->n_slots) * e->max_depths);
+    EN_CUDA(cudaMemcpyAsync(all.data(), e->d.counts, 8 * all.size(), cudaMemcpyDeviceToHost, st));
+    EN_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint32_t> released(k);
+    for (uint32_t i = 0; i < k; i++) {
+        const uint32_t s = ring[(e->done_seen + i) % e->n_slots];
+        tags[i] = e->slot_tag[s];
+        n_depths[i] = slots[s].depth;
+        std::memcpy(counts + uint64_t(i) * e->max_depths, all.data() + uint64_t(s) * e->max_depths,
+                    8ull * e->max_depths);
+        free_space(e, e->slot_off[s], e->slot_words[s]);
+        e->free_slots.push_back(s);
+        released[i] = s;
+    }
+    uint32_t* d_rel = e->d.done_list + e->n_slots;  // scratch after the ring
+    EN_CUDA(cudaMemcpyAsync(d_rel, released.data(), 4ull * k, cudaMemcpyHostToDevice, st));
+    psb::engine_release<<<(k + 255) / 256, 256, 0, st>>>(e->d, d_rel, k);
+    EN_CUDA(cudaGetLastError());
+    EN_CUDA(cudaStreamSynchronize(st));
+    e->done_seen += k;
+    e->active -= k;
+    *n = k;
+    return PSB_OK;
+}
+
+int psb_engine_info(psb_engine* e, uint32_t* active, uint64_t* free_bytes, uint64_t* levels_run) {
+    if (!e) return psb_set_error(PSB_ERR_ARG, "engine is NULL");
+    if (active) *active = e->active;
+    if (free_bytes) {
+        uint64_t best = 0;
+        for (auto& kv : e->free_space) best = std::max(best, kv.second);
+        *free_bytes = best * 8;
+    }
+    if (levels_run) *levels_run = e->levels_run;
+    return PSB_OK;
+}
+
+}  // extern "C"

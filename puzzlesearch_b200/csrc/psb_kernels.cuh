@@ -219,21 +219,29 @@ __device__ __forceinline__ uint32_t bytes_to_bits(const uint32_t* b8) {
     return r;
 }
 
-template <class PZ, int MODE>
-__global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks) level_kernel(LevelArgs a) {
-    constexpr int kThreads = Shape<MODE>::threads;
+// Shared variables of one window pass (a kernel's static shared memory).
+struct WindowShared {
+    uint32_t any;         // some warp found a frontier state in the window
+    uint32_t next_chunk;  // chunks are handed out dynamically so warps finish together
+};
+
+// One window of one level (see the top of this file).  KTHREADS threads of
+// the block take part; smem64 is the block's dynamic shared memory.  The
+// function ends with a block barrier, so a persistent kernel can call it for
+// window after window.
+template <class PZ, int MODE, int KTHREADS>
+__device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window, unsigned long long* smem64,
+                                             WindowShared& sh) {
+    constexpr int kThreads = KTHREADS;
     constexpr int kWarps = kThreads / 32;
     constexpr uint32_t kSPU = states_per_unit(MODE);
     constexpr uint32_t kChunk = 32 * kSPU;           // states per warp chunk
     constexpr int kWPU = MODE == kFrontier ? 4 : 1;  // 64-bit frontier words per unit
-    extern __shared__ __align__(16) unsigned long long smem64[];
-    __shared__ uint32_t s_any;
-    __shared__ uint32_t s_next_chunk;  // chunks are handed out dynamically so warps finish together
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t W = 1u << a.window_bits;
-    const uint64_t base = uint64_t(blockIdx.x) << a.window_bits;
+    const uint64_t base = window << a.window_bits;
     if (base >= a.n_states) return;
-    if (a.wflag_cur && !a.wflag_cur[blockIdx.x]) return;  // no frontier state can be in this window
+    if (a.wflag_cur && !a.wflag_cur[window]) return;  // no frontier state can be in this window
     const uint64_t remaining = a.n_states - base;
     const uint32_t span = remaining < W ? uint32_t(remaining) : W;
     const uint32_t units = (span + kSPU - 1) / kSPU;
@@ -245,8 +253,8 @@ __global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks)
 
     for (uint32_t i = tid; i < mbytes / 16; i += kThreads) reinterpret_cast<uint4*>(smem64)[i] = make_uint4(0, 0, 0, 0);
     if (tid == 0) {
-        s_any = 0;
-        s_next_chunk = kWarps;  // chunks 0 .. kWarps-1 go to warps 0 .. kWarps-1
+        sh.any = 0;
+        sh.next_chunk = kWarps;  // chunks 0 .. kWarps-1 go to warps 0 .. kWarps-1
     }
     __syncthreads();
 
@@ -274,7 +282,7 @@ __global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks)
     load(ch, cw);
     while (ch < chunks) {  // uniform within the warp
         uint32_t nch = 0;
-        if (lane == 0) nch = atomicAdd(&s_next_chunk, 1u);
+        if (lane == 0) nch = atomicAdd(&sh.next_chunk, 1u);
         nch = __shfl_sync(0xFFFFFFFFu, nch, 0);
         load(nch, nw);
         const uint32_t u = ch * 32 + uint32_t(lane);
@@ -346,12 +354,12 @@ __global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks)
         for (int q = 0; q < kWPU; ++q) cw[q] = nw[q];
         ch = nch;
     }
-    if (found) s_any = 1;
+    if (found) sh.any = 1;
     __syncthreads();
 
     // Flush the window's shared-memory marks (only if it had frontier states).
-    if (s_any) {
-        if (a.wflag_next && tid == 0) a.wflag_next[blockIdx.x] = 1;
+    if (sh.any) {
+        if (a.wflag_next && tid == 0) a.wflag_next[window] = 1;
         if constexpr (MODE == kTwoBit) {
             const uint32_t next_pat = em.next_pat;
             unsigned long long* codes = reinterpret_cast<unsigned long long*>(a.marks) + (base >> 5);
@@ -390,6 +398,14 @@ __global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks)
         if (c2) atomicAdd(&a.stats[2], (unsigned long long)c2);
         if (c3) atomicOr(&a.stats[3], 1ull);
     }
+    __syncthreads();  // the shared marks and lists may be reused for another window
+}
+
+template <class PZ, int MODE>
+__global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks) level_kernel(LevelArgs a) {
+    extern __shared__ __align__(16) unsigned long long smem64[];
+    __shared__ WindowShared sh;
+    level_window<PZ, MODE, Shape<MODE>::threads>(a, blockIdx.x, smem64, sh);
 }
 
 // Level 0 of frontier search (InMemoryFrontierSearch.cpp:81-88): expand the
