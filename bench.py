@@ -250,6 +250,83 @@ def batch_bench(args):
     return 0
 
 
+SERVE_TYPES = [("sliding", 2, 4), ("sliding", 3, 3), ("sliding", 2, 5), ("sliding", 3, 4)] + \
+              [("pancake", n, 0) for n in range(8, 13)] + [("hanoi4", n, 0) for n in range(8, 15)]
+
+
+def serve_bench(args):
+    """seeded Poisson request streams (rates 10..2000 req/s),
+    request type uniform over sliding 2x4/3x3/2x5/3x4, pancake 8..12 and Hanoi
+    8..14 disks, random solvable starts.  The server (continuous batching,
+    admission by HBM footprint) against plain sequential solves of the same
+    stream (one search at a time, FIFO), both on this GPU.  Latency = arrival
+    to completion."""
+    import random
+
+    import puzzlesearch_b200 as psb
+    puzzles = {t: _make(psb, *t) for t in SERVE_TYPES}
+    sessions = {t: psb.BfsSession(puzzles[t], "two_bit") for t in SERVE_TYPES}
+    for t in SERVE_TYPES:  # warm-up: load every kernel once
+        sessions[t].run(0)
+    rows = []
+    for rate in args.rates:
+        rng = random.Random(int(rate))
+        n_req = int(max(30, min(args.max_requests, rate * args.window)))
+        arrivals, reqs, t = [], [], 0.0
+        for _ in range(n_req):
+            t += rng.expovariate(rate)
+            ty = SERVE_TYPES[rng.randrange(len(SERVE_TYPES))]
+            arrivals.append(t)
+            reqs.append((ty, solvable_start(rng, *ty, puzzles[ty])))
+        # plain: one search at a time in arrival order
+        service = []
+        plain_counts = []
+        for ty, st in reqs:
+            t0 = time.perf_counter()
+            c, _ = sessions[ty].run(st)
+            service.append(time.perf_counter() - t0)
+            plain_counts.append(c)
+        free_at, plain_lat = 0.0, []
+        for a, sv in zip(arrivals, service):
+            begin = max(a, free_at)
+            free_at = begin + sv
+            plain_lat.append(free_at - a)
+        plain_span = free_at - arrivals[0]
+        # served: submit at the arrival times, continuous batching on the GPU
+        srv = psb.Server(max_instances=1024, max_depths=256, pool_bytes=args.pool_gb << 30)
+        t_start = time.perf_counter()
+        tickets = {}
+        done = {}
+        for i, (a, (ty, st)) in enumerate(zip(arrivals, reqs)):
+            while time.perf_counter() - t_start < a:
+                done.update(srv.poll())
+                time.sleep(0.0005)
+            tickets[srv.submit(puzzles[ty], st)] = i
+        while len(done) < n_req:
+            done.update(srv.poll())
+            time.sleep(0.001)
+        t_end = time.perf_counter()
+        srv.stop()
+        lat = sorted(done[k][2] for k in tickets)
+        for k, i in tickets.items():
+            assert done[k][0] == 0 and done[k][1] == plain_counts[i], "served result differs from the plain solve"
+        pl = sorted(plain_lat)
+        q = lambda v, f: v[min(len(v) - 1, int(f * len(v)))]
+        rows.append({"rate": rate, "requests": n_req,
+                     "served": {"solves_per_s": n_req / (t_end - t_start - arrivals[0]),
+                                "p50_s": q(lat, 0.5), "p99_s": q(lat, 0.99)},
+                     "plain": {"solves_per_s": n_req / plain_span, "p50_s": q(pl, 0.5), "p99_s": q(pl, 0.99)},
+                     "mean_eccentricity": sum(len(done[k][1]) - 1 for k in tickets) / n_req})
+        print(json.dumps({"progress": rows[-1]}), file=sys.stderr, flush=True)
+    line = {"metric": "served solves/s and p50/p99 latency (config 5: Poisson streams, continuous batching)",
+            "value": max(r["served"]["solves_per_s"] for r in rows), "unit": "solves/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "u64", "data": "seeded Poisson streams, random solvable starts",
+            "config": {"workload": "serve", "types": len(SERVE_TYPES), "pool_gb": args.pool_gb},
+            "rates": rows, "results_equal_plain": True}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def profile_once(args):
     """One search with per-level device times (the command ncu wraps)."""
     import puzzlesearch_b200 as psb
@@ -270,18 +347,25 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pancake13-3bit", choices=sorted(WORKLOADS) + ["batch4096"])
+    ap.add_argument("--workload", default="pancake13-3bit", choices=sorted(WORKLOADS) + ["batch4096", "serve"])
     ap.add_argument("--window-bits", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-once", action="store_true",
                     help="run ONE search (no warm-up, no e2e, no CPU baseline) and print per-level times; for ncu")
     ap.add_argument("--max-depth", type=int, default=0, help="with --profile-once: stop after this depth")
     ap.add_argument("--instances", type=int, default=4096, help="--workload batch4096: number of searches")
+    ap.add_argument("--rates", type=float, nargs="+", default=[10, 30, 100, 300, 1000, 2000],
+                    help="--workload serve: request rates (req/s)")
+    ap.add_argument("--window", type=float, default=3.0, help="--workload serve: seconds of arrivals per rate")
+    ap.add_argument("--max-requests", type=int, default=400, help="--workload serve: requests per rate at most")
+    ap.add_argument("--pool-gb", type=int, default=32, help="--workload serve: engine pool (HBM admission limit)")
     args = ap.parse_args()
     if args.profile_once:
         return profile_once(args)
     if args.workload == "batch4096":
         return batch_bench(args)
+    if args.workload == "serve":
+        return serve_bench(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

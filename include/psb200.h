@@ -212,7 +212,8 @@ typedef struct {
 } psb_engine_opts;
 int psb_engine_create(const psb_engine_opts* opts, psb_engine** out);
 int psb_engine_destroy(psb_engine* e);
-/* Device bytes one instance takes in the pool (2 bits per state, padded). */
+/* Device bytes one instance takes in the pool: its two-bit array (2 bits per
+ * state, padded) plus two bytes per window of active-window flags. */
 int psb_engine_footprint(int kind, int a, int b, uint64_t* bytes);
 /* Admits one search; PSB_ERR_CAPACITY when no slot or pool space is free. */
 int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial_index, uint64_t tag, uint32_t* slot);
@@ -223,6 +224,30 @@ int psb_engine_step(psb_engine* e, uint32_t levels);
 int psb_engine_poll(psb_engine* e, uint64_t* tags, uint32_t* n_depths, uint64_t* counts, uint32_t cap, uint32_t* n);
 /* Active searches, largest free pool extent, levels stepped so far. */
 int psb_engine_info(psb_engine* e, uint32_t* active, uint64_t* largest_free_bytes, uint64_t* levels_run);
+
+/* --- Solve server (continuous batching) -------------------------------------
+ * No counterpart in the reference.  A server thread owns a psb_engine: it
+ * admits submitted requests first come first served while a slot and pool
+ * space are free (admission by HBM footprint), advances all resident searches
+ * one level per step, and completes each with its per-depth counts, its
+ * eccentricity (n_depths - 1) and its latency from submission.  Submit and
+ * poll are non-blocking and may be called from any thread. */
+typedef struct psb_server psb_server;
+typedef struct {
+    uint32_t struct_size;     /* sizeof(psb_server_opts) */
+    uint32_t levels_per_step; /* BFS levels per engine step (0 = 1) */
+    psb_engine_opts engine;
+} psb_server_opts;
+int psb_server_start(const psb_server_opts* opts, psb_server** out);
+int psb_server_submit(psb_server* s, int kind, int a, int b, uint64_t initial_index, uint64_t* ticket);
+/* Completed requests: ticket, status (PSB_OK or the admission error), depth
+ * count, per-depth counts (max_depths per row), latency in seconds. */
+int psb_server_poll(psb_server* s, uint64_t* tickets, int* status, uint32_t* n_depths, uint64_t* counts,
+                    double* latency_s, uint32_t cap, uint32_t* n);
+/* Queued and running requests, completed requests, engine steps; returns the
+ * server's fatal error if it stopped on one. */
+int psb_server_info(psb_server* s, uint32_t* queued, uint32_t* running, uint64_t* completed, uint64_t* steps);
+int psb_server_stop(psb_server* s);
 
 /* --- Search without device allocation --------------------------------------
  * No counterpart in the reference.  For callers that may not call cudaMalloc

@@ -64,6 +64,10 @@ class EngineOpts(ctypes.Structure):
                 ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("levels_per_step", ctypes.c_uint32), ("engine", EngineOpts)]
+
+
 class CodecBlock(ctypes.Structure):
     """psb_codec_block: one block of a compressed frontier stream."""
     _fields_ = [("offset", ctypes.c_uint64), ("count", ctypes.c_uint32), ("bytes", ctypes.c_uint32),
@@ -115,6 +119,12 @@ def lib():
         L.psb_engine_step.argtypes = [P, ctypes.c_uint32]
         L.psb_engine_poll.argtypes = [P, u64p, u32p, u64p, ctypes.c_uint32, u32p]
         L.psb_engine_info.argtypes = [P, u32p, u64p, u64p]
+        L.psb_server_start.argtypes = [ctypes.POINTER(ServerOpts), ctypes.POINTER(P)]
+        L.psb_server_submit.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, u64p]
+        L.psb_server_poll.argtypes = [P, u64p, ctypes.POINTER(ctypes.c_int), u32p, u64p,
+                                      ctypes.POINTER(ctypes.c_double), ctypes.c_uint32, u32p]
+        L.psb_server_info.argtypes = [P, u32p, u32p, u64p, u64p]
+        L.psb_server_stop.argtypes = [P]
         L.psb_bfs_noalloc.argtypes = [P, ctypes.c_int, ctypes.c_uint64, u64p, ctypes.c_uint64, ctypes.c_uint32,
                                       ctypes.c_void_p, u64p, ctypes.c_uint32, u32p]
         _lib = L
@@ -395,6 +405,60 @@ class Engine:
     def __del__(self):
         if _lib is not None:
             self.close()
+
+
+class Server:
+    """psb_server: a solve server with continuous batching on one GPU."""
+
+    def __init__(self, max_instances=1024, max_depths=256, pool_bytes=16 << 30, levels_per_step=1, device=-1):
+        o = ServerOpts()
+        o.struct_size = ctypes.sizeof(ServerOpts)
+        o.levels_per_step = levels_per_step
+        e = o.engine
+        e.struct_size = ctypes.sizeof(EngineOpts)
+        e.max_instances = max_instances
+        e.max_depths = max_depths
+        e.device = device
+        e.pool_bytes = pool_bytes
+        e.use_graph = 1
+        h = ctypes.c_void_p()
+        _check(lib().psb_server_start(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.max_depths = max_depths
+
+    def submit(self, puzzle, initial):
+        t = ctypes.c_uint64()
+        _check(lib().psb_server_submit(self._h, puzzle.kind, puzzle.a, puzzle.b, initial, ctypes.byref(t)))
+        return t.value
+
+    def poll(self, cap=1024):
+        """Completed requests: {ticket: (status, counts, latency_s)}; eccentricity = len(counts) - 1."""
+        tickets = (ctypes.c_uint64 * cap)()
+        status = (ctypes.c_int * cap)()
+        nd = (ctypes.c_uint32 * cap)()
+        counts = (ctypes.c_uint64 * (cap * self.max_depths))()
+        lat = (ctypes.c_double * cap)()
+        n = ctypes.c_uint32()
+        _check(lib().psb_server_poll(self._h, tickets, status, nd, counts, lat, cap, ctypes.byref(n)))
+        out = {}
+        for i in range(n.value):
+            row = i * self.max_depths
+            out[tickets[i]] = (status[i], list(counts[row:row + nd[i]]), lat[i])
+        return out
+
+    def info(self):
+        q, r, c, st = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint64()
+        rc = lib().psb_server_info(self._h, ctypes.byref(q), ctypes.byref(r), ctypes.byref(c), ctypes.byref(st))
+        return {"queued": q.value, "running": r.value, "completed": c.value, "steps": st.value, "status": rc}
+
+    def stop(self):
+        if getattr(self, "_h", None):
+            lib().psb_server_stop(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.stop()
 
 
 def frontier_index(data):

@@ -44,11 +44,12 @@ constexpr int kEMinBlocks = 2;
 constexpr uint32_t kEWindowBitsMax = 16;
 
 struct EngineSlot {
-    LevelArgs args;   // per-instance level arguments (front = marks = its codes)
-    uint32_t type;    // EngineType
-    uint32_t state;   // 0 free, 1 active, 2 done (waiting for the host to collect)
-    uint32_t depth;   // counts recorded so far
-    uint32_t windows; // windows of this instance
+    LevelArgs args;     // per-instance level arguments (front = marks = its codes)
+    uint8_t* flags[2];  // active-window flags, windows bytes each (see psb_bfs)
+    uint32_t type;      // EngineType
+    uint32_t state;     // 0 free, 1 active, 2 done (waiting for the host to collect)
+    uint32_t depth;     // counts recorded so far
+    uint32_t windows;   // windows of this instance
 };
 
 struct EngineDev {
@@ -182,7 +183,35 @@ __global__ void __launch_bounds__(1024) engine_epilogue(EngineDev d) {
         d.counts[uint64_t(s) * d.max_depths + slot.depth] = count;
         slot.depth++;
         slot.args.cur_code = 5u - slot.args.cur_code;
+        // Active-window flags, the psb_bfs policy: the flags this level
+        // recorded (if it recorded any) steer the next level's sweep, and the
+        // next level records flags when this level's frontier is sparse.
+        uint8_t* produced = slot.args.wflag_next;
+        slot.args.wflag_cur = produced;
+        if (count < slot.args.n_states / 64) {
+            uint8_t* other = produced == slot.flags[0] ? slot.flags[1] : slot.flags[0];
+            uint4* z = reinterpret_cast<uint4*>(other);
+            for (uint32_t i = 0; i < (slot.windows + 15) / 16; i++) z[i] = make_uint4(0, 0, 0, 0);
+            slot.args.wflag_next = other;
+        } else {
+            slot.args.wflag_next = nullptr;
+        }
     }
+}
+
+// Copies the finished instances [first, first + n) of the completion list into
+// one staging buffer: per instance [slot, depth, counts[max_depths]].
+__global__ void engine_collect(EngineDev d, uint32_t first, uint32_t n, unsigned long long* staging) {
+    const uint32_t i = blockIdx.x;
+    if (i >= n) return;
+    const uint32_t s = d.done_list[(first + i) % d.n_slots];
+    unsigned long long* row = staging + uint64_t(i) * (d.max_depths + 2);
+    if (threadIdx.x == 0) {
+        row[0] = s;
+        row[1] = d.slots[s].depth;
+    }
+    for (uint32_t k = threadIdx.x; k < d.max_depths; k += blockDim.x)
+        row[2 + k] = d.counts[uint64_t(s) * d.max_depths + k];
 }
 
 // Frees the slots the host has collected.
@@ -213,6 +242,8 @@ struct psb_engine {
     size_t smem = 0;
     uint64_t levels_run = 0;
     uint32_t* h_done_count = nullptr;  // pinned
+    unsigned long long* d_staging = nullptr;  // collect rows (device)
+    std::vector<unsigned long long> h_staging;
 
     ~psb_engine() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -224,6 +255,7 @@ struct psb_engine {
         cudaFree(d.item_start);
         cudaFree(d.err);
         if (h_done_count) cudaFreeHost(h_done_count);
+        cudaFree(d_staging);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -263,6 +295,17 @@ int engine_window_bits(uint64_t n) {
 }
 
 uint64_t two_bit_words(uint64_t n) { return ((2 * n + 63) / 64 + 31) / 32 * 32; }
+
+uint32_t instance_windows(uint64_t n) {
+    const int wb = engine_window_bits(n);
+    return uint32_t((n + (uint64_t(1) << wb) - 1) >> wb);
+}
+
+// Two 256-byte-aligned arrays of one flag byte per window.
+uint64_t flag_words_for(uint64_t n) { return 2 * ((uint64_t(instance_windows(n)) + 255) / 256 * 32); }
+
+// Pool words of one instance: its two-bit array plus its window flags.
+uint64_t instance_words(uint64_t n) { return two_bit_words(n) + flag_words_for(n); }
 
 int alloc_space(psb_engine* e, uint64_t words, uint64_t* off) {
     for (auto it = e->free_space.begin(); it != e->free_space.end(); ++it) {
@@ -344,6 +387,8 @@ int psb_engine_create(const psb_engine_opts* opts, psb_engine** out) {
     EN_CUDA(cudaMemsetAsync(e->d.stats, 0, 8 * 8ull * e->n_slots, e->stream));
     EN_CUDA(cudaMemsetAsync(ib, 0, ints * 4 + 16, e->stream));
     EN_CUDA(cudaMallocHost(&e->h_done_count, 4));
+    EN_CUDA(cudaMalloc(&e->d_staging, 8ull * e->n_slots * (e->max_depths + 2)));
+    e->h_staging.resize(size_t(e->n_slots) * (e->max_depths + 2));
     e->host_slots.assign(e->n_slots, psb::EngineSlot{});
     e->slot_off.assign(e->n_slots, 0);
     e->slot_words.assign(e->n_slots, 0);
@@ -379,7 +424,7 @@ int psb_engine_destroy(psb_engine* e) {
 int psb_engine_footprint(int kind, int a, int b, uint64_t* bytes) {
     psb_puzzle* p = nullptr;
     if (int rc = psb_puzzle_create(kind, a, b, &p)) return rc;
-    *bytes = two_bit_words(p->n_states) * 8;
+    *bytes = instance_words(p->n_states) * 8;
     psb_puzzle_destroy(p);
     return PSB_OK;
 }
@@ -393,7 +438,11 @@ int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial, uint
     std::unique_ptr<psb_puzzle, int (*)(psb_puzzle*)> guard(p, psb_puzzle_destroy);
     if (initial >= p->n_states) return psb_set_error(PSB_ERR_ARG, "initial index >= IndexesCount()");
     if (e->free_slots.empty()) return psb_set_error(PSB_ERR_CAPACITY, "no free instance slot");
-    const uint64_t words = two_bit_words(p->n_states);
+    const int wb = engine_window_bits(p->n_states);
+    const uint32_t windows = instance_windows(p->n_states);
+    const uint64_t code_words = two_bit_words(p->n_states);
+    const uint64_t flag_words = flag_words_for(p->n_states);
+    const uint64_t words = instance_words(p->n_states);
     uint64_t off = 0;
     if (int rc = alloc_space(e, words, &off)) return rc;
     const uint32_t s = e->free_slots.back();
@@ -405,8 +454,9 @@ int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial, uint
     slot.type = type;
     slot.state = 1;
     slot.depth = 0;
-    const int wb = engine_window_bits(p->n_states);
-    slot.windows = uint32_t((p->n_states + (uint64_t(1) << wb) - 1) >> wb);
+    slot.windows = windows;
+    slot.flags[0] = reinterpret_cast<uint8_t*>(e->pool + off + code_words);
+    slot.flags[1] = slot.flags[0] + flag_words * 4;
     psb::LevelArgs& la = slot.args;
     la.front = la.marks = e->pool + off;
     la.n_states = p->n_states;
@@ -416,10 +466,14 @@ int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial, uint
     la.odd = p->odd;
     la.pz = p->pz;
     la.stats = e->d.stats + 8ull * s;
-    la.wflag_cur = nullptr;
-    la.wflag_next = nullptr;
+    // Level 0 sweeps only the start state's window and records flags for level 1.
+    la.wflag_cur = slot.flags[0];
+    la.wflag_next = slot.flags[1];
     cudaStream_t st = e->stream;
     EN_CUDA(cudaMemsetAsync(e->pool + off, 0, words * 8, st));
+    static thread_local uint8_t one;
+    one = 1;
+    EN_CUDA(cudaMemcpyAsync(slot.flags[0] + (initial >> wb), &one, 1, cudaMemcpyHostToDevice, st));
     static thread_local uint64_t word;
     word = uint64_t(1) << ((2 * initial) & 63);  // code CUR = 2 at the initial state: bit 2i
     EN_CUDA(cudaMemcpyAsync(e->pool + off + (2 * initial) / 64, &word, 8, cudaMemcpyHostToDevice, st));
@@ -456,20 +510,18 @@ int psb_engine_poll(psb_engine* e, uint64_t* tags, uint32_t* n_depths, uint64_t*
     const uint32_t done = *e->h_done_count;
     const uint32_t k = std::min(cap, done - e->done_seen);
     if (k == 0) return PSB_OK;
-    std::vector<uint32_t> ring(e->n_slots);
-    EN_CUDA(cudaMemcpyAsync(ring.data(), e->d.done_list, 4ull * e->n_slots, cudaMemcpyDeviceToHost, st));
-    std::vector<psb::EngineSlot> slots(e->n_slots);
-    EN_CUDA(cudaMemcpyAsync(slots.data(), e->d.slots, sizeof(psb::EngineSlot) * e->n_slots, cudaMemcpyDeviceToHost, st));
-    std::vector<uint64_t> all(uint64_t(e->n_slots) * e->max_depths);
-    EN_CUDA(cudaMemcpyAsync(all.data(), e->d.counts, 8 * all.size(), cudaMemcpyDeviceToHost, st));
+    const size_t row = size_t(e->max_depths) + 2;
+    psb::engine_collect<<<k, 128, 0, st>>>(e->d, e->done_seen, k, e->d_staging);
+    EN_CUDA(cudaGetLastError());
+    EN_CUDA(cudaMemcpyAsync(e->h_staging.data(), e->d_staging, 8 * row * k, cudaMemcpyDeviceToHost, st));
     EN_CUDA(cudaStreamSynchronize(st));
     std::vector<uint32_t> released(k);
     for (uint32_t i = 0; i < k; i++) {
-        const uint32_t s = ring[(e->done_seen + i) % e->n_slots];
+        const unsigned long long* r = e->h_staging.data() + row * i;
+        const uint32_t s = uint32_t(r[0]);
         tags[i] = e->slot_tag[s];
-        n_depths[i] = slots[s].depth;
-        std::memcpy(counts + uint64_t(i) * e->max_depths, all.data() + uint64_t(s) * e->max_depths,
-                    8ull * e->max_depths);
+        n_depths[i] = uint32_t(r[1]);
+        std::memcpy(counts + uint64_t(i) * e->max_depths, r + 2, 8ull * e->max_depths);
         free_space(e, e->slot_off[s], e->slot_words[s]);
         e->free_slots.push_back(s);
         released[i] = s;

@@ -1,0 +1,197 @@
+// psb_server.cu -- a solve server with continuous batching (no counterpart in
+// the reference, which solves one puzzle per call).
+//
+// Clients submit solve requests (puzzle, start state) from any thread without
+// blocking.  One server thread owns a psb_engine and loops:
+//   1. admit queued requests, first come first served, while an instance
+//      slot and pool space for the request's two-bit array are free
+//      (admission by HBM footprint: 2 bits x states, padded);
+//   2. advance every resident search by one BFS level (psb_engine_step), so
+//      requests that arrive while others are running overlap on the GPU;
+//   3. collect finished searches: per-depth counts, eccentricity (the last
+//      depth) and latency from submission to completion.
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/psb200.h"
+#include "psb_internal.h"
+
+namespace {
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t ticket;
+    int kind, a, b;
+    uint64_t initial;
+    Clock::time_point submitted;
+};
+
+struct Done {
+    uint64_t ticket;
+    int status;  // PSB_OK or the admission/engine error
+    std::vector<uint64_t> counts;
+    double latency;
+};
+}  // namespace
+
+struct psb_server {
+    psb_engine* engine = nullptr;
+    uint32_t max_depths = 0;
+    uint32_t levels_per_step = 1;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Request> queue;
+    std::vector<Done> done;
+    std::unordered_map<uint64_t, Request> running;
+    std::atomic<bool> stop{false};
+    std::atomic<uint64_t> next_ticket{1};
+    int fatal = PSB_OK;
+    std::string fatal_msg;
+    uint64_t admitted = 0, completed = 0, steps = 0;
+};
+
+namespace {
+
+void serve(psb_server* s) {
+    std::vector<uint64_t> tags(1024), counts;
+    std::vector<uint32_t> nd(1024);
+    counts.resize(size_t(1024) * s->max_depths);
+    for (;;) {
+        std::vector<Request> admit;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            if (s->running.empty())
+                s->cv.wait(lock, [&] { return s->stop.load() || !s->queue.empty(); });
+            if (s->stop.load()) return;
+            // FIFO admission while the engine has room.
+            while (!s->queue.empty()) {
+                const Request& r = s->queue.front();
+                uint32_t slot = 0;
+                const int rc = psb_engine_add(s->engine, r.kind, r.a, r.b, r.initial, r.ticket, &slot);
+                if (rc == PSB_ERR_CAPACITY) break;  // wait for a slot or pool space to free up
+                if (rc != PSB_OK) {                 // unsupported puzzle or bad start: report, drop
+                    s->done.push_back(Done{r.ticket, rc, {}, 0.0});
+                    s->queue.pop_front();
+                    continue;
+                }
+                s->running.emplace(r.ticket, r);
+                s->admitted++;
+                s->queue.pop_front();
+            }
+        }
+        if (!s->running.empty()) {
+            int rc = psb_engine_step(s->engine, s->levels_per_step);
+            uint32_t n = 0;
+            if (rc == PSB_OK) rc = psb_engine_poll(s->engine, tags.data(), nd.data(), counts.data(), 1024, &n);
+            const auto now = Clock::now();
+            std::lock_guard<std::mutex> lock(s->mu);
+            s->steps++;
+            if (rc != PSB_OK) {
+                char buf[512];
+                psb_last_error(buf, sizeof buf);
+                s->fatal = rc;
+                s->fatal_msg = buf;
+                for (auto& kv : s->running) s->done.push_back(Done{kv.first, rc, {}, 0.0});
+                s->running.clear();
+                s->stop = true;
+                return;
+            }
+            for (uint32_t i = 0; i < n; i++) {
+                auto it = s->running.find(tags[i]);
+                if (it == s->running.end()) continue;
+                const double lat = std::chrono::duration<double>(now - it->second.submitted).count();
+                const uint64_t* row = counts.data() + size_t(i) * s->max_depths;
+                s->done.push_back(Done{tags[i], PSB_OK, std::vector<uint64_t>(row, row + nd[i]), lat});
+                s->running.erase(it);
+                s->completed++;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int psb_server_start(const psb_server_opts* opts, psb_server** out) {
+    if (!opts || !out || opts->struct_size != sizeof(psb_server_opts)) return psb_set_error(PSB_ERR_ARG, "bad options");
+    auto* s = new psb_server();
+    if (int rc = psb_engine_create(&opts->engine, &s->engine)) { delete s; return rc; }
+    s->max_depths = opts->engine.max_depths;
+    s->levels_per_step = opts->levels_per_step ? opts->levels_per_step : 1;
+    int device = -1;
+    cudaGetDevice(&device);
+    s->worker = std::thread([s, device] {
+        cudaSetDevice(device);
+        serve(s);
+    });
+    *out = s;
+    return PSB_OK;
+}
+
+int psb_server_submit(psb_server* s, int kind, int a, int b, uint64_t initial, uint64_t* ticket) {
+    if (!s || !ticket) return psb_set_error(PSB_ERR_ARG, "bad argument");
+    Request r{s->next_ticket.fetch_add(1), kind, a, b, initial, Clock::now()};
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->stop.load()) return psb_set_error(s->fatal ? s->fatal : PSB_ERR_ARG, "server stopped");
+        s->queue.push_back(r);
+    }
+    s->cv.notify_one();
+    *ticket = r.ticket;
+    return PSB_OK;
+}
+
+int psb_server_poll(psb_server* s, uint64_t* tickets, int* status, uint32_t* n_depths, uint64_t* counts,
+                    double* latency_s, uint32_t cap, uint32_t* n) {
+    if (!s || !n || (cap && (!tickets || !status || !n_depths || !counts || !latency_s)))
+        return psb_set_error(PSB_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    const uint32_t k = uint32_t(std::min<size_t>(cap, s->done.size()));
+    for (uint32_t i = 0; i < k; i++) {
+        const Done& d = s->done[i];
+        tickets[i] = d.ticket;
+        status[i] = d.status;
+        n_depths[i] = uint32_t(d.counts.size());
+        latency_s[i] = d.latency;
+        std::memset(counts + size_t(i) * s->max_depths, 0, 8ull * s->max_depths);
+        std::memcpy(counts + size_t(i) * s->max_depths, d.counts.data(), 8 * d.counts.size());
+    }
+    s->done.erase(s->done.begin(), s->done.begin() + k);
+    *n = k;
+    return PSB_OK;
+}
+
+int psb_server_info(psb_server* s, uint32_t* queued, uint32_t* running, uint64_t* completed, uint64_t* steps) {
+    if (!s) return psb_set_error(PSB_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (queued) *queued = uint32_t(s->queue.size());
+    if (running) *running = uint32_t(s->running.size());
+    if (completed) *completed = s->completed;
+    if (steps) *steps = s->steps;
+    return s->fatal;
+}
+
+int psb_server_stop(psb_server* s) {
+    if (!s) return PSB_OK;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    psb_engine_destroy(s->engine);
+    delete s;
+    return PSB_OK;
+}
+
+}  // extern "C"
