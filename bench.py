@@ -334,7 +334,8 @@ def profile_once(args):
     kind, a, b, algo, desc = WORKLOADS[args.workload]
     puzzle = {"pancake": lambda: psb.PancakeSimple(a), "sliding": lambda: psb.SlidingTilePuzzleSimple(a, b),
               "hanoi4": lambda: psb.FourPegHanoiSimple(a, bool(b))}[kind]()
-    r = psb.bfs(puzzle, algo, 0, max_depth=args.max_depth, window_bits=args.window_bits, levels=True)
+    r = psb.bfs(puzzle, algo, 0, max_depth=args.max_depth, window_bits=args.window_bits, levels=True,
+                direction=args.direction, bottom_up_ratio=args.bottom_up_ratio)
     out = {"workload": args.workload, "counts": r["counts"], "level_ms": [round(x, 3) for x in r["level_ms"]],
            "level_children": r["level_children"], "stats": r["stats"]}
     print(json.dumps(out), flush=True)
@@ -350,6 +351,10 @@ def main():
     ap.add_argument("--workload", default="pancake13-3bit", choices=sorted(WORKLOADS) + ["batch4096", "serve"])
     ap.add_argument("--window-bits", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--direction", default="auto", choices=["auto", "top_down", "bottom_up"],
+                    help="level direction (PSB_DIR_*): auto switches to bottom-up on the last dense levels")
+    ap.add_argument("--bottom-up-ratio", type=float, default=0.0,
+                    help="auto: a level runs bottom-up when unvisited < ratio x frontier (0 = library default)")
     ap.add_argument("--profile-once", action="store_true",
                     help="run ONE search (no warm-up, no e2e, no CPU baseline) and print per-level times; for ncu")
     ap.add_argument("--max-depth", type=int, default=0, help="with --profile-once: stop after this depth")
@@ -383,7 +388,7 @@ def main():
     N = puzzle.IndexesCount()
     stream = torch.cuda.Stream()
     # Session on torch's stream so the CUDA events below bracket exactly the searches.
-    opts = psb._opts(0, args.window_bits, local, stream.cuda_stream)
+    opts = psb._opts(0, args.window_bits, local, stream.cuda_stream, direction=args.direction)
     h = ctypes.c_void_p()
     psb._check(psb.lib().psb_bfs_session_create(puzzle.handle, psb._algo(algo), ctypes.byref(opts), ctypes.byref(h)))
     cap = 1 << 16
@@ -393,7 +398,8 @@ def main():
     def run_once():
         st = psb.BfsStats()
         st.struct_size = ctypes.sizeof(psb.BfsStats)
-        o = psb._opts(0, 0, local, stream.cuda_stream)
+        o = psb._opts(0, 0, local, stream.cuda_stream, direction=args.direction,
+                      bottom_up_ratio=args.bottom_up_ratio)
         psb._check(psb.lib().psb_bfs_session_run(h, 0, ctypes.byref(o), counts, cap, ctypes.byref(nd), ctypes.byref(st)))
         return list(counts[:nd.value]), st
 
@@ -431,8 +437,11 @@ def main():
     barrier()
     t0 = time.perf_counter()
     levels = 0
+    calls = []
     for _ in range(args.steps):
-        r = psb.bfs(puzzle, algo, 0, device=local)
+        tc = time.perf_counter()
+        r = psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio)
+        calls.append(time.perf_counter() - tc)
         assert r["counts"] == ref_counts
         levels = r["stats"]["levels"]
     torch.cuda.synchronize()
@@ -463,7 +472,9 @@ def main():
     expand_ms = sum(s.expand_ms for s in stats) / len(stats)
     achieved = alg_bytes / (expand_ms / 1000.0) / 1e9
     peak, peak_kind = load_peaks()
-    launches_per_step = st.levels * (2 if algo in ("three_bit", "classic") else 1)
+    # level kernels + one finalize per level (three-bit, classic) or one
+    # CUR -> OLD pass per bottom-up level (two-bit)
+    launches_per_step = st.levels + (st.levels if algo in ("three_bit", "classic") else st.bottom_up_levels)
 
     line = {
         "metric": f"BFS states/sec ({desc})", "value": value, "unit": "states/s", "n_gpus": world,
@@ -475,13 +486,15 @@ def main():
                    "l2": "inputs larger than L2 (bit arrays of %d MB resident in HBM)" % (st.device_bytes >> 20),
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "e2e": {"value": e2e_value, "unit": "states/s", "h2d_bytes_per_step": 8,
-                "d2h_bytes_per_step": 64 * levels + 8 * len(ref_counts)},
+                "d2h_bytes_per_step": 64 * levels + 8 * len(ref_counts),
+                "call_s": [round(c, 4) for c in calls]},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None,
                      "note": f"level kernel, {peak_kind} peak; algorithmic bytes/level = sweep + 8 B/child"},
         "kernel_ms_per_step": {"level": expand_ms, "finalize": sum(s.finalize_ms for s in stats) / len(stats)},
         "children_per_step": st.children, "local_child_fraction": st.local_children / max(st.children, 1),
+        "direction": {"mode": args.direction, "bottom_up_levels": st.bottom_up_levels, "levels": st.levels},
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline and world == 1:

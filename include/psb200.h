@@ -111,7 +111,20 @@ typedef struct {
     float* level_ms;       /* optional, counts_cap entries: entry d = device ms of the level that expanded depth d */
     uint64_t* level_children; /* optional, counts_cap entries: entry d = children generated from depth d
                               (two-bit writes one more entry, for its final empty sweep, when it fits) */
+    int32_t direction;     /* PSB_DIR_AUTO (0), PSB_DIR_TOP_DOWN or PSB_DIR_BOTTOM_UP; see below */
+    float bottom_up_ratio; /* PSB_DIR_AUTO: a dense level runs bottom-up when unvisited < ratio * frontier (0 = 1.0) */
 } psb_bfs_opts;
+
+/* Level direction.  A top-down level expands every frontier state and marks
+ * its children, as the reference does.  A bottom-up level (three-bit,
+ * two-bit and classic searches of pancakes, sliding tiles and Hanoi without
+ * symmetry) makes every still unvisited state probe its neighbours for a
+ * frontier state; on the last, dense levels of a search that is far less
+ * work.  Counts and final arrays are the same either way.  Three-bit searches
+ * that may go bottom-up keep one more bit per state (the visited set). */
+#define PSB_DIR_AUTO 0      /* top-down; bottom-up on dense levels once unvisited < ratio * frontier */
+#define PSB_DIR_TOP_DOWN 1  /* every level top-down (no visited array) */
+#define PSB_DIR_BOTTOM_UP 2 /* every level bottom-up where the search supports it (tests) */
 
 typedef struct {
     uint32_t struct_size;     /* sizeof(psb_bfs_stats) */
@@ -126,6 +139,7 @@ typedef struct {
     uint64_t local_children;  /* children marked in the block's shared-memory window */
     uint64_t expand_launches; /* level-kernel launches (one per level) */
     uint64_t device_bytes;    /* device memory held by the search */
+    uint64_t bottom_up_levels; /* levels that ran bottom-up (their "children" are probes) */
 } psb_bfs_stats;
 
 /* Size in 64-bit words of the final arrays that psb_bfs copies out:
@@ -143,7 +157,8 @@ int psb_final_words(const psb_puzzle* p, int algo, uint64_t* words);
 int psb_bfs(const psb_puzzle* p, int algo, uint64_t initial_index, const psb_bfs_opts* opts,
             uint64_t* depth_counts, uint32_t counts_cap, uint32_t* n_depths, psb_bfs_stats* stats);
 
-/* Device memory the search of psb_bfs would allocate (bytes). */
+/* Device memory the search of psb_bfs would allocate (bytes), for the
+ * default direction (PSB_DIR_AUTO). */
 int psb_bfs_footprint(const psb_puzzle* p, int algo, uint64_t* bytes);
 
 /* Reusable device state: allocate once, run many searches (benchmarks and
@@ -153,6 +168,12 @@ int psb_bfs_session_create(const psb_puzzle* p, int algo, const psb_bfs_opts* op
 int psb_bfs_session_run(psb_bfs_session* s, uint64_t initial_index, const psb_bfs_opts* opts,
                         uint64_t* depth_counts, uint32_t counts_cap, uint32_t* n_depths, psb_bfs_stats* stats);
 int psb_bfs_session_destroy(psb_bfs_session* s);
+
+/* Search arrays (psb_bfs and sessions) come from a per-device memory pool
+ * that keeps freed memory reserved for the next search instead of returning
+ * it to the driver after every call.  This returns the reserved memory of
+ * `device` (-1 = current) to the driver; it waits for the device first. */
+int psb_release_cached_memory(int device);
 
 /* --- Frontier compression (Common/FrontierCompression.cpp, StreamVInt.cpp,
  *     CompressedFrontier.cpp) -------------------------------------------------

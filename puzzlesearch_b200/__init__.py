@@ -43,7 +43,8 @@ class BfsOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
                 ("window_bits", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("stream", ctypes.c_void_p), ("final_words", u64p), ("final_cap", ctypes.c_uint64),
-                ("level_ms", ctypes.POINTER(ctypes.c_float)), ("level_children", u64p)]
+                ("level_ms", ctypes.POINTER(ctypes.c_float)), ("level_children", u64p),
+                ("direction", ctypes.c_int32), ("bottom_up_ratio", ctypes.c_float)]
 
 
 class BfsStats(ctypes.Structure):
@@ -52,7 +53,8 @@ class BfsStats(ctypes.Structure):
                 ("total_ms", ctypes.c_double), ("expand_ms", ctypes.c_double),
                 ("finalize_ms", ctypes.c_double), ("expanded", ctypes.c_uint64),
                 ("children", ctypes.c_uint64), ("local_children", ctypes.c_uint64),
-                ("expand_launches", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
+                ("expand_launches", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64),
+                ("bottom_up_levels", ctypes.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}
@@ -105,6 +107,7 @@ def lib():
         L.psb_bfs_session_run.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(BfsOpts), u64p, ctypes.c_uint32,
                                           u32p, ctypes.POINTER(BfsStats)]
         L.psb_bfs_session_destroy.argtypes = [P]
+        L.psb_release_cached_memory.argtypes = [ctypes.c_int]
         L.psb_frontier_encode.argtypes = [u64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
                                           u64p, ctypes.POINTER(CodecBlock), ctypes.c_uint32, u32p, ctypes.c_void_p]
         L.psb_frontier_index.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(CodecBlock),
@@ -264,9 +267,15 @@ def _algo(algo):
     return ALGOS[algo] if isinstance(algo, str) else int(algo)
 
 
-def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_ms=None, level_children=None):
+DIRECTIONS = {"auto": 0, "top_down": 1, "bottom_up": 2}
+
+
+def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_ms=None, level_children=None,
+          direction="auto", bottom_up_ratio=0.0):
     o = BfsOpts()
     o.struct_size = ctypes.sizeof(BfsOpts)
+    o.direction = DIRECTIONS[direction] if isinstance(direction, str) else int(direction)
+    o.bottom_up_ratio = bottom_up_ratio
     o.max_depth = max_depth
     o.window_bits = window_bits
     o.device = device
@@ -281,9 +290,11 @@ def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_
     return o
 
 
-def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels=False, device=-1):
+def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels=False, device=-1,
+        direction="auto", bottom_up_ratio=0.0):
     """Runs psb_bfs.  Returns a dict with counts, stats and optionally the final
-    arrays (list of 64-bit words in the reference's layout) and per-level data."""
+    arrays (list of 64-bit words in the reference's layout) and per-level data.
+    direction: "auto", "top_down" or "bottom_up" (PSB_DIR_*)."""
     if isinstance(initial, str):
         initial = puzzle.Parse(initial)
     cap = 1 << 16
@@ -294,7 +305,7 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
         fin = (ctypes.c_uint64 * puzzle.final_words(algo))()
     lm = (ctypes.c_float * cap)() if levels else None
     lc = (ctypes.c_uint64 * cap)() if levels else None
-    o = _opts(max_depth, window_bits, device, None, fin, lm, lc)
+    o = _opts(max_depth, window_bits, device, None, fin, lm, lc, direction, bottom_up_ratio)
     st = BfsStats()
     st.struct_size = ctypes.sizeof(BfsStats)
     _check(lib().psb_bfs(puzzle.handle, _algo(algo), initial, ctypes.byref(o), counts, cap, ctypes.byref(nd),
@@ -311,21 +322,22 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
 class BfsSession:
     """psb_bfs_session: device arrays allocated once, reused by run()."""
 
-    def __init__(self, puzzle, algo, window_bits=0, device=-1):
+    def __init__(self, puzzle, algo, window_bits=0, device=-1, direction="auto"):
         self.puzzle = puzzle
         self.algo = _algo(algo)
+        self.direction = direction
         h = ctypes.c_void_p()
-        o = _opts(0, window_bits, device)
+        o = _opts(0, window_bits, device, direction=direction)
         _check(lib().psb_bfs_session_create(puzzle.handle, self.algo, ctypes.byref(o), ctypes.byref(h)))
         self._h = h
         self._cap = 1 << 16
         self._counts = (ctypes.c_uint64 * self._cap)()
 
-    def run(self, initial=0, max_depth=0):
+    def run(self, initial=0, max_depth=0, bottom_up_ratio=0.0):
         nd = ctypes.c_uint32()
         st = BfsStats()
         st.struct_size = ctypes.sizeof(BfsStats)
-        o = _opts(max_depth)
+        o = _opts(max_depth, direction=self.direction, bottom_up_ratio=bottom_up_ratio)
         _check(lib().psb_bfs_session_run(self._h, initial, ctypes.byref(o), self._counts, self._cap,
                                          ctypes.byref(nd), ctypes.byref(st)))
         return list(self._counts[:nd.value]), st.as_dict()
@@ -459,6 +471,11 @@ class Server:
     def __del__(self):
         if _lib is not None:
             self.stop()
+
+
+def release_cached_memory(device=-1):
+    """psb_release_cached_memory: return the search arrays' reserved pool memory to the driver."""
+    _check(lib().psb_release_cached_memory(device))
 
 
 def frontier_index(data):

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -66,6 +67,85 @@ __global__ void __launch_bounds__(kThreads) finalize_classic(ulonglong2* __restr
         k.y |= n.y;
         closed[i] = k;
         c += __popcll(n.x) + __popcll(n.y);
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// Three-bit level end of a search that keeps a visited array for bottom-up
+// levels: as finalize_three_bit, plus visited |= new.  The visited array is
+// not one of the reference's arrays; old/cur/new stay bit-identical.
+__global__ void __launch_bounds__(kThreads) finalize_three_bit_visited(const ulonglong2* __restrict__ cur,
+                                                                      ulonglong2* __restrict__ nw,
+                                                                      ulonglong2* __restrict__ old,
+                                                                      ulonglong2* __restrict__ visited,
+                                                                      uint64_t n2, int odd, int zero_old,
+                                                                      unsigned long long* count) {
+    uint32_t c = 0;
+    for (uint64_t i = blockIdx.x * uint64_t(kThreads) + threadIdx.x; i < n2; i += uint64_t(gridDim.x) * kThreads) {
+        ulonglong2 n = nw[i];
+        const ulonglong2 o = old[i];
+        n.x &= ~o.x;
+        n.y &= ~o.y;
+        if (odd) {
+            const ulonglong2 k = cur[i];
+            n.x &= ~k.x;
+            n.y &= ~k.y;
+        }
+        nw[i] = n;
+        if (zero_old) old[i] = make_ulonglong2(0, 0);
+        if (n.x | n.y) {
+            ulonglong2 v = visited[i];
+            v.x |= n.x;
+            v.y |= n.y;
+            visited[i] = v;
+        }
+        c += __popcll(n.x) + __popcll(n.y);
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// Classic level end after a bottom-up level: as finalize_classic, plus the
+// clearing of `open` that the top-down sweep does (BitArray::ScanBitsAndClear).
+__global__ void __launch_bounds__(kThreads) finalize_classic_clear(ulonglong2* __restrict__ nw,
+                                                                  ulonglong2* __restrict__ closed,
+                                                                  ulonglong2* __restrict__ open, uint64_t n2,
+                                                                  unsigned long long* count) {
+    uint32_t c = 0;
+    for (uint64_t i = blockIdx.x * uint64_t(kThreads) + threadIdx.x; i < n2; i += uint64_t(gridDim.x) * kThreads) {
+        ulonglong2 n = nw[i];
+        ulonglong2 k = closed[i];
+        n.x &= ~k.x;
+        n.y &= ~k.y;
+        nw[i] = n;
+        k.x |= n.x;
+        k.y |= n.y;
+        closed[i] = k;
+        open[i] = make_ulonglong2(0, 0);
+        c += __popcll(n.x) + __popcll(n.y);
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// Two-bit level end after a bottom-up level: every CUR code becomes OLD
+// (the CUR -> OLD step of InMemoryTwoBitBFS.cpp:52-56, which the top-down
+// sweep does in place), and the CUR states are counted (the depth's count).
+__global__ void __launch_bounds__(kThreads) retire_two_bit(ulonglong2* __restrict__ codes, uint64_t n2,
+                                                          uint32_t cur_code, unsigned long long* count) {
+    uint32_t c = 0;
+    auto retire = [&](unsigned long long& w) {
+        const uint64_t hi = w & kEven, lo = (w >> 1) & kEven;
+        const uint64_t cur = hi & (cur_code == 3 ? lo : ~lo);
+        w ^= cur | (cur_code == 2 ? (cur << 1) : 0);
+        c += __popcll(cur);
+    };
+    for (uint64_t i = blockIdx.x * uint64_t(kThreads) + threadIdx.x; i < n2; i += uint64_t(gridDim.x) * kThreads) {
+        ulonglong2 w = codes[i];
+        retire(w.x);
+        retire(w.y);
+        codes[i] = w;
     }
     c = __reduce_add_sync(0xFFFFFFFFu, c);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
@@ -423,6 +503,37 @@ int psb_final_words(const psb_puzzle* p, int algo, uint64_t* words) {
 // ---------------------------------------------------------------------------
 // In-memory search session.
 // ---------------------------------------------------------------------------
+namespace {
+
+// Search arrays come from one stream-ordered memory pool per device that keeps
+// freed memory reserved (release threshold: everything), so back-to-back
+// psb_bfs calls reuse their arrays.  Mapping and unmapping gigabytes per
+// call is what cudaMalloc/cudaFree would do, and on B200 a cudaFree of a few
+// GB took from 5 to 650 ms.  psb_release_cached_memory() returns the memory.
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+
+int session_pool(int device, cudaMemPool_t* out) {
+    if (device < 0 || device >= kMaxPoolDevices) return fail(PSB_ERR_ARG, "device %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        PSB_CUDA(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = ~uint64_t(0);
+        PSB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        g_pools[device] = pool;
+    }
+    *out = g_pools[device];
+    return PSB_OK;
+}
+
+}  // namespace
+
 struct psb_bfs_session {
     psb_puzzle p;
     int algo = 0, mode = 0, device = -1, window_bits = 0;
@@ -431,17 +542,27 @@ struct psb_bfs_session {
     uint64_t* arr[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t words[4] = {0, 0, 0, 0};  // padded sizes
     int n_arr = 0;
+    uint64_t* visited = nullptr;  // three-bit searches that may run bottom-up: states at depth <= current
+    bool bottom_up = false;       // this search's algorithm and puzzle support bottom-up levels
     unsigned long long* d_stats = nullptr;
     unsigned long long* h_stats = nullptr;
     uint8_t* wflags[2] = {nullptr, nullptr};  // active-window flags (1 byte per window), double-buffered
     uint64_t n_windows = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t bytes = 0;
+    cudaMemPool_t pool = nullptr;
+
+    int alloc(void** ptr, size_t size) {  // stream-ordered, from the device's session pool
+        PSB_CUDA(cudaMallocFromPoolAsync(ptr, size, pool, stream));
+        bytes += size;
+        return PSB_OK;
+    }
 
     ~psb_bfs_session() {
-        for (auto* a : arr) if (a) cudaFree(a);
-        if (d_stats) cudaFree(d_stats);
-        for (auto* f : wflags) if (f) cudaFree(f);
+        for (auto* a : arr) if (a) cudaFreeAsync(a, stream);
+        if (visited) cudaFreeAsync(visited, stream);
+        if (d_stats) cudaFreeAsync(d_stats, stream);
+        for (auto* f : wflags) if (f) cudaFreeAsync(f, stream);
         if (h_stats) cudaFreeHost(h_stats);
         for (auto& e : ev) if (e) cudaEventDestroy(e);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -469,6 +590,20 @@ int layout(const psb_puzzle* p, int algo, uint64_t* words, int* n_arr) {
         return PSB_OK;
     }
     return fail(PSB_ERR_ARG, "unknown algorithm %d", algo);
+}
+
+// Bottom-up levels need "v has a frontier neighbour" to equal "v is a child
+// of a frontier state" on the states they scan.  That holds for the pancake,
+// sliding-tile and plain Hanoi moves, which are undone by a move of the same
+// puzzle, and it fails for Hanoi with symmetry, whose index space also holds
+// non-canonical states that expand to canonical children.  Frontier search
+// keeps no visited information.
+// Default switch ratio of PSB_DIR_AUTO (unvisited < ratio x frontier).
+constexpr double kBottomUpRatio = 1.0;
+
+bool supports_bottom_up(const psb_puzzle* p, int algo) {
+    if (algo != PSB_THREE_BIT && algo != PSB_TWO_BIT && algo != PSB_CLASSIC) return false;
+    return !(p->kind == PSB_HANOI4 && p->pz.sym);
 }
 
 // Window of 2^16 states for the permutation puzzles and 2^17 for Hanoi
@@ -510,7 +645,13 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     cudaStream_t s = S->stream;
     if (S->device >= 0) PSB_CUDA(cudaSetDevice(S->device));
     for (int i = 0; i < S->n_arr; i++) PSB_CUDA(cudaMemsetAsync(S->arr[i], 0, S->words[i] * 8, s));
+    if (S->visited) PSB_CUDA(cudaMemsetAsync(S->visited, 0, S->words[0] * 8, s));
     PSB_CUDA(cudaEventRecord(S->ev[0], s));
+    const int direction = opts ? opts->direction : PSB_DIR_AUTO;
+    const double bu_ratio = (opts && opts->bottom_up_ratio > 0) ? double(opts->bottom_up_ratio) : kBottomUpRatio;
+    // Three-bit needs its visited array; classic (closed) and two-bit (codes) carry the information.
+    const bool can_bu = S->bottom_up && direction != PSB_DIR_TOP_DOWN &&
+                        (S->algo != PSB_THREE_BIT || S->visited != nullptr);
 
     const uint64_t W1 = words_for(N), W2 = words_for(2 * N), W4 = (N + 15) / 16;
     const unsigned grid = unsigned((N + (uint64_t(1) << S->window_bits) - 1) >> S->window_bits);
@@ -529,7 +670,10 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     uint32_t cur_code = 2;
 
     switch (S->algo) {
-    case PSB_THREE_BIT: if (int rc = set_bit(cur, initial, s)) return rc; break;
+    case PSB_THREE_BIT:
+        if (int rc = set_bit(cur, initial, s)) return rc;
+        if (S->visited) if (int rc = set_bit(S->visited, initial, s)) return rc;
+        break;
     case PSB_CLASSIC:
         if (int rc = set_bit(open, initial, s)) return rc;
         if (int rc = set_bit(closed, initial, s)) return rc;
@@ -557,7 +701,9 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
 
     std::vector<uint64_t> res;
     double expand_ms = 0, finalize_ms = 0;
-    uint64_t expanded = 0, children = 0, local = 0, launches = 0;
+    uint64_t expanded = 0, children = 0, local = 0, launches = 0, bu_levels = 0;
+    uint64_t seen = 0;       // states at depth < the frontier's depth
+    uint64_t frontier = 1;   // states at the frontier's depth (two-bit: the kernel's estimate)
     const bool want_final = opts && opts->final_words;
     bool first = true;
     uint32_t iteration = 0;
@@ -569,9 +715,28 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         if (produce) PSB_CUDA(cudaMemsetAsync(S->wflags[flags_next], 0, S->n_windows, s));
         a.wflag_cur = flags_valid >= 0 ? S->wflags[flags_valid] : nullptr;
         a.wflag_next = produce ? S->wflags[flags_next] : nullptr;
+        // Direction of this level: bottom-up once the unvisited states are
+        // fewer than ratio x the frontier (they probe until a round hits; the
+        // frontier would generate every child).  Sparse frontiers stay
+        // top-down: their levels sweep only the flagged windows, while a
+        // bottom-up level sweeps every window.
+        const uint64_t unvisited = N - std::min(N, seen + frontier);
+        const bool bu = can_bu && (direction == PSB_DIR_BOTTOM_UP ||
+                                   (frontier >= sparse_limit && double(unvisited) < bu_ratio * double(frontier)));
         PSB_CUDA(cudaEventRecord(S->ev[1], s));
         uint64_t count = 0;
-        if (S->algo == PSB_FRONTIER && first) {
+        if (bu) {
+            a.wflag_cur = nullptr;
+            a.cur_code = cur_code;
+            switch (S->algo) {
+            case PSB_THREE_BIT: a.front = S->visited; a.probe = cur; a.marks = nw; a.front_words = W1; a.mark_words = W1; break;
+            case PSB_CLASSIC: a.front = closed; a.probe = open; a.marks = nopen; a.front_words = W1; a.mark_words = W1; break;
+            case PSB_TWO_BIT: a.front = codes; a.probe = codes; a.marks = codes; a.front_words = W2; a.mark_words = W2; break;
+            }
+            PSB_CUDA(P.k.level_bu[S->mode](a, grid, smem, s));
+            launches++;
+            bu_levels++;
+        } else if (S->algo == PSB_FRONTIER && first) {
             a.marks = fnext; a.excl_next = nex; a.mark_words = W4;
             PSB_CUDA(P.k.seed(a, initial, s));
         } else {
@@ -591,13 +756,26 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         if (S->algo == PSB_THREE_BIT || S->algo == PSB_CLASSIC) {
             const unsigned fgrid = 148 * 8;
             const uint64_t n2 = (W1 + 1) / 2;
-            if (S->algo == PSB_THREE_BIT)
+            if (S->algo == PSB_THREE_BIT && S->visited)
+                psb::finalize_three_bit_visited<<<fgrid, psb::kThreads, 0, s>>>(
+                    reinterpret_cast<const ulonglong2*>(cur), reinterpret_cast<ulonglong2*>(nw),
+                    reinterpret_cast<ulonglong2*>(old_), reinterpret_cast<ulonglong2*>(S->visited), n2, P.odd,
+                    want_final ? 0 : 1, S->d_stats + 4);
+            else if (S->algo == PSB_THREE_BIT)
                 psb::finalize_three_bit<<<fgrid, psb::kThreads, 0, s>>>(
                     reinterpret_cast<const ulonglong2*>(cur), reinterpret_cast<ulonglong2*>(nw),
                     reinterpret_cast<ulonglong2*>(old_), n2, P.odd, want_final ? 0 : 1, S->d_stats + 4);
+            else if (bu)
+                psb::finalize_classic_clear<<<fgrid, psb::kThreads, 0, s>>>(
+                    reinterpret_cast<ulonglong2*>(nopen), reinterpret_cast<ulonglong2*>(closed),
+                    reinterpret_cast<ulonglong2*>(open), n2, S->d_stats + 4);
             else
                 psb::finalize_classic<<<fgrid, psb::kThreads, 0, s>>>(
                     reinterpret_cast<ulonglong2*>(nopen), reinterpret_cast<ulonglong2*>(closed), n2, S->d_stats + 4);
+            PSB_CUDA(cudaGetLastError());
+        } else if (S->algo == PSB_TWO_BIT && bu) {
+            psb::retire_two_bit<<<148 * 8, psb::kThreads, 0, s>>>(reinterpret_cast<ulonglong2*>(codes), (W2 + 1) / 2,
+                                                                 cur_code, S->d_stats + 4);
             PSB_CUDA(cudaGetLastError());
         }
         PSB_CUDA(cudaEventRecord(S->ev[3], s));
@@ -633,7 +811,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             std::swap(open, nopen);
             break;
         case PSB_TWO_BIT:
-            count = S->h_stats[0];  // states found with code CUR = states at this depth
+            count = bu ? S->h_stats[4] : S->h_stats[0];  // states with code CUR = states at this depth
             if (count == 0) goto done;
             res.push_back(count);
             cur_code = 5 - cur_code;
@@ -652,6 +830,13 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         first = false;
         flags_valid = produce ? flags_next : -1;
         estimate = count;
+        if (S->algo == PSB_TWO_BIT) {  // res holds depths 0..d; the next frontier is only estimated
+            seen += count;
+            frontier = S->h_stats[5];
+        } else {                       // res holds depths 0..d+1
+            seen += res[res.size() - 2];
+            frontier = res.back();
+        }
         if (res.size() > cap) return fail(PSB_ERR_CAPACITY, "more than %u depths", cap);
     }
 done:
@@ -695,6 +880,7 @@ done:
         stats->local_children = local;
         stats->expand_launches = launches;
         stats->device_bytes = S->bytes;
+        stats->bottom_up_levels = bu_levels;
     }
     return PSB_OK;
 }
@@ -709,6 +895,7 @@ int psb_bfs_footprint(const psb_puzzle* p, int algo, uint64_t* bytes) {
     int n = 0;
     if (int rc = layout(p, algo, w, &n)) return rc;
     *bytes = (w[0] + w[1] + w[2] + w[3]) * 8 + 64;
+    if (algo == PSB_THREE_BIT && supports_bottom_up(p, algo)) *bytes += w[0] * 8;  // visited array
     return PSB_OK;
 }
 
@@ -734,16 +921,16 @@ int psb_bfs_session_create(const psb_puzzle* p, int algo, const psb_bfs_opts* op
         PSB_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
         S->own_stream = true;
     }
-    for (int i = 0; i < S->n_arr; i++) {
-        PSB_CUDA(cudaMalloc(&S->arr[i], S->words[i] * 8));
-        S->bytes += S->words[i] * 8;
-    }
+    if (int rc = session_pool(S->device, &S->pool)) return rc;
+    for (int i = 0; i < S->n_arr; i++)
+        if (int rc = S->alloc(reinterpret_cast<void**>(&S->arr[i]), S->words[i] * 8)) return rc;
+    S->bottom_up = supports_bottom_up(p, algo);
+    if (S->bottom_up && algo == PSB_THREE_BIT && !(opts && opts->direction == PSB_DIR_TOP_DOWN))
+        if (int rc = S->alloc(reinterpret_cast<void**>(&S->visited), S->words[0] * 8)) return rc;
     S->n_windows = (p->n_states + (uint64_t(1) << S->window_bits) - 1) >> S->window_bits;
-    for (auto& f : S->wflags) {
-        PSB_CUDA(cudaMalloc(&f, S->n_windows));
-        S->bytes += S->n_windows;
-    }
-    PSB_CUDA(cudaMalloc(&S->d_stats, 8 * sizeof(unsigned long long)));
+    for (auto& f : S->wflags)
+        if (int rc = S->alloc(reinterpret_cast<void**>(&f), S->n_windows)) return rc;
+    if (int rc = S->alloc(reinterpret_cast<void**>(&S->d_stats), 8 * sizeof(unsigned long long))) return rc;
     PSB_CUDA(cudaMallocHost(&S->h_stats, 8 * sizeof(unsigned long long)));
     for (auto& e : S->ev) PSB_CUDA(cudaEventCreate(&e));
     *out = S.release();
@@ -759,6 +946,21 @@ int psb_bfs_session_run(psb_bfs_session* s, uint64_t initial, const psb_bfs_opts
 
 int psb_bfs_session_destroy(psb_bfs_session* s) {
     delete s;
+    return PSB_OK;
+}
+
+int psb_release_cached_memory(int device) {
+    if (int rc = ensure_device(device)) return rc;
+    if (device < 0) PSB_CUDA(cudaGetDevice(&device));
+    if (device >= kMaxPoolDevices) return PSB_OK;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        pool = g_pools[device];
+    }
+    if (!pool) return PSB_OK;
+    PSB_CUDA(cudaDeviceSynchronize());  // frees still queued on streams return first
+    PSB_CUDA(cudaMemPoolTrimTo(pool, 0));
     return PSB_OK;
 }
 

@@ -27,4 +27,12 @@ __global__ void finalize_three_bit(const ulonglong2* __restrict__ cur, ulonglong
                                    unsigned long long* count);
 __global__ void finalize_classic(ulonglong2* __restrict__ nw, ulonglong2* __restrict__ closed, uint64_t n2,
                                  unsigned long long* count);
+// Variants used by searches that may run bottom-up levels.
+__global__ void finalize_three_bit_visited(const ulonglong2* __restrict__ cur, ulonglong2* __restrict__ nw,
+                                           ulonglong2* __restrict__ old, ulonglong2* __restrict__ visited,
+                                           uint64_t n2, int odd, int zero_old, unsigned long long* count);
+__global__ void finalize_classic_clear(ulonglong2* __restrict__ nw, ulonglong2* __restrict__ closed,
+                                       ulonglong2* __restrict__ open, uint64_t n2, unsigned long long* count);
+__global__ void retire_two_bit(ulonglong2* __restrict__ codes, uint64_t n2, uint32_t cur_code,
+                               unsigned long long* count);
 }  // namespace psb

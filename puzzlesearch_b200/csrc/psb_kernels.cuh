@@ -40,12 +40,16 @@ constexpr int kThreads = 256;  // finalize and batched-expand kernels
 
 enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 
+#ifndef PSB_BU_MIN_BLOCKS
+#define PSB_BU_MIN_BLOCKS 4
+#endif
+
 // Block shape of the level kernel per mode, chosen by a sweep on B200:
 // two-bit reads the target's code before each long-range mark, so it wants
 // more resident warps (four 256-thread blocks per SM); three-bit's marks are
 // fire-and-forget, and it runs fastest without a register cap.
 // PSB_THREADS / PSB_MIN_BLOCKS override every mode (tuning builds only).
-template <int MODE>
+template <int MODE, bool BU = false>
 struct Shape {
 #ifdef PSB_THREADS
     static constexpr int threads = PSB_THREADS;
@@ -55,7 +59,9 @@ struct Shape {
 #ifdef PSB_MIN_BLOCKS
     static constexpr int min_blocks = PSB_MIN_BLOCKS;
 #else
-    static constexpr int min_blocks = MODE == kTwoBit ? 4 : MODE == kFrontier ? 2 : 1;
+    // Bottom-up levels wait on their probe loads, so they want resident warps
+    // too, but not at the price of spills (two-bit's 64-register cap spills).
+    static constexpr int min_blocks = BU ? PSB_BU_MIN_BLOCKS : MODE == kTwoBit ? 4 : MODE == kFrontier ? 2 : 1;
 #endif
 };
 
@@ -72,31 +78,51 @@ struct PuzzleArgs {
     int sym;    // Hanoi: symmetry flag
 };
 
-// Adapters giving the three puzzles one device interface.
+// Adapters giving the three puzzles one device interface.  probe_range
+// generates the children of one bottom-up probe round: the round starting at
+// child `first` covers children first .. first+kProbeRound-1 in expansion order.
+#ifndef PSB_PROBE_ROUND
+#define PSB_PROBE_ROUND 4
+#endif
 template <int N>
 struct PancakeK {
     static constexpr int kBranch = N - 1;
     static constexpr int kOps = N - 1;
+    static constexpr int kProbeRound = PSB_PROBE_ROUND < N - 1 ? PSB_PROBE_ROUND : N - 1;
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs&, E& e) {
         Pancake<N>::template expand<kOpBits>(i, ob, e);
+    }
+    template <class E>
+    __device__ __forceinline__ static void probe_range(uint64_t i, int first, int last, const PuzzleArgs&, E& e) {
+        Pancake<N>::template expand_range<false>(i, 0u, first, last, e);
     }
 };
 template <int N>
 struct SlidingK {
     static constexpr int kBranch = 4;
     static constexpr int kOps = 4;
+    static constexpr int kProbeRound = 4;  // one round: four cheap children
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs& a, E& e) {
         Sliding<N>::template expand<kOpBits>(i, ob, a.width, e);
+    }
+    template <class E>
+    __device__ __forceinline__ static void probe_range(uint64_t i, int, int, const PuzzleArgs& a, E& e) {
+        Sliding<N>::template expand<false>(i, 0u, a.width, e);
     }
 };
 struct HanoiK {
     static constexpr int kBranch = 6;
     static constexpr int kOps = 4;
+    static constexpr int kProbeRound = 6;  // one round: six cheap children
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs& a, E& e) {
         Hanoi::template expand<kOpBits>(i, ob, a.disks, a.sym != 0, e);
+    }
+    template <class E>
+    __device__ __forceinline__ static void probe_range(uint64_t i, int, int, const PuzzleArgs& a, E& e) {
+        Hanoi::template expand<false>(i, 0u, a.disks, a.sym != 0, e);
     }
 };
 
@@ -112,9 +138,11 @@ struct LevelArgs {
     uint32_t cur_code;         // two-bit: code of the frontier (2 or 3); NEXT = 5 - CUR
     int odd;                   // frontier search: exclusion bitsets in use
     PuzzleArgs pz;
-    unsigned long long* stats;  // [0] frontier states, [1] children, [2] local children, [3] error flag
+    unsigned long long* stats;  // [0] frontier (bottom-up: unvisited) states, [1] children (probes),
+                                // [2] local children (bottom-up: found), [3] error flag, [5] two-bit next-frontier size
     const uint8_t* wflag_cur;   // optional: 1 byte per window, non-zero if the window may hold frontier states
     uint8_t* wflag_next;        // optional: set for every window that receives a mark this level
+    const uint64_t* probe;      // bottom-up levels: the frontier array the unvisited states probe
 };
 
 constexpr uint64_t kEven = 0x5555555555555555ull;
@@ -179,6 +207,7 @@ struct Emitter {
     uint8_t* wflag_next;  // optional active-window flags of the next level
     int window_bits;
     uint32_t children = 0, local = 0, bad = 0;
+    uint32_t marked = 0;  // two-bit: long-range UNVISITED -> NEXT marks issued (two lanes may mark one state)
 
     __device__ __forceinline__ void operator()(uint64_t c, uint32_t op) {
         if (c >= n_states) { bad = 1; return; }  // never expected: keeps a bad index off the memory system
@@ -203,10 +232,41 @@ struct Emitter {
             if (((v >> sh) & 3u) == 0) {  // UNVISITED -> NEXT
                 if (wflag_next) wflag_next[c >> window_bits] = 1;
                 atomicOr(w, (unsigned long long)next_pat << sh);
+                ++marked;
             }
         } else {
             if (wflag_next) wflag_next[c >> window_bits] = 1;
             atomicOr(reinterpret_cast<unsigned int*>(gmarks) + (c >> 5), 1u << (uint32_t(c) & 31u));
+        }
+    }
+};
+
+// Bottom-up probe of one round: each child of an unvisited state that is in
+// the frontier (three-bit `cur`, classic `open`: one bit per state; two-bit:
+// code CUR) is a hit.  The probes of a round are independent loads, issued
+// back to back; the state leaves the rounds at its first round with a hit.
+// All three puzzles have symmetric moves (a flip, a slide or a disk move is
+// undone by a move of the same puzzle), so "v has a frontier neighbour"
+// equals "v is a child of a frontier state".
+template <int MODE>
+struct Probe {
+    const uint64_t* front;
+    uint64_t n_states;
+    uint32_t cur_pat;  // two-bit: bits of the CUR code (hi at bit 0, lo at bit 1)
+    bool hit = false;
+    uint32_t probes = 0, bad = 0;
+
+    __device__ __forceinline__ void operator()(uint64_t c, uint32_t) {
+        if (c >= n_states) { bad = 1; return; }
+        ++probes;
+        if constexpr (MODE == kTwoBit) {
+            // Plain load: other blocks set NEXT bits in these words meanwhile,
+            // which never changes a CUR code.
+            const uint64_t w = front[c >> 5];
+            hit |= ((w >> (2u * (uint32_t(c) & 31u))) & 3u) == cur_pat;
+        } else {
+            const uint64_t w = __ldg(front + (c >> 6));  // read-only during a bottom-up level
+            hit |= ((w >> (uint32_t(c) & 63u)) & 1u) != 0;
         }
     }
 };
@@ -229,9 +289,20 @@ struct WindowShared {
 // the block take part; smem64 is the block's dynamic shared memory.  The
 // function ends with a block barrier, so a persistent kernel can call it for
 // window after window.
-template <class PZ, int MODE, int KTHREADS>
+//
+// Bottom-up levels (BU = true; three-bit, classic and two-bit) turn the
+// roles around: the sweep reads the visited information (three-bit: its
+// visited array, classic: `closed`, two-bit: codes != UNVISITED), the list
+// holds the window's UNVISITED states, and each probes its neighbours for a
+// frontier state (Probe).  Found states are marked in the shared bitmap of
+// their own window and flushed exactly as top-down marks are.  The probed
+// arrays do not change during the level: two-bit's CUR -> OLD step runs
+// afterwards (retire_two_bit), classic's clearing of `open` in
+// finalize_classic_clear.
+template <class PZ, int MODE, int KTHREADS, bool BU = false>
 __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window, unsigned long long* smem64,
                                              WindowShared& sh) {
+    static_assert(!BU || MODE != kFrontier, "frontier search keeps no visited information");
     constexpr int kThreads = KTHREADS;
     constexpr int kWarps = kThreads / 32;
     constexpr uint32_t kSPU = states_per_unit(MODE);
@@ -241,7 +312,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     const uint32_t W = 1u << a.window_bits;
     const uint64_t base = window << a.window_bits;
     if (base >= a.n_states) return;
-    if (a.wflag_cur && !a.wflag_cur[window]) return;  // no frontier state can be in this window
+    if (!BU && a.wflag_cur && !a.wflag_cur[window]) return;  // no frontier state can be in this window
     const uint64_t remaining = a.n_states - base;
     const uint32_t span = remaining < W ? uint32_t(remaining) : W;
     const uint32_t units = (span + kSPU - 1) / kSPU;
@@ -261,6 +332,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     Emitter<MODE> em{base, W, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u), a.wflag_next,
                      a.window_bits};
     uint32_t found = 0;
+    uint32_t probes = 0, hits = 0, pbad = 0;  // bottom-up counters
 
     // Each warp takes chunks on its own (its first chunk is its warp index,
     // later ones come from a shared counter): lane l sweeps unit 32*chunk + l,
@@ -287,7 +359,17 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
         load(nch, nw);
         const uint32_t u = ch * 32 + uint32_t(lane);
         uint64_t pmask = 0;
-        if (u < units) {
+        if (BU && u < units) {
+            // Unvisited states of the unit, restricted to indexes < n_states.
+            const uint32_t left = span - u * kSPU;  // >= 1
+            if constexpr (MODE == kTwoBit) {
+                const uint64_t w = cw[0];
+                pmask = gather_even(~(w | (w >> 1)) & kEven);
+            } else {
+                pmask = ~cw[0];
+            }
+            if (left < kSPU) pmask &= (uint64_t(1) << left) - 1u;
+        } else if (u < units) {
             if constexpr (MODE == kThreeBit) {
                 pmask = cw[0];
             } else if constexpr (MODE == kClassic) {
@@ -317,6 +399,16 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
         }
         const uint32_t cnt = __popcll(pmask);
         found += cnt;
+        auto entry_of = [&](uint32_t j) -> Entry {
+            const uint32_t ub = uint32_t(lane) * kSPU;
+            if constexpr (MODE == kFrontier) {
+                const uint64_t word = j < 16 ? cw[0 % kWPU] : j < 32 ? cw[1 % kWPU] : j < 48 ? cw[2 % kWPU] : cw[3 % kWPU];
+                const uint32_t bits = uint32_t(word >> (4 * (j & 15))) & 15u;
+                return Entry((ub + j) | (bits << 16));
+            } else {
+                return Entry(ub + j);
+            }
+        };
         uint32_t incl = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -326,20 +418,52 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
         if (total) {
             uint32_t off = incl - cnt;
-            const uint32_t ub = uint32_t(lane) * kSPU;
             while (pmask) {
                 const uint32_t j = __ffsll((long long)pmask) - 1;
                 pmask &= pmask - 1;
-                if constexpr (MODE == kFrontier) {
-                    const uint64_t word = j < 16 ? cw[0 % kWPU] : j < 32 ? cw[1 % kWPU] : j < 48 ? cw[2 % kWPU] : cw[3 % kWPU];
-                    const uint32_t bits = uint32_t(word >> (4 * (j & 15))) & 15u;
-                    wlist[off++] = Entry((ub + j) | (bits << 16));
-                } else {
-                    wlist[off++] = Entry(ub + j);
-                }
+                wlist[off++] = entry_of(j);
             }
             __syncwarp();
             const uint64_t cbase = base + uint64_t(ch) * kChunk;
+            if constexpr (BU) {
+                // Probe rounds: the round starting at child `first` probes
+                // children first .. first+R-1 of every state still listed;
+                // states with a hit are marked, the rest are compacted in
+                // place (ballot) for the next round, so every round keeps all
+                // lanes busy whatever the hit pattern.
+                constexpr int R = PZ::kProbeRound;
+                const uint32_t cur_pat = a.cur_code == 2 ? 1u : 3u;
+                uint32_t left = total;
+                for (int first = 0; first < PZ::kBranch && left; first += R) {
+                    uint32_t kept = 0;
+                    for (uint32_t e0 = 0; e0 < left; e0 += 32) {
+                        const uint32_t e = e0 + uint32_t(lane);
+                        bool miss = false;
+                        Entry entry = 0;
+                        if (e < left) {
+                            entry = wlist[e];
+                            const uint32_t o = uint32_t(ch) * kChunk + entry;  // offset in the window
+                            Probe<MODE> pr{a.probe, a.n_states, cur_pat};
+                            PZ::probe_range(base + o, first, first + R, a.pz, pr);
+                            probes += pr.probes;
+                            pbad |= pr.bad;
+                            if (pr.hit) {
+                                ++hits;
+                                if constexpr (kByteMarks) reinterpret_cast<uint8_t*>(smarks)[o] = 1;
+                                else atomicOr(&smarks[o >> 5], 1u << (o & 31u));
+                            } else {
+                                miss = true;
+                            }
+                        }
+                        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, miss);
+                        // kept <= e0: the writes only reach entries this step has read
+                        if (miss) wlist[kept + __popc(bal & ((1u << lane) - 1u))] = entry;
+                        kept += __popc(bal);
+                        __syncwarp();
+                    }
+                    left = kept;
+                }
+            } else
             for (uint32_t e = uint32_t(lane); e < total; e += 32) {
                 if constexpr (MODE == kFrontier) {
                     const uint32_t v = wlist[e];
@@ -354,10 +478,11 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
         for (int q = 0; q < kWPU; ++q) cw[q] = nw[q];
         ch = nch;
     }
-    if (found) sh.any = 1;
+    if (BU ? hits != 0 : found != 0) sh.any = 1;
     __syncthreads();
 
     // Flush the window's shared-memory marks (only if it had frontier states).
+    uint32_t fresh = 0;  // two-bit: states this flush moves from UNVISITED to NEXT
     if (sh.any) {
         if (a.wflag_next && tid == 0) a.wflag_next[window] = 1;
         if constexpr (MODE == kTwoBit) {
@@ -369,7 +494,10 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 const uint64_t w = __ldcg(codes + i);
                 const uint64_t unvisited = ~(w | (w >> 1)) & kEven;
                 const uint64_t m = spread_even(v) & unvisited;
-                if (m) atomicOr(codes + i, (unsigned long long)(m | ((next_pat & 2u) ? (m << 1) : 0)));
+                if (m) {
+                    atomicOr(codes + i, (unsigned long long)(m | ((next_pat & 2u) ? (m << 1) : 0)));
+                    fresh += __popcll(m);
+                }
             }
         } else {
             constexpr uint32_t kShift = MODE == kFrontier ? 4 : 6;  // states per 64-bit word: 16 or 64
@@ -389,10 +517,15 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
 
     // Counters: one atomic per warp and counter.
     uint32_t c0 = __reduce_add_sync(0xFFFFFFFFu, found);
-    uint32_t c1 = __reduce_add_sync(0xFFFFFFFFu, em.children);
-    uint32_t c2 = __reduce_add_sync(0xFFFFFFFFu, em.local);
-    uint32_t c3 = __reduce_or_sync(0xFFFFFFFFu, em.bad);
+    uint32_t c1 = __reduce_add_sync(0xFFFFFFFFu, BU ? probes : em.children);
+    uint32_t c2 = __reduce_add_sync(0xFFFFFFFFu, BU ? hits : em.local);
+    uint32_t c3 = __reduce_or_sync(0xFFFFFFFFu, BU ? pbad : em.bad);
+    // Two-bit: size of the next frontier (exact for bottom-up levels, an
+    // upper estimate otherwise); steers the choice of the next direction.
+    uint32_t c5 = 0;
+    if constexpr (MODE == kTwoBit) c5 = __reduce_add_sync(0xFFFFFFFFu, BU ? hits : em.marked + fresh);
     if (lane == 0) {
+        if (c5) atomicAdd(&a.stats[5], (unsigned long long)c5);
         if (c0) atomicAdd(&a.stats[0], (unsigned long long)c0);
         if (c1) atomicAdd(&a.stats[1], (unsigned long long)c1);
         if (c2) atomicAdd(&a.stats[2], (unsigned long long)c2);
@@ -401,11 +534,11 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     __syncthreads();  // the shared marks and lists may be reused for another window
 }
 
-template <class PZ, int MODE>
-__global__ void __launch_bounds__(Shape<MODE>::threads, Shape<MODE>::min_blocks) level_kernel(LevelArgs a) {
+template <class PZ, int MODE, bool BU = false>
+__global__ void __launch_bounds__(Shape<MODE, BU>::threads, Shape<MODE, BU>::min_blocks) level_kernel(LevelArgs a) {
     extern __shared__ __align__(16) unsigned long long smem64[];
     __shared__ WindowShared sh;
-    level_window<PZ, MODE, Shape<MODE>::threads>(a, blockIdx.x, smem64, sh);
+    level_window<PZ, MODE, Shape<MODE, BU>::threads, BU>(a, blockIdx.x, smem64, sh);
 }
 
 // Level 0 of frontier search (InMemoryFrontierSearch.cpp:81-88): expand the
@@ -472,18 +605,19 @@ using ExpandLaunch = cudaError_t (*)(const uint64_t*, const uint32_t*, uint64_t,
                                      PuzzleArgs, unsigned long long*, bool, cudaStream_t);
 
 struct PuzzleKernels {
-    LevelLaunch level[4];  // indexed by Mode
+    LevelLaunch level[4];     // indexed by Mode
+    LevelLaunch level_bu[4];  // bottom-up levels, indexed by Mode (none for frontier search)
     SeedLaunch seed;
     ExpandLaunch expand;
     int branching;
 };
 
-template <class PZ, int MODE>
+template <class PZ, int MODE, bool BU = false>
 cudaError_t launch_level(const LevelArgs& a, unsigned grid, size_t smem, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(level_kernel<PZ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(level_kernel<PZ, MODE, BU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(smem));
     if (e != cudaSuccess) return e;
-    level_kernel<PZ, MODE><<<grid, Shape<MODE>::threads, smem, s>>>(a);
+    level_kernel<PZ, MODE, BU><<<grid, Shape<MODE, BU>::threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -515,6 +649,10 @@ PuzzleKernels make_kernels() {
     k.level[kClassic] = &launch_level<PZ, kClassic>;
     k.level[kTwoBit] = &launch_level<PZ, kTwoBit>;
     k.level[kFrontier] = &launch_level<PZ, kFrontier>;
+    k.level_bu[kThreeBit] = &launch_level<PZ, kThreeBit, true>;
+    k.level_bu[kClassic] = &launch_level<PZ, kClassic, true>;
+    k.level_bu[kTwoBit] = &launch_level<PZ, kTwoBit, true>;
+    k.level_bu[kFrontier] = nullptr;
     k.seed = &launch_seed<PZ>;
     k.expand = &launch_expand<PZ>;
     k.branching = PZ::kBranch;

@@ -101,6 +101,13 @@ struct Pancake {
 
     template <bool kOpBits, class Emit>
     __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, Emit& emit) {
+        expand_range<kOpBits>(index, opbits, 0, N - 1, emit);
+    }
+
+    // Only the children with operator in [first, last) (bottom-up probe rounds).
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void expand_range(uint64_t index, uint32_t opbits, int first, int last,
+                                                        Emit& emit) {
         uint32_t d[N], v[N];
         perm_digits<N>(index, d);
         perm_values<N>(d, v);
@@ -112,7 +119,8 @@ struct Pancake {
         for (int m = 2; m <= N; ++m) {
             low += uint64_t(d[N - m]) * fact(m - 1);
             const int op = m - 2;
-            if (kOpBits && (opbits >> op) & 1u) continue;
+            if (op >= last) return;
+            if (op < first || (kOpBits && (opbits >> op) & 1u)) continue;
             uint32_t seen = bit[N - m];
             uint64_t s;
             if (m <= 12) {  // m is a compile-time constant after unrolling; low_m < m! <= 12! < 2^32

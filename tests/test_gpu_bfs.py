@@ -151,7 +151,7 @@ def test_session_reuse_and_starts():
 
 def test_stats_are_consistent():
     p = psb.PancakeSimple(11)
-    r = psb.bfs(p, "three_bit", 0, levels=True)
+    r = psb.bfs(p, "three_bit", 0, levels=True, direction="top_down")
     st = r["stats"]
     assert st["expanded"] == math.factorial(11)
     assert st["children"] == 10 * math.factorial(11)
@@ -164,3 +164,16 @@ def test_trivial_puzzles():
     assert psb.bfs(psb.PancakeSimple(2), "three_bit", 0)["counts"] == [1, 1]
     assert psb.bfs(psb.FourPegHanoiSimple(1), "two_bit", 0)["counts"] == [1, 3]
     assert psb.bfs(psb.SlidingTilePuzzleSimple(2, 1), "classic", 0)["counts"] == [1, 1]
+
+
+def test_pool_reuse_and_release():
+    """Back-to-back searches reuse the pooled arrays (same results); releasing
+    the pool between searches changes nothing either."""
+    p = psb.PancakeSimple(10)
+    expect = O.bfs(["pancake", 10, 0], "three_bit")[0]
+    for _ in range(3):
+        assert psb.bfs(p, "three_bit", 0)["counts"] == expect
+    psb.release_cached_memory()
+    assert psb.bfs(p, "three_bit", 0)["counts"] == expect
+    assert psb.bfs(p, "two_bit", 0)["counts"] == expect
+    psb.release_cached_memory(0)
