@@ -199,7 +199,7 @@ __host__ __device__ constexpr size_t list_entry_bytes(int mode) { return mode ==
 template <int MODE>
 struct Emitter {
     uint64_t base;        // first state of the block's window
-    uint32_t span;        // states in the window
+    uint32_t span;        // states of the window below n_states
     uint32_t* smarks;     // shared-memory window marks
     uint64_t* gmarks;     // global mark array
     uint64_t n_states;
@@ -207,22 +207,25 @@ struct Emitter {
     uint8_t* wflag_next;  // optional active-window flags of the next level
     int window_bits;
     uint32_t children = 0, local = 0, bad = 0;
-    uint32_t marked = 0;  // two-bit: long-range UNVISITED -> NEXT marks issued (two lanes may mark one state)
+    uint32_t marked = 0;      // two-bit: long-range UNVISITED -> NEXT marks issued (two lanes may mark one state)
+    uint32_t parent_off = 0;  // offset of the parent being expanded in the window (rel)
 
-    __device__ __forceinline__ void operator()(uint64_t c, uint32_t op) {
+    __device__ __forceinline__ void mark_local(uint32_t o, uint32_t op) {
+        ++children;
+        ++local;
+        if constexpr (MODE == kFrontier) {
+            atomicOr(&smarks[o >> 3], 1u << (4 * (o & 7u) + op));
+        } else if constexpr (kByteMarks) {
+            reinterpret_cast<uint8_t*>(smarks)[o] = 1;
+        } else {
+            atomicOr(&smarks[o >> 5], 1u << (o & 31u));
+        }
+    }
+
+    __device__ __forceinline__ void mark_remote(uint64_t c, uint32_t op) {
         if (c >= n_states) { bad = 1; return; }  // never expected: keeps a bad index off the memory system
         ++children;
-        const uint64_t o = c - base;
-        if (o < span) {
-            ++local;
-            if constexpr (MODE == kFrontier) {
-                atomicOr(&smarks[o >> 3], 1u << (4 * (uint32_t(o) & 7u) + op));
-            } else if constexpr (kByteMarks) {
-                reinterpret_cast<uint8_t*>(smarks)[o] = 1;
-            } else {
-                atomicOr(&smarks[o >> 5], 1u << (uint32_t(o) & 31u));
-            }
-        } else if constexpr (MODE == kFrontier) {
+        if constexpr (MODE == kFrontier) {
             if (wflag_next) wflag_next[c >> window_bits] = 1;
             atomicOr(reinterpret_cast<unsigned int*>(gmarks) + (c >> 3), 1u << (4 * (uint32_t(c) & 7u) + op));
         } else if constexpr (MODE == kTwoBit) {
@@ -238,6 +241,19 @@ struct Emitter {
             if (wflag_next) wflag_next[c >> window_bits] = 1;
             atomicOr(reinterpret_cast<unsigned int*>(gmarks) + (c >> 5), 1u << (uint32_t(c) & 31u));
         }
+    }
+
+    __device__ __forceinline__ void operator()(uint64_t c, uint32_t op) {
+        const uint64_t o = c - base;
+        if (o < span) mark_local(uint32_t(o), op);
+        else mark_remote(c, op);
+    }
+
+    // Child = parent + delta, with the parent at parent_off in the window.
+    __device__ __forceinline__ void rel(uint64_t parent, int32_t delta, uint32_t op) {
+        const uint32_t o = parent_off + uint32_t(delta);
+        if (o < span) mark_local(o, op);
+        else mark_remote(parent + int64_t(delta), op);
     }
 };
 
@@ -329,7 +345,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     }
     __syncthreads();
 
-    Emitter<MODE> em{base, W, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u), a.wflag_next,
+    Emitter<MODE> em{base, span, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u), a.wflag_next,
                      a.window_bits};
     uint32_t found = 0;
     uint32_t probes = 0, hits = 0, pbad = 0;  // bottom-up counters
@@ -467,8 +483,10 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
             for (uint32_t e = uint32_t(lane); e < total; e += 32) {
                 if constexpr (MODE == kFrontier) {
                     const uint32_t v = wlist[e];
+                    em.parent_off = ch * kChunk + (v & 0xFFFFu);
                     PZ::template expand<true>(cbase + (v & 0xFFFFu), v >> 16, a.pz, em);
                 } else {
+                    em.parent_off = ch * kChunk + wlist[e];
                     PZ::template expand<false>(cbase + wlist[e], 0u, a.pz, em);
                 }
             }

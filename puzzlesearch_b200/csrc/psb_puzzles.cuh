@@ -16,10 +16,19 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 namespace psb {
 
 constexpr uint64_t kInvalidIndex = ~uint64_t(0);  // Common/Puzzle.h:19
+
+// Emitters with a member rel(parent, delta, op) take a child given as its
+// parent's index plus a signed 32-bit delta (see Pancake); others get the
+// child's index.
+template <class E, class = void>
+struct EmitRel : std::false_type {};
+template <class E>
+struct EmitRel<E, decltype(void(&E::rel))> : std::true_type {};
 
 __host__ __device__ constexpr uint64_t fact(int k) { return k <= 1 ? 1 : uint64_t(k) * fact(k - 1); }
 constexpr uint32_t kF12 = 479001600u;  // 12!
@@ -105,44 +114,53 @@ struct Pancake {
     }
 
     // Only the children with operator in [first, last) (bottom-up probe rounds).
+    //
+    // Rank of the child of flip m: with pre = the values left of the suffix
+    // (positions < n-m) and pb[j] = the values left of position j that are
+    // smaller than v[j], the count above is popc(pb[j] & ~pre).  For m <= 12
+    // every quantity is below 12! < 2^31, so the child is passed to emitters
+    // that take it (EmitRel) as the parent plus a 32-bit signed delta.
     template <bool kOpBits, class Emit>
     __device__ __forceinline__ static void expand_range(uint64_t index, uint32_t opbits, int first, int last,
                                                         Emit& emit) {
         uint32_t d[N], v[N];
         perm_digits<N>(index, d);
         perm_values<N>(d, v);
-        uint32_t below[N], bit[N];
+        uint32_t pre[N], pb[N];
+        uint32_t acc = 0;
 #pragma unroll
-        for (int i = 0; i < N; ++i) { bit[i] = 1u << v[i]; below[i] = bit[i] - 1u; }
-        uint64_t low = d[N - 1];  // low_1 = d_{n-1} * 0! (always 0)
+        for (int i = 0; i < N; ++i) {
+            pre[i] = acc;
+            pb[i] = acc & ((1u << v[i]) - 1u);
+            acc |= 1u << v[i];
+        }
+        uint32_t low32 = 0;  // low_m for m <= 12 (d[n-1] is always 0)
+        uint64_t low64 = 0;  // low_m for m > 12
 #pragma unroll
         for (int m = 2; m <= N; ++m) {
-            low += uint64_t(d[N - m]) * fact(m - 1);
+            if (m <= 12) low32 += d[N - m] * uint32_t(fact(m - 1));
+            else low64 = (m == 13 ? uint64_t(low32) : low64) + uint64_t(d[N - m]) * fact(m - 1);
             const int op = m - 2;
             if (op >= last) return;
             if (op < first || (kOpBits && (opbits >> op) & 1u)) continue;
-            uint32_t seen = bit[N - m];
-            uint64_t s;
-            if (m <= 12) {  // m is a compile-time constant after unrolling; low_m < m! <= 12! < 2^32
+            const uint32_t excl = pre[N - m];
+            if (m <= 12) {  // m is a compile-time constant after unrolling
                 uint32_t s32 = 0;
 #pragma unroll
-                for (int q = 1; q < m; ++q) {
-                    s32 += uint32_t(fact(q)) * __popc(seen & below[N - m + q]);
-                    seen |= bit[N - m + q];
-                }
-                s = s32;
+                for (int q = 1; q < m; ++q) s32 += uint32_t(fact(q)) * __popc(pb[N - m + q] & ~excl);
+                const int32_t delta = int32_t(s32 - low32);
+                if constexpr (EmitRel<Emit>::value) emit.rel(index, delta, uint32_t(op));
+                else emit(index + int64_t(delta), uint32_t(op));
             } else {
                 uint32_t s32 = 0, t = 0;
 #pragma unroll
                 for (int q = 1; q < m; ++q) {
-                    const uint32_t c = __popc(seen & below[N - m + q]);
+                    const uint32_t c = __popc(pb[N - m + q] & ~excl);
                     if (q < 12) s32 += uint32_t(fact(q)) * c;
                     else t += uint32_t(fact(q) / kF12) * c;
-                    seen |= bit[N - m + q];
                 }
-                s = uint64_t(t) * kF12 + s32;
+                emit(index - low64 + (uint64_t(t) * kF12 + s32), uint32_t(op));
             }
-            emit(index - low + s, uint32_t(op));
         }
     }
 };
