@@ -40,6 +40,12 @@ constexpr int kThreads = 256;  // finalize and batched-expand kernels
 
 enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 
+#ifndef PSB_PAIR_WORDS
+#define PSB_PAIR_WORDS 1
+#endif
+#ifndef PSB_TD_MIN_BLOCKS
+#define PSB_TD_MIN_BLOCKS 1
+#endif
 #ifndef PSB_BU_MIN_BLOCKS
 #define PSB_BU_MIN_BLOCKS 4
 #endif
@@ -61,7 +67,8 @@ struct Shape {
 #else
     // Bottom-up levels wait on their probe loads, so they want resident warps
     // too, but not at the price of spills (two-bit's 64-register cap spills).
-    static constexpr int min_blocks = BU ? PSB_BU_MIN_BLOCKS : MODE == kTwoBit ? 4 : MODE == kFrontier ? 2 : 1;
+    static constexpr int min_blocks = BU ? PSB_BU_MIN_BLOCKS : MODE == kTwoBit ? 4 : MODE == kFrontier ? 2
+                                                                                : PSB_TD_MIN_BLOCKS;
 #endif
 };
 
@@ -84,14 +91,23 @@ struct PuzzleArgs {
 #ifndef PSB_PROBE_ROUND
 #define PSB_PROBE_ROUND 4
 #endif
+// kPairOp0: operator 0 maps state i to i ^ 1 (the pancake flip of the last
+// two values only toggles the lowest Lehmer digit, of weight 1!), so a level
+// kernel can mark those children for a whole frontier word at once and expand
+// the rest with expand_from<1>.
 template <int N>
 struct PancakeK {
     static constexpr int kBranch = N - 1;
     static constexpr int kOps = N - 1;
     static constexpr int kProbeRound = PSB_PROBE_ROUND < N - 1 ? PSB_PROBE_ROUND : N - 1;
+    static constexpr bool kPairOp0 = true;
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs&, E& e) {
         Pancake<N>::template expand<kOpBits>(i, ob, e);
+    }
+    template <int F, class E>
+    __device__ __forceinline__ static void expand_from(uint64_t i, const PuzzleArgs&, E& e) {
+        Pancake<N>::template expand_range<false>(i, 0u, F, N - 1, e);
     }
     template <class E>
     __device__ __forceinline__ static void probe_range(uint64_t i, int first, int last, const PuzzleArgs&, E& e) {
@@ -103,6 +119,7 @@ struct SlidingK {
     static constexpr int kBranch = 4;
     static constexpr int kOps = 4;
     static constexpr int kProbeRound = 4;  // one round: four cheap children
+    static constexpr bool kPairOp0 = false;
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs& a, E& e) {
         Sliding<N>::template expand<kOpBits>(i, ob, a.width, e);
@@ -116,6 +133,7 @@ struct HanoiK {
     static constexpr int kBranch = 6;
     static constexpr int kOps = 4;
     static constexpr int kProbeRound = 6;  // one round: six cheap children
+    static constexpr bool kPairOp0 = false;
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs& a, E& e) {
         Hanoi::template expand<kOpBits>(i, ob, a.disks, a.sym != 0, e);
@@ -319,6 +337,8 @@ template <class PZ, int MODE, int KTHREADS, bool BU = false>
 __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window, unsigned long long* smem64,
                                              WindowShared& sh) {
     static_assert(!BU || MODE != kFrontier, "frontier search keeps no visited information");
+    // Operator-0 children marked per frontier word in the sweep (see PancakeK).
+    constexpr bool kPairs = PSB_PAIR_WORDS && PZ::kPairOp0 && MODE != kFrontier && !BU && !kByteMarks;
     constexpr int kThreads = KTHREADS;
     constexpr int kWarps = kThreads / 32;
     constexpr uint32_t kSPU = states_per_unit(MODE);
@@ -413,6 +433,21 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 }
             }
         }
+        if constexpr (kPairs) {
+            // children i ^ 1 of the unit's frontier states: swap adjacent bits
+            const uint64_t pairs = ((pmask & kEven) << 1) | ((pmask >> 1) & kEven);
+            if (pairs) {
+                if constexpr (kSPU == 64) {
+                    if (uint32_t(pairs)) atomicOr(&smarks[2 * u], uint32_t(pairs));
+                    if (uint32_t(pairs >> 32)) atomicOr(&smarks[2 * u + 1], uint32_t(pairs >> 32));
+                } else {
+                    atomicOr(&smarks[u], uint32_t(pairs));
+                }
+                const uint32_t np = __popcll(pairs);
+                em.children += np;
+                em.local += np;
+            }
+        }
         const uint32_t cnt = __popcll(pmask);
         found += cnt;
         auto entry_of = [&](uint32_t j) -> Entry {
@@ -487,7 +522,8 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                     PZ::template expand<true>(cbase + (v & 0xFFFFu), v >> 16, a.pz, em);
                 } else {
                     em.parent_off = ch * kChunk + wlist[e];
-                    PZ::template expand<false>(cbase + wlist[e], 0u, a.pz, em);
+                    if constexpr (kPairs) PZ::template expand_from<1>(cbase + wlist[e], a.pz, em);
+                    else PZ::template expand<false>(cbase + wlist[e], 0u, a.pz, em);
                 }
             }
             __syncwarp();
