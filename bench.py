@@ -24,6 +24,7 @@ import ctypes
 import json
 import math
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -108,6 +109,16 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def level_traffic(workload):
+    """DRAM bytes per level-kernel launch from the committed ncu launch list
+    (mean over one search's launches), or None for workloads without one."""
+    path = os.path.join(REPO, "profiles", f"level_kernel_{workload.replace('-', '_')}_launches.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic bytes per level launch: (\d+)", open(path).read())
+    return int(m.group(1)) if m else None
 
 
 def dist_setup(n_gpus):
@@ -472,6 +483,7 @@ def main():
     expand_ms = sum(s.expand_ms for s in stats) / len(stats)
     achieved = alg_bytes / (expand_ms / 1000.0) / 1e9
     peak, peak_kind = load_peaks()
+    traffic = level_traffic(args.workload) if args.direction == "auto" else None
     # level kernels + one finalize per level (three-bit, classic) or one
     # CUR -> OLD pass per bottom-up level (two-bit)
     launches_per_step = st.levels + (st.levels if algo in ("three_bit", "classic") else st.bottom_up_levels)
@@ -490,8 +502,10 @@ def main():
                 "call_s": [round(c, 4) for c in calls]},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "note": f"level kernel, {peak_kind} peak; algorithmic bytes/level = sweep + 8 B/child"},
+                     "frac": achieved / peak, "traffic": traffic,
+                     "note": f"level kernel (top-down and bottom-up launches), {peak_kind} peak; algorithmic bytes"
+                             " per level = N/8 sweep + 8 B per child generated or probe issued; traffic = ncu DRAM"
+                             " read+write bytes per level launch (profiles/level_kernel_pancake13_3bit_launches.md)"},
         "kernel_ms_per_step": {"level": expand_ms, "finalize": sum(s.finalize_ms for s in stats) / len(stats)},
         "children_per_step": st.children, "local_child_fraction": st.local_children / max(st.children, 1),
         "direction": {"mode": args.direction, "bottom_up_levels": st.bottom_up_levels, "levels": st.levels},
