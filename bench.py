@@ -444,6 +444,10 @@ def main():
     value = world * args.steps * states_per_step / (elapsed_ms / 1000.0)
 
     # e2e: the public C-ABI entry point, host in/out, allocation included.
+    # Untimed warm-up calls first, as for the device loop: the first call
+    # grows the library's memory pool.
+    for _ in range(args.warmup):
+        psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()

@@ -106,6 +106,48 @@ __global__ void __launch_bounds__(kThreads) finalize_three_bit_visited(const ulo
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
 }
 
+// Three-bit level end of a sparse level, window by window: only windows
+// flagged in new_flags can hold new states, and only windows flagged in
+// old_flags (NULL: none) can hold old states, which are zeroed for reuse.
+// Same result as finalize_three_bit(_visited) with zero_old = 1.
+__global__ void __launch_bounds__(kThreads) finalize_three_bit_flagged(
+    const ulonglong2* __restrict__ cur, ulonglong2* __restrict__ nw, ulonglong2* __restrict__ old,
+    ulonglong2* __restrict__ visited, uint64_t n2, const uint8_t* __restrict__ new_flags,
+    const uint8_t* __restrict__ old_flags, uint64_t n_windows, uint32_t per_window, int odd,
+    unsigned long long* count) {
+    uint32_t c = 0;
+    for (uint64_t w = blockIdx.x; w < n_windows; w += gridDim.x) {
+        const bool fn = new_flags[w] != 0;
+        const bool fo = old_flags && old_flags[w] != 0;
+        if (!fn && !fo) continue;
+        const uint64_t i0 = w * per_window, i1 = i0 + per_window < n2 ? i0 + per_window : n2;
+        for (uint64_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
+            if (fn) {
+                ulonglong2 n = nw[i];
+                const ulonglong2 o = old[i];
+                n.x &= ~o.x;
+                n.y &= ~o.y;
+                if (odd) {
+                    const ulonglong2 k = cur[i];
+                    n.x &= ~k.x;
+                    n.y &= ~k.y;
+                }
+                nw[i] = n;
+                if (visited && (n.x | n.y)) {
+                    ulonglong2 v = visited[i];
+                    v.x |= n.x;
+                    v.y |= n.y;
+                    visited[i] = v;
+                }
+                c += __popcll(n.x) + __popcll(n.y);
+            }
+            if (fo) old[i] = make_ulonglong2(0, 0);
+        }
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
 // Classic level end after a bottom-up level: as finalize_classic, plus the
 // clearing of `open` that the top-down sweep does (BitArray::ScanBitsAndClear).
 __global__ void __launch_bounds__(kThreads) finalize_classic_clear(ulonglong2* __restrict__ nw,
@@ -546,7 +588,7 @@ struct psb_bfs_session {
     bool bottom_up = false;       // this search's algorithm and puzzle support bottom-up levels
     unsigned long long* d_stats = nullptr;
     unsigned long long* h_stats = nullptr;
-    uint8_t* wflags[2] = {nullptr, nullptr};  // active-window flags (1 byte per window), double-buffered
+    uint8_t* wflags[3] = {nullptr, nullptr, nullptr};  // active-window flags (1 byte per window), three levels
     uint64_t n_windows = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t bytes = 0;
@@ -686,7 +728,11 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     // N/64) records every window it marks; the next level then sweeps only
     // those windows.  Flags are a superset of the windows holding frontier
     // states, so skipping the others is exact.
+    // Three flag arrays in rotation: the windows of this level's frontier
+    // (flags_valid), of the previous level's states (flags_old; the three-bit
+    // `old` array) and the ones this level marks.
     int flags_valid = -1;          // index of the flag array valid for this level, -1 = sweep every window
+    int flags_old = -1;            // windows of the previous depth: -1 unknown, -2 none
     uint64_t estimate = 1;         // last known frontier size
     const uint64_t sparse_limit = N / 64;
     if (S->algo != PSB_FRONTIER) {
@@ -697,6 +743,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         PSB_CUDA(cudaMemcpyAsync(S->wflags[0] + (initial >> S->window_bits), &one, 1, cudaMemcpyHostToDevice, s));
         PSB_CUDA(cudaStreamSynchronize(s));
         flags_valid = 0;
+        flags_old = -2;  // depth -1 is empty
     }
 
     std::vector<uint64_t> res;
@@ -711,7 +758,8 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         if (max_depth && res.size() >= size_t(max_depth) + 1) break;
         PSB_CUDA(cudaMemsetAsync(S->d_stats, 0, 8 * sizeof(unsigned long long), s));
         const bool produce = estimate < sparse_limit;
-        const int flags_next = flags_valid < 0 ? 0 : 1 - flags_valid;
+        int flags_next = 0;
+        while (flags_next == flags_valid || flags_next == flags_old) flags_next++;
         if (produce) PSB_CUDA(cudaMemsetAsync(S->wflags[flags_next], 0, S->n_windows, s));
         a.wflag_cur = flags_valid >= 0 ? S->wflags[flags_valid] : nullptr;
         a.wflag_next = produce ? S->wflags[flags_next] : nullptr;
@@ -756,7 +804,13 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         if (S->algo == PSB_THREE_BIT || S->algo == PSB_CLASSIC) {
             const unsigned fgrid = 148 * 8;
             const uint64_t n2 = (W1 + 1) / 2;
-            if (S->algo == PSB_THREE_BIT && S->visited)
+            if (S->algo == PSB_THREE_BIT && produce && flags_old != -1 && !want_final)
+                psb::finalize_three_bit_flagged<<<fgrid, psb::kThreads, 0, s>>>(
+                    reinterpret_cast<const ulonglong2*>(cur), reinterpret_cast<ulonglong2*>(nw),
+                    reinterpret_cast<ulonglong2*>(old_), reinterpret_cast<ulonglong2*>(S->visited), n2,
+                    S->wflags[flags_next], flags_old >= 0 ? S->wflags[flags_old] : nullptr, S->n_windows,
+                    uint32_t((uint64_t(1) << S->window_bits) / 128), P.odd, S->d_stats + 4);
+            else if (S->algo == PSB_THREE_BIT && S->visited)
                 psb::finalize_three_bit_visited<<<fgrid, psb::kThreads, 0, s>>>(
                     reinterpret_cast<const ulonglong2*>(cur), reinterpret_cast<ulonglong2*>(nw),
                     reinterpret_cast<ulonglong2*>(old_), reinterpret_cast<ulonglong2*>(S->visited), n2, P.odd,
@@ -828,6 +882,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             break;
         }
         first = false;
+        flags_old = flags_valid;
         flags_valid = produce ? flags_next : -1;
         estimate = count;
         if (S->algo == PSB_TWO_BIT) {  // res holds depths 0..d; the next frontier is only estimated

@@ -33,6 +33,11 @@ __global__ void finalize_three_bit_visited(const ulonglong2* __restrict__ cur, u
                                            uint64_t n2, int odd, int zero_old, unsigned long long* count);
 __global__ void finalize_classic_clear(ulonglong2* __restrict__ nw, ulonglong2* __restrict__ closed,
                                        ulonglong2* __restrict__ open, uint64_t n2, unsigned long long* count);
+__global__ void finalize_three_bit_flagged(const ulonglong2* __restrict__ cur, ulonglong2* __restrict__ nw,
+                                           ulonglong2* __restrict__ old, ulonglong2* __restrict__ visited,
+                                           uint64_t n2, const uint8_t* __restrict__ new_flags,
+                                           const uint8_t* __restrict__ old_flags, uint64_t n_windows,
+                                           uint32_t per_window, int odd, unsigned long long* count);
 __global__ void retire_two_bit(ulonglong2* __restrict__ codes, uint64_t n2, uint32_t cur_code,
                                unsigned long long* count);
 }  // namespace psb
