@@ -175,6 +175,30 @@ int psb_bfs_session_destroy(psb_bfs_session* s);
  * `device` (-1 = current) to the driver; it waits for the device first. */
 int psb_release_cached_memory(int device);
 
+/* --- Device bit arrays (Common/BitArray.h:69-169) -------------------------
+ * Bit i of an array of n_bits bits is bit i%64 of 64-bit word i/64 (device
+ * memory, ceil(n_bits/64) words), the reference's BitArray layout.  The
+ * searches fuse these operations into their kernels; these calls run them on
+ * their own.  Each returns after the stream has reached it when it returns a
+ * count (scan, and_not_count); set_stride and or are only enqueued. */
+
+/* BitArray::Set(first + k*stride) for every such index below n_bits (:81-83). */
+int psb_bits_set_stride(uint64_t* d_words, uint64_t n_bits, uint64_t first, uint64_t stride, void* stream);
+
+/* BitArray::ScanBits (:138-145), ScanBitsAndClear (clear != 0, :147-155) and
+ * ScanBitsAndClearWithExcl (d_exclude != NULL, :157-166) with the callback
+ * "count the index and add it to a sum": *count = bits visited, *index_sum =
+ * sum of their indexes mod 2^64.  Whole words are scanned, as the reference does. */
+int psb_bits_scan(uint64_t* d_words, const uint64_t* d_exclude, uint64_t n_bits, int clear, uint64_t* count,
+                  uint64_t* index_sum, void* stream);
+
+/* BitArray::AndNotAndCount (:117-125): words &= ~exclude; *count = bits left. */
+int psb_bits_and_not_count(uint64_t* d_words, const uint64_t* d_exclude, uint64_t n_bits, uint64_t* count,
+                           void* stream);
+
+/* BitArray::Or (:103-107): words |= other. */
+int psb_bits_or(uint64_t* d_words, const uint64_t* d_other, uint64_t n_bits, void* stream);
+
 /* --- Frontier compression (Common/FrontierCompression.cpp, StreamVInt.cpp,
  *     CompressedFrontier.cpp) -------------------------------------------------
  * A segment's frontier -- the set bits of a bitmap range of at most 2^32

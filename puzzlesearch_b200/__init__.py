@@ -108,6 +108,11 @@ def lib():
                                           u32p, ctypes.POINTER(BfsStats)]
         L.psb_bfs_session_destroy.argtypes = [P]
         L.psb_release_cached_memory.argtypes = [ctypes.c_int]
+        vp = ctypes.c_void_p
+        L.psb_bits_set_stride.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, vp]
+        L.psb_bits_scan.argtypes = [vp, vp, ctypes.c_uint64, ctypes.c_int, u64p, u64p, vp]
+        L.psb_bits_and_not_count.argtypes = [vp, vp, ctypes.c_uint64, u64p, vp]
+        L.psb_bits_or.argtypes = [vp, vp, ctypes.c_uint64, vp]
         L.psb_frontier_encode.argtypes = [u64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
                                           u64p, ctypes.POINTER(CodecBlock), ctypes.c_uint32, u32p, ctypes.c_void_p]
         L.psb_frontier_index.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(CodecBlock),
@@ -476,6 +481,30 @@ class Server:
 def release_cached_memory(device=-1):
     """psb_release_cached_memory: return the search arrays' reserved pool memory to the driver."""
     _check(lib().psb_release_cached_memory(device))
+
+
+def bits_set_stride(d_words, n_bits, first, stride, stream=None):
+    """psb_bits_set_stride: BitArray::Set(first + k*stride) on a device bit array (pointer)."""
+    _check(lib().psb_bits_set_stride(d_words, n_bits, first, stride, stream))
+
+
+def bits_scan(d_words, n_bits, clear=False, d_exclude=None, stream=None):
+    """psb_bits_scan: (count, sum of indexes mod 2^64) of the set bits; optionally clears them."""
+    c, t = ctypes.c_uint64(), ctypes.c_uint64()
+    _check(lib().psb_bits_scan(d_words, d_exclude, n_bits, 1 if clear else 0, ctypes.byref(c), ctypes.byref(t), stream))
+    return c.value, t.value
+
+
+def bits_and_not_count(d_words, d_exclude, n_bits, stream=None):
+    """psb_bits_and_not_count: words &= ~exclude; returns the bits left."""
+    c = ctypes.c_uint64()
+    _check(lib().psb_bits_and_not_count(d_words, d_exclude, n_bits, ctypes.byref(c), stream))
+    return c.value
+
+
+def bits_or(d_words, d_other, n_bits, stream=None):
+    """psb_bits_or: words |= other."""
+    _check(lib().psb_bits_or(d_words, d_other, n_bits, stream))
 
 
 def frontier_index(data):
