@@ -121,7 +121,8 @@ def level_traffic(workload):
     return int(m.group(1)) if m else None
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
+    """One process per GPU (torchrun): returns (rank, world, local_rank, torch.distributed or None)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -132,9 +133,24 @@ def dist_setup(n_gpus):
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return rank, world, local, pg
+
+
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest x over all ranks (the timing rule: a multi-GPU time is the slowest rank's)."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, steps, units_per_step, seconds):
+    """Whole-job throughput: every rank processes units_per_step per step (replicas, weak scaling)."""
+    return world * steps * units_per_step / seconds
 
 
 def cpu_reference_sample(sample=REF_SAMPLE):
@@ -435,13 +451,9 @@ def main():
         end.record(stream)
         torch.cuda.synchronize()
     barrier()
-    elapsed_ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([elapsed_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(start.elapsed_time(end), dist)
     states_per_step = sum(ref_counts)
-    value = world * args.steps * states_per_step / (elapsed_ms / 1000.0)
+    value = job_rate(world, args.steps, states_per_step, elapsed_ms / 1000.0)
 
     # e2e: the public C-ABI entry point, host in/out, allocation included.
     # Untimed warm-up calls first, as for the device loop: the first call
@@ -460,12 +472,8 @@ def main():
         assert r["counts"] == ref_counts
         levels = r["stats"]["levels"]
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * args.steps * states_per_step / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    e2e_value = job_rate(world, args.steps, states_per_step, e2e_s)
 
     psb.lib().psb_bfs_session_destroy(h)
     if rank != 0:
