@@ -398,8 +398,7 @@ int psb_engine_create(const psb_engine_opts* opts, psb_engine** out) {
     EN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
     const int per_sm = opts->blocks_per_sm > 0 ? opts->blocks_per_sm : psb::kEMinBlocks;
     e->grid = unsigned(sms * per_sm);
-    e->smem = psb::mark_bytes(psb::kTwoBit, size_t(1) << psb::kEWindowBitsMax) +
-              size_t(psb::kEThreads) / 32 * 32 * psb::states_per_unit(psb::kTwoBit) * psb::list_entry_bytes(psb::kTwoBit);
+    e->smem = psb::level_smem_bytes(psb::kTwoBit, size_t(1) << psb::kEWindowBitsMax, psb::kEThreads);
     EN_CUDA(cudaFuncSetAttribute(psb::engine_level, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->smem)));
     EN_CUDA(cudaStreamSynchronize(e->stream));
     if (e->use_graph) {

@@ -662,10 +662,7 @@ int auto_window_bits(const psb_puzzle* p, int algo) {
 }
 
 size_t smem_bytes(int mode, int wb) {
-    // window marks + one list of a warp chunk's states per warp (see level_kernel)
-    const size_t W = size_t(1) << wb;
-    const size_t warps = size_t(psb::level_threads(mode)) / 32;
-    return psb::mark_bytes(mode, W) + warps * 32 * psb::states_per_unit(mode) * psb::list_entry_bytes(mode);
+    return psb::level_smem_bytes(mode, size_t(1) << wb, psb::level_threads(mode));
 }
 
 int set_bit(uint64_t* d_word_base, uint64_t bit, cudaStream_t s) {

@@ -95,12 +95,28 @@ struct PuzzleArgs {
 // two values only toggles the lowest Lehmer digit, of weight 1!), so a level
 // kernel can mark those children for a whole frontier word at once and expand
 // the rest with expand_from<1>.
+// kChunkPrefix: the level kernel unranks the shared leading positions of a
+// chunk's states once (make_prefix, two blocks of 7! indexes at most per
+// chunk) and each state's remaining positions from index % 7!.
 template <int N>
 struct PancakeK {
     static constexpr int kBranch = N - 1;
     static constexpr int kOps = N - 1;
     static constexpr int kProbeRound = PSB_PROBE_ROUND < N - 1 ? PSB_PROBE_ROUND : N - 1;
     static constexpr bool kPairOp0 = true;
+    static constexpr bool kChunkPrefix = true;
+    static constexpr uint32_t kBlock = Pancake<N>::kBlock;
+    using Prefix = typename Pancake<N>::Prefix;
+    __device__ __forceinline__ static void make_prefix(uint32_t q, Prefix& P) { Pancake<N>::make_prefix(q, P); }
+    template <int F, class E>
+    __device__ __forceinline__ static void expand_from_prefixed(uint64_t i, const Prefix& P, uint32_t r, E& e) {
+        Pancake<N>::template expand_prefixed<false>(i, P, r, 0u, F, N - 1, e);
+    }
+    template <class E>
+    __device__ __forceinline__ static void probe_prefixed(uint64_t i, const Prefix& P, uint32_t r, int first,
+                                                          int last, E& e) {
+        Pancake<N>::template expand_prefixed<false>(i, P, r, 0u, first, last, e);
+    }
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs&, E& e) {
         Pancake<N>::template expand<kOpBits>(i, ob, e);
@@ -120,6 +136,9 @@ struct SlidingK {
     static constexpr int kOps = 4;
     static constexpr int kProbeRound = 4;  // one round: four cheap children
     static constexpr bool kPairOp0 = false;
+    static constexpr bool kChunkPrefix = false;
+    static constexpr uint32_t kBlock = 1;
+    struct Prefix { uint32_t unused; };
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs& a, E& e) {
         Sliding<N>::template expand<kOpBits>(i, ob, a.width, e);
@@ -134,6 +153,9 @@ struct HanoiK {
     static constexpr int kOps = 4;
     static constexpr int kProbeRound = 6;  // one round: six cheap children
     static constexpr bool kPairOp0 = false;
+    static constexpr bool kChunkPrefix = false;
+    static constexpr uint32_t kBlock = 1;
+    struct Prefix { uint32_t unused; };
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs& a, E& e) {
         Hanoi::template expand<kOpBits>(i, ob, a.disks, a.sym != 0, e);
@@ -213,6 +235,14 @@ __host__ __device__ constexpr size_t mark_bytes(int mode, size_t window_states) 
 // Warp chunk: 32 lanes x one unit each (64 states; 32 for two-bit codes).
 __host__ __device__ constexpr uint32_t states_per_unit(int mode) { return mode == kTwoBit ? 32 : 64; }
 __host__ __device__ constexpr size_t list_entry_bytes(int mode) { return mode == kFrontier ? 4 : 2; }
+constexpr size_t kWarpScratch = 256;  // per warp: the chunk's two unranking prefixes (kChunkPrefix)
+
+// Dynamic shared memory of a level_window pass: window marks, then one list
+// of a chunk's states per warp, then each warp's scratch.
+__host__ __device__ constexpr size_t level_smem_bytes(int mode, size_t window_states, int threads) {
+    return mark_bytes(mode, window_states) +
+           size_t(threads / 32) * (32 * states_per_unit(mode) * list_entry_bytes(mode) + kWarpScratch);
+}
 
 template <int MODE>
 struct Emitter {
@@ -357,6 +387,12 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     uint32_t* smarks = reinterpret_cast<uint32_t*>(smem64);
     using Entry = typename std::conditional<MODE == kFrontier, uint32_t, uint16_t>::type;
     Entry* wlist = reinterpret_cast<Entry*>(reinterpret_cast<char*>(smem64) + mbytes) + size_t(warp) * kChunk;
+    // Unranking prefixes of the chunk's (at most two) blocks of PZ::kBlock indexes.
+    constexpr bool kPrefixed = PZ::kChunkPrefix && MODE != kFrontier;
+    using Prefix = typename PZ::Prefix;
+    static_assert(2 * sizeof(Prefix) <= kWarpScratch, "prefix scratch");
+    Prefix* pref = reinterpret_cast<Prefix*>(reinterpret_cast<char*>(smem64) + mbytes +
+                                             size_t(kWarps) * kChunk * sizeof(Entry) + size_t(warp) * kWarpScratch);
 
     for (uint32_t i = tid; i < mbytes / 16; i += kThreads) reinterpret_cast<uint4*>(smem64)[i] = make_uint4(0, 0, 0, 0);
     if (tid == 0) {
@@ -476,6 +512,18 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
             }
             __syncwarp();
             const uint64_t cbase = base + uint64_t(ch) * kChunk;
+            uint32_t q0 = 0;  // block of the chunk's first state
+            if constexpr (kPrefixed) {
+                q0 = uint32_t(cbase / PZ::kBlock);
+                if (lane < 2) PZ::make_prefix(q0 + uint32_t(lane), pref[lane]);
+                __syncwarp();
+            }
+            // state p = q*kBlock + r with q = q0 or q0 + 1 (a chunk is shorter than a block)
+            auto split = [&](uint64_t p, uint32_t& var) -> uint32_t {
+                const uint32_t r0 = uint32_t(p - uint64_t(q0) * PZ::kBlock);
+                var = r0 >= PZ::kBlock ? 1u : 0u;
+                return r0 - var * PZ::kBlock;
+            };
             if constexpr (BU) {
                 // Probe rounds: the round starting at child `first` probes
                 // children first .. first+R-1 of every state still listed;
@@ -495,7 +543,13 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                             entry = wlist[e];
                             const uint32_t o = uint32_t(ch) * kChunk + entry;  // offset in the window
                             Probe<MODE> pr{a.probe, a.n_states, cur_pat};
-                            PZ::probe_range(base + o, first, first + R, a.pz, pr);
+                            if constexpr (kPrefixed) {
+                                uint32_t var;
+                                const uint32_t r = split(base + o, var);
+                                PZ::probe_prefixed(base + o, pref[var], r, first, first + R, pr);
+                            } else {
+                                PZ::probe_range(base + o, first, first + R, a.pz, pr);
+                            }
                             probes += pr.probes;
                             pbad |= pr.bad;
                             if (pr.hit) {
@@ -522,8 +576,16 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                     PZ::template expand<true>(cbase + (v & 0xFFFFu), v >> 16, a.pz, em);
                 } else {
                     em.parent_off = ch * kChunk + wlist[e];
-                    if constexpr (kPairs) PZ::template expand_from<1>(cbase + wlist[e], a.pz, em);
-                    else PZ::template expand<false>(cbase + wlist[e], 0u, a.pz, em);
+                    const uint64_t p = cbase + wlist[e];
+                    if constexpr (kPrefixed) {
+                        uint32_t var;
+                        const uint32_t r = split(p, var);
+                        PZ::template expand_from_prefixed<kPairs ? 1 : 0>(p, pref[var], r, em);
+                    } else if constexpr (kPairs) {
+                        PZ::template expand_from<1>(p, a.pz, em);
+                    } else {
+                        PZ::template expand<false>(p, 0u, a.pz, em);
+                    }
                 }
             }
             __syncwarp();

@@ -152,8 +152,7 @@ extern "C" int psb_bfs_noalloc(const psb_puzzle* p, int algo, uint64_t initial, 
     a.stats = d_stats;
     const unsigned grid = unsigned(n_windows);
     const size_t W = size_t(1) << wb;
-    const size_t smem = psb::mark_bytes(mode, W) + size_t(psb::level_threads(mode)) / 32 * 32 *
-                                                        psb::states_per_unit(mode) * psb::list_entry_bytes(mode);
+    const size_t smem = psb::level_smem_bytes(mode, W, psb::level_threads(mode));
     uint32_t cur_code = 2;
     uint64_t estimate = 1;
     const uint64_t sparse_limit = N / 64;

@@ -108,25 +108,26 @@ struct Pancake {
     static constexpr int kBranch = N - 1;
     static constexpr int kOps = N - 1;
 
-    template <bool kOpBits, class Emit>
-    __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, Emit& emit) {
-        expand_range<kOpBits>(index, opbits, 0, N - 1, emit);
-    }
+    // Chunk-shared unranking.  Digit i has weight (n-1-i)!, so the first
+    // kL = n-7 positions of an index depend only on index / 7!: every index
+    // of a block of 7! = 5040 consecutive indexes shares them.  A Prefix holds
+    // those positions (digits, pre, pb) and the other 7 values as a 32-bit
+    // nibble list; unrank_suffix completes a state from index % 7!.
+    static constexpr int kL = N > 7 ? N - 7 : 0;
+    static constexpr uint32_t kBlock = 5040;  // 7!
+    struct Prefix {
+        uint32_t d[kL > 0 ? kL : 1], pre[kL > 0 ? kL : 1], pb[kL > 0 ? kL : 1];
+        uint32_t acc;     // values at positions < kL, one bit each
+        uint32_t tiles7;  // the other 7 values, ascending, one nibble each
+    };
 
-    // Only the children with operator in [first, last) (bottom-up probe rounds).
-    //
-    // Rank of the child of flip m: with pre = the values left of the suffix
-    // (positions < n-m) and pb[j] = the values left of position j that are
-    // smaller than v[j], the count above is popc(pb[j] & ~pre).  For m <= 12
-    // every quantity is below 12! < 2^31, so the child is passed to emitters
-    // that take it (EmitRel) as the parent plus a 32-bit signed delta.
-    template <bool kOpBits, class Emit>
-    __device__ __forceinline__ static void expand_range(uint64_t index, uint32_t opbits, int first, int last,
-                                                        Emit& emit) {
-        uint32_t d[N], v[N];
+    // Lehmer digits d, and for each position j: pre[j] = values left of j,
+    // pb[j] = those of them smaller than v[j] (one bit per value).
+    __device__ __forceinline__ static void unrank(uint64_t index, uint32_t (&d)[N], uint32_t (&pre)[N],
+                                                  uint32_t (&pb)[N]) {
+        uint32_t v[N];
         perm_digits<N>(index, d);
         perm_values<N>(d, v);
-        uint32_t pre[N], pb[N];
         uint32_t acc = 0;
 #pragma unroll
         for (int i = 0; i < N; ++i) {
@@ -134,6 +135,95 @@ struct Pancake {
             pb[i] = acc & ((1u << v[i]) - 1u);
             acc |= 1u << v[i];
         }
+    }
+
+    // Prefix of the indexes in [q*7!, (q+1)*7!); q < n!/7! <= 16!/7! < 2^32.
+    __device__ __forceinline__ static void make_prefix(uint32_t q, Prefix& P) {
+        if constexpr (kL > 0) {
+            uint32_t d[kL];
+#pragma unroll
+            for (int i = kL - 1; i >= 0; --i) {
+                d[i] = q % uint32_t(N - i);
+                q /= uint32_t(N - i);
+            }
+            uint64_t tiles = 0xFEDCBA9876543210ull;
+            uint32_t acc = 0;
+#pragma unroll
+            for (int i = 0; i < kL; ++i) {
+                const uint32_t s = 4u * d[i];
+                const uint32_t v = uint32_t(tiles >> s) & 15u;
+                tiles = (((tiles >> s) >> 4) << s) | (tiles & ((uint64_t(1) << s) - 1));
+                P.d[i] = d[i];
+                P.pre[i] = acc;
+                P.pb[i] = acc & ((1u << v) - 1u);
+                acc |= 1u << v;
+            }
+            P.acc = acc;
+            P.tiles7 = uint32_t(tiles) & 0x0FFFFFFFu;
+        } else {
+            P.acc = 0;
+            P.tiles7 = 0x06543210u;
+        }
+    }
+
+    // State of index q*7! + r from its block's prefix (r < 7!).
+    __device__ __forceinline__ static void unrank_suffix(const Prefix& P, uint32_t r, uint32_t (&d)[N],
+                                                         uint32_t (&pre)[N], uint32_t (&pb)[N]) {
+#pragma unroll
+        for (int i = 0; i < kL; ++i) {
+            d[i] = P.d[i];
+            pre[i] = P.pre[i];
+            pb[i] = P.pb[i];
+        }
+#pragma unroll
+        for (int i = N - 1; i >= kL; --i) {
+            d[i] = r % uint32_t(N - i);
+            r /= uint32_t(N - i);
+        }
+        uint32_t t = P.tiles7, acc = P.acc;
+#pragma unroll
+        for (int i = kL; i < N; ++i) {
+            const uint32_t s = 4u * d[i];
+            const uint32_t v = (t >> s) & 15u;
+            t = ((t >> s) >> 4 << s) | (t & ((1u << s) - 1u));
+            pre[i] = acc;
+            pb[i] = acc & ((1u << v) - 1u);
+            acc |= 1u << v;
+        }
+    }
+
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, Emit& emit) {
+        expand_range<kOpBits>(index, opbits, 0, N - 1, emit);
+    }
+
+    // Only the children with operator in [first, last) (bottom-up probe rounds).
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void expand_range(uint64_t index, uint32_t opbits, int first, int last,
+                                                        Emit& emit) {
+        uint32_t d[N], pre[N], pb[N];
+        unrank(index, d, pre, pb);
+        children<kOpBits>(index, d, pre, pb, opbits, first, last, emit);
+    }
+
+    // expand_range for index = q*7! + r, with P = make_prefix(q).
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void expand_prefixed(uint64_t index, const Prefix& P, uint32_t r,
+                                                           uint32_t opbits, int first, int last, Emit& emit) {
+        uint32_t d[N], pre[N], pb[N];
+        unrank_suffix(P, r, d, pre, pb);
+        children<kOpBits>(index, d, pre, pb, opbits, first, last, emit);
+    }
+
+    // Rank of the child of flip m: with pre = the values left of the suffix
+    // (positions < n-m) and pb[j] = the values left of position j that are
+    // smaller than v[j], the count above is popc(pb[j] & ~pre).  For m <= 12
+    // every quantity is below 12! < 2^31, so the child is passed to emitters
+    // that take it (EmitRel) as the parent plus a 32-bit signed delta.
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void children(uint64_t index, const uint32_t (&d)[N], const uint32_t (&pre)[N],
+                                                    const uint32_t (&pb)[N], uint32_t opbits, int first, int last,
+                                                    Emit& emit) {
         uint32_t low32 = 0;  // low_m for m <= 12 (d[n-1] is always 0)
         uint64_t low64 = 0;  // low_m for m > 12
 #pragma unroll
