@@ -367,8 +367,13 @@ template <class PZ, int MODE, int KTHREADS, bool BU = false>
 __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window, unsigned long long* smem64,
                                              WindowShared& sh) {
     static_assert(!BU || MODE != kFrontier, "frontier search keeps no visited information");
-    // Operator-0 children marked per frontier word in the sweep (see PancakeK).
+    // Operator-0 children marked per frontier word in the sweep (see PancakeK);
+    // bottom-up: unvisited states whose operator-0 neighbour is in the
+    // frontier, found per word before any probing.
     constexpr bool kPairs = PSB_PAIR_WORDS && PZ::kPairOp0 && MODE != kFrontier && !BU && !kByteMarks;
+    constexpr bool kBuPairs = PSB_PAIR_WORDS && PZ::kPairOp0 && BU && !kByteMarks;
+    // three-bit / classic bottom-up pairs also read the unit's frontier word
+    constexpr bool kProbeWord = kBuPairs && MODE != kTwoBit;
     constexpr int kThreads = KTHREADS;
     constexpr int kWarps = kThreads / 32;
     constexpr uint32_t kSPU = states_per_unit(MODE);
@@ -421,14 +426,20 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
             w[q] = (ch < chunks && u < units && wi < a.front_words) ? a.front[wi] : 0;
         }
     };
+    auto load_probe = [&](uint32_t ch) -> uint64_t {
+        const uint32_t u = ch * 32 + uint32_t(lane);
+        return (kProbeWord && ch < chunks && u < units) ? __ldg(a.probe + (base >> 6) + u) : 0;
+    };
     uint64_t cw[kWPU], nw[kWPU];
     uint32_t ch = uint32_t(warp);
     load(ch, cw);
+    uint64_t cp = load_probe(ch), np = 0;
     while (ch < chunks) {  // uniform within the warp
         uint32_t nch = 0;
         if (lane == 0) nch = atomicAdd(&sh.next_chunk, 1u);
         nch = __shfl_sync(0xFFFFFFFFu, nch, 0);
         load(nch, nw);
+        if constexpr (kProbeWord) np = load_probe(nch);
         const uint32_t u = ch * 32 + uint32_t(lane);
         uint64_t pmask = 0;
         if (BU && u < units) {
@@ -441,6 +452,26 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 pmask = ~cw[0];
             }
             if (left < kSPU) pmask &= (uint64_t(1) << left) - 1u;
+            if constexpr (kBuPairs) {
+                uint64_t fw;  // the unit's frontier states
+                if constexpr (MODE == kTwoBit) {
+                    const uint64_t w = cw[0], hi = w & kEven, lo = (w >> 1) & kEven;
+                    fw = gather_even(hi & (a.cur_code == 3 ? lo : ~lo));
+                } else {
+                    fw = cp;
+                }
+                const uint64_t hit2 = pmask & (((fw & kEven) << 1) | ((fw >> 1) & kEven));
+                if (hit2) {
+                    if constexpr (kSPU == 64) {
+                        if (uint32_t(hit2)) atomicOr(&smarks[2 * u], uint32_t(hit2));
+                        if (uint32_t(hit2 >> 32)) atomicOr(&smarks[2 * u + 1], uint32_t(hit2 >> 32));
+                    } else {
+                        atomicOr(&smarks[u], uint32_t(hit2));
+                    }
+                    hits += __popcll(hit2);
+                    pmask &= ~hit2;
+                }
+            }
         } else if (u < units) {
             if constexpr (MODE == kThreeBit) {
                 pmask = cw[0];
@@ -533,7 +564,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 constexpr int R = PZ::kProbeRound;
                 const uint32_t cur_pat = a.cur_code == 2 ? 1u : 3u;
                 uint32_t left = total;
-                for (int first = 0; first < PZ::kBranch && left; first += R) {
+                for (int first = kBuPairs ? 1 : 0; first < PZ::kBranch && left; first += R) {
                     uint32_t kept = 0;
                     for (uint32_t e0 = 0; e0 < left; e0 += 32) {
                         const uint32_t e = e0 + uint32_t(lane);
@@ -592,6 +623,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
         }
 #pragma unroll
         for (int q = 0; q < kWPU; ++q) cw[q] = nw[q];
+        cp = np;
         ch = nch;
     }
     if (BU ? hits != 0 : found != 0) sh.any = 1;
