@@ -219,6 +219,54 @@ __device__ __forceinline__ uint32_t nibble_flags(uint64_t x) {
     return uint32_t(t);
 }
 
+// L2 eviction-priority hints (PTX createpolicy / .L2::cache_hint, sm_80+).
+// Far children (pancake flips of more than 12) land anywhere in the array and
+// are never reused, so they are marked evict-first: they no longer displace
+// the region that the flips of 9..12 keep hitting (a flip of m stays inside
+// its aligned block of m! states).  13-pancake depth 11: 79 -> 72 ms.
+#ifndef PSB_FAR_HINT
+#define PSB_FAR_HINT 1
+#endif
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void red_or_far(unsigned int* a, unsigned int v) {
+    if constexpr (PSB_FAR_HINT)
+        asm volatile("red.global.or.b32.L2::cache_hint [%0], %1, %2;" ::"l"(a), "r"(v), "l"(l2_evict_first())
+                     : "memory");
+    else
+        atomicOr(a, v);
+}
+__device__ __forceinline__ uint64_t ld_cg_far(const unsigned long long* a) {
+    if constexpr (PSB_FAR_HINT) {
+        uint64_t v;
+        asm volatile("ld.global.cg.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
+        return v;
+    } else {
+        return __ldcg(a);
+    }
+}
+__device__ __forceinline__ uint64_t ld_nc_far(const uint64_t* a) {
+    if constexpr (PSB_FAR_HINT) {
+        uint64_t v;
+        asm("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
+        return v;
+    } else {
+        return __ldg(a);
+    }
+}
+__device__ __forceinline__ uint64_t ld_far(const uint64_t* a) {
+    if constexpr (PSB_FAR_HINT) {
+        uint64_t v;
+        asm volatile("ld.global.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
+        return v;
+    } else {
+        return *a;
+    }
+}
+
 // Shared-memory marks: one bit per state (1-bit modes) or four operator bits
 // per state (frontier search).  PSB_BYTE_MARKS (tuning builds) keeps one byte
 // per state for the 1-bit modes and marks with plain stores instead of atomics.
@@ -270,6 +318,7 @@ struct Emitter {
         }
     }
 
+    template <bool kFar = false>
     __device__ __forceinline__ void mark_remote(uint64_t c, uint32_t op) {
         if (c >= n_states) { bad = 1; return; }  // never expected: keeps a bad index off the memory system
         ++children;
@@ -279,7 +328,7 @@ struct Emitter {
         } else if constexpr (MODE == kTwoBit) {
             unsigned long long* w = reinterpret_cast<unsigned long long*>(gmarks) + (c >> 5);
             const uint32_t sh = 2u * (uint32_t(c) & 31u);
-            const uint64_t v = __ldcg(reinterpret_cast<const unsigned long long*>(w));
+            const uint64_t v = kFar ? ld_cg_far(w) : __ldcg(reinterpret_cast<const unsigned long long*>(w));
             if (((v >> sh) & 3u) == 0) {  // UNVISITED -> NEXT
                 if (wflag_next) wflag_next[c >> window_bits] = 1;
                 atomicOr(w, (unsigned long long)next_pat << sh);
@@ -287,7 +336,9 @@ struct Emitter {
             }
         } else {
             if (wflag_next) wflag_next[c >> window_bits] = 1;
-            atomicOr(reinterpret_cast<unsigned int*>(gmarks) + (c >> 5), 1u << (uint32_t(c) & 31u));
+            unsigned int* w = reinterpret_cast<unsigned int*>(gmarks) + (c >> 5);
+            if constexpr (kFar) red_or_far(w, 1u << (uint32_t(c) & 31u));
+            else atomicOr(w, 1u << (uint32_t(c) & 31u));
         }
     }
 
@@ -295,6 +346,13 @@ struct Emitter {
         const uint64_t o = c - base;
         if (o < span) mark_local(uint32_t(o), op);
         else mark_remote(c, op);
+    }
+
+    // A child anywhere in the index space (see EmitFar).
+    __device__ __forceinline__ void far(uint64_t c, uint32_t op) {
+        const uint64_t o = c - base;
+        if (o < span) mark_local(uint32_t(o), op);
+        else mark_remote<true>(c, op);
     }
 
     // Child = parent + delta, with the parent at parent_off in the window.
@@ -320,19 +378,23 @@ struct Probe {
     bool hit = false;
     uint32_t probes = 0, bad = 0;
 
-    __device__ __forceinline__ void operator()(uint64_t c, uint32_t) {
+    template <bool kFar = false>
+    __device__ __forceinline__ void probe(uint64_t c) {
         if (c >= n_states) { bad = 1; return; }
         ++probes;
         if constexpr (MODE == kTwoBit) {
             // Plain load: other blocks set NEXT bits in these words meanwhile,
             // which never changes a CUR code.
-            const uint64_t w = front[c >> 5];
+            const uint64_t w = kFar ? ld_far(front + (c >> 5)) : front[c >> 5];
             hit |= ((w >> (2u * (uint32_t(c) & 31u))) & 3u) == cur_pat;
         } else {
-            const uint64_t w = __ldg(front + (c >> 6));  // read-only during a bottom-up level
+            // read-only during a bottom-up level
+            const uint64_t w = kFar ? ld_nc_far(front + (c >> 6)) : __ldg(front + (c >> 6));
             hit |= ((w >> (uint32_t(c) & 63u)) & 1u) != 0;
         }
     }
+    __device__ __forceinline__ void operator()(uint64_t c, uint32_t) { probe<false>(c); }
+    __device__ __forceinline__ void far(uint64_t c, uint32_t) { probe<true>(c); }
 };
 
 // 32 marks held as bytes (0/1) -> 32-bit mask.

@@ -30,6 +30,14 @@ struct EmitRel : std::false_type {};
 template <class E>
 struct EmitRel<E, decltype(void(&E::rel))> : std::true_type {};
 
+// Emitters with a member far(child, op) take children that can land anywhere
+// in a large index space (pancake flips of more than 12) there, so they can
+// mark them without displacing cached data that nearer children reuse.
+template <class E, class = void>
+struct EmitFar : std::false_type {};
+template <class E>
+struct EmitFar<E, decltype(void(&E::far))> : std::true_type {};
+
 __host__ __device__ constexpr uint64_t fact(int k) { return k <= 1 ? 1 : uint64_t(k) * fact(k - 1); }
 constexpr uint32_t kF12 = 479001600u;  // 12!
 
@@ -249,7 +257,9 @@ struct Pancake {
                     if (q < 12) s32 += uint32_t(fact(q)) * c;
                     else t += uint32_t(fact(q) / kF12) * c;
                 }
-                emit(index - low64 + (uint64_t(t) * kF12 + s32), uint32_t(op));
+                const uint64_t child = index - low64 + (uint64_t(t) * kF12 + s32);
+                if constexpr (EmitFar<Emit>::value) emit.far(child, uint32_t(op));
+                else emit(child, uint32_t(op));
             }
         }
     }
