@@ -46,6 +46,9 @@ enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 #ifndef PSB_TD_MIN_BLOCKS
 #define PSB_TD_MIN_BLOCKS 1
 #endif
+#ifndef PSB_TD2_MIN_BLOCKS
+#define PSB_TD2_MIN_BLOCKS 4
+#endif
 #ifndef PSB_BU_MIN_BLOCKS
 #define PSB_BU_MIN_BLOCKS 4
 #endif
@@ -67,8 +70,8 @@ struct Shape {
 #else
     // Bottom-up levels wait on their probe loads, so they want resident warps
     // too, but not at the price of spills (two-bit's 64-register cap spills).
-    static constexpr int min_blocks = BU ? PSB_BU_MIN_BLOCKS : MODE == kTwoBit ? 4 : MODE == kFrontier ? 2
-                                                                                : PSB_TD_MIN_BLOCKS;
+    static constexpr int min_blocks = BU ? PSB_BU_MIN_BLOCKS : MODE == kTwoBit ? PSB_TD2_MIN_BLOCKS
+                                        : MODE == kFrontier ? 2 : PSB_TD_MIN_BLOCKS;
 #endif
 };
 
