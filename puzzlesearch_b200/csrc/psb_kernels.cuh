@@ -43,6 +43,9 @@ enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 #ifndef PSB_PAIR_WORDS
 #define PSB_PAIR_WORDS 1
 #endif
+#ifndef PSB_FLIP3_WORDS
+#define PSB_FLIP3_WORDS 1
+#endif
 #ifndef PSB_TD_MIN_BLOCKS
 #define PSB_TD_MIN_BLOCKS 1
 #endif
@@ -107,6 +110,7 @@ struct PancakeK {
     static constexpr int kOps = N - 1;
     static constexpr int kProbeRound = PSB_PROBE_ROUND < N - 1 ? PSB_PROBE_ROUND : N - 1;
     static constexpr bool kPairOp0 = true;
+    static constexpr bool kFlip3Op1 = N >= 3;  // operator 1 permutes each aligned block of 6 (see flip3_push)
     static constexpr bool kChunkPrefix = true;
     static constexpr uint32_t kBlock = Pancake<N>::kBlock;
     using Prefix = typename Pancake<N>::Prefix;
@@ -139,6 +143,7 @@ struct SlidingK {
     static constexpr int kOps = 4;
     static constexpr int kProbeRound = 4;  // one round: four cheap children
     static constexpr bool kPairOp0 = false;
+    static constexpr bool kFlip3Op1 = false;
     static constexpr bool kChunkPrefix = false;
     static constexpr uint32_t kBlock = 1;
     struct Prefix { uint32_t unused; };
@@ -156,6 +161,7 @@ struct HanoiK {
     static constexpr int kOps = 4;
     static constexpr int kProbeRound = 6;  // one round: six cheap children
     static constexpr bool kPairOp0 = false;
+    static constexpr bool kFlip3Op1 = false;
     static constexpr bool kChunkPrefix = false;
     static constexpr uint32_t kBlock = 1;
     struct Prefix { uint32_t unused; };
@@ -293,6 +299,70 @@ constexpr size_t kWarpScratch = 256;  // per warp: the chunk's two unranking pre
 __host__ __device__ constexpr size_t level_smem_bytes(int mode, size_t window_states, int threads) {
     return mark_bytes(mode, window_states) +
            size_t(threads / 32) * (32 * states_per_unit(mode) * list_entry_bytes(mode) + kWarpScratch);
+}
+
+// Pancake operator 1 (flip of the last three values) only changes the two
+// lowest Lehmer digits: it maps index 6q + r to 6q + pi3(r) with
+// pi3 = (5 3 4 1 2 0), an involution, and n! is a multiple of 6.  So for a
+// unit of UW consecutive states (UW = 64 or 32, first state g*UW) the
+// children of a frontier mask F are shifts of F by +5 (r = 0), +2 (r = 1, 2),
+// -2 (r = 3, 4) and -5 (r = 5) under residue masks; bits shifted out of the
+// unit belong to the neighbouring units.
+__host__ __device__ constexpr uint64_t res6_mask(int phase, int r0, int r1, int width) {
+    uint64_t m = 0;
+    for (int b = 0; b < width; ++b)
+        if ((phase + b) % 6 == r0 || (phase + b) % 6 == r1) m |= uint64_t(1) << b;
+    return m;
+}
+template <int UW>
+struct Res6 {  // residue masks of a unit whose first state is phase (mod 6)
+    uint64_t m0, m12, m34, m5;
+    __device__ __forceinline__ explicit Res6(uint64_t g) {  // g = global unit index
+        // phase = (g * UW) mod 6, which depends on g mod 3 only
+        constexpr int p1 = (UW % 6), p2 = (2 * UW) % 6;
+        const uint32_t k = uint32_t(g % 3u);
+        m0 = k == 0 ? res6_mask(0, 0, 0, UW) : k == 1 ? res6_mask(p1, 0, 0, UW) : res6_mask(p2, 0, 0, UW);
+        m12 = k == 0 ? res6_mask(0, 1, 2, UW) : k == 1 ? res6_mask(p1, 1, 2, UW) : res6_mask(p2, 1, 2, UW);
+        m34 = k == 0 ? res6_mask(0, 3, 4, UW) : k == 1 ? res6_mask(p1, 3, 4, UW) : res6_mask(p2, 3, 4, UW);
+        m5 = k == 0 ? res6_mask(0, 5, 5, UW) : k == 1 ? res6_mask(p1, 5, 5, UW) : res6_mask(p2, 5, 5, UW);
+    }
+};
+// Top-down: the operator-1 children of frontier mask F of unit g, split into
+// the unit itself, the previous unit and the next one.
+template <int UW>
+__device__ __forceinline__ void flip3_push(uint64_t F, uint64_t g, uint64_t& prev, uint64_t& own, uint64_t& next) {
+    const Res6<UW> m(g);
+    const uint64_t p0 = F & m.m0, p12 = F & m.m12, p34 = F & m.m34, p5 = F & m.m5;
+    constexpr uint64_t kLow = UW == 64 ? ~uint64_t(0) : 0xFFFFFFFFull;
+    const uint64_t up = (p0 << 5) | (p12 << 2);  // UW = 32: bits above 31 overflow into the next unit
+    own = (up | (p34 >> 2) | (p5 >> 5)) & kLow;
+    if constexpr (UW == 64) {
+        next = (p0 >> 59) | (p12 >> 62);
+        prev = (p34 << 62) | (p5 << 59);
+    } else {
+        next = up >> 32;
+        prev = ((p34 << 30) | (p5 << 27)) & kLow;
+    }
+}
+// Bottom-up: the states of unit g whose operator-1 partner is in the
+// frontier, from the frontier masks of units g-1, g and g+1.
+template <int UW>
+__device__ __forceinline__ uint64_t flip3_pull(uint64_t prevF, uint64_t F, uint64_t nextF, uint64_t g) {
+    const Res6<UW> m(g);
+    uint64_t up5, up2, dn2, dn5;  // bit b: frontier bit of state b+5, b+2, b-2, b-5
+    if constexpr (UW == 64) {
+        up5 = (F >> 5) | (nextF << 59);
+        up2 = (F >> 2) | (nextF << 62);
+        dn2 = (F << 2) | (prevF >> 62);
+        dn5 = (F << 5) | (prevF >> 59);
+    } else {
+        const uint64_t x = (nextF << 32) | F, y = (F << 32) | prevF;
+        up5 = (x >> 5) & 0xFFFFFFFFull;
+        up2 = (x >> 2) & 0xFFFFFFFFull;
+        dn2 = (y << 2) >> 32;
+        dn5 = (y << 5) >> 32;
+    }
+    return (m.m0 & up5) | (m.m12 & up2) | (m.m34 & dn2) | (m.m5 & dn5);
 }
 
 template <int MODE>
@@ -439,6 +509,10 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     constexpr bool kBuPairs = PSB_PAIR_WORDS && PZ::kPairOp0 && BU && !kByteMarks;
     // three-bit / classic bottom-up pairs also read the unit's frontier word
     constexpr bool kProbeWord = kBuPairs && MODE != kTwoBit;
+    // Operator-1 children (top-down) and hits (bottom-up) per unit as well
+    // (flip3_push / flip3_pull); per-state expansion then starts at operator 2.
+    constexpr bool kFlip3 = PSB_FLIP3_WORDS && kPairs && PZ::kFlip3Op1;
+    constexpr bool kBuFlip3 = PSB_FLIP3_WORDS && kBuPairs && PZ::kFlip3Op1;
     constexpr int kThreads = KTHREADS;
     constexpr int kWarps = kThreads / 32;
     constexpr uint32_t kSPU = states_per_unit(MODE);
@@ -474,6 +548,20 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     Emitter<MODE> em{base, span, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u), a.wflag_next,
                      a.window_bits};
     uint32_t found = 0;
+    // ORs a mask of unit x's states into the window's shared marks.
+    auto mark_unit = [&](uint32_t x, uint64_t m) {
+        if constexpr (kSPU == 64) {
+            if (uint32_t(m)) atomicOr(&smarks[2 * x], uint32_t(m));
+            if (uint32_t(m >> 32)) atomicOr(&smarks[2 * x + 1], uint32_t(m >> 32));
+        } else {
+            atomicOr(&smarks[x], uint32_t(m));
+        }
+    };
+    // The CUR states of two-bit code word x (one bit per state).
+    auto cur_states = [&](uint64_t x) -> uint64_t {
+        const uint64_t hi = x & kEven, lo = (x >> 1) & kEven;
+        return gather_even(hi & (a.cur_code == 3 ? lo : ~lo));
+    };
     uint32_t probes = 0, hits = 0, pbad = 0;  // bottom-up counters
 
     // Each warp takes chunks on its own (its first chunk is its warp index,
@@ -536,6 +624,24 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                     hits += __popcll(hit2);
                     pmask &= ~hit2;
                 }
+                if constexpr (kBuFlip3) {
+                    // neighbouring units' frontier states (stable during a bottom-up level)
+                    const uint64_t g = (MODE == kTwoBit ? (base >> 5) : (base >> 6)) + u;
+                    uint64_t pf = 0, nf = 0;
+                    if constexpr (MODE == kTwoBit) {
+                        if (g > 0) pf = cur_states(a.front[g - 1]);
+                        if (g + 1 < a.front_words) nf = cur_states(a.front[g + 1]);
+                    } else {
+                        if (g > 0) pf = __ldg(a.probe + g - 1);
+                        if (g + 1 < a.front_words) nf = __ldg(a.probe + g + 1);
+                    }
+                    const uint64_t hit3 = pmask & flip3_pull<kSPU>(pf, fw, nf, g);
+                    if (hit3) {
+                        mark_unit(u, hit3);
+                        hits += __popcll(hit3);
+                        pmask &= ~hit3;
+                    }
+                }
             }
         } else if (u < units) {
             if constexpr (MODE == kThreeBit) {
@@ -579,6 +685,33 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 em.children += np;
                 em.local += np;
             }
+        }
+        if constexpr (kFlip3) {
+            uint64_t pv, own, nx;
+            flip3_push<kSPU>(pmask, (MODE == kTwoBit ? (base >> 5) : (base >> 6)) + u, pv, own, nx);
+            if (own) {
+                mark_unit(u, own);
+                em.children += __popcll(own);
+                em.local += __popcll(own);
+            }
+            // children in the neighbouring units: shared marks inside the
+            // window, the emitter's long-range path outside it
+            auto side = [&](uint64_t m, int64_t x) {
+                if (!m) return;
+                if (x >= 0 && x < int64_t(W / kSPU)) {
+                    mark_unit(uint32_t(x), m);
+                    em.children += __popcll(m);
+                    em.local += __popcll(m);
+                } else {
+                    while (m) {
+                        const uint32_t bit = __ffsll((long long)m) - 1;
+                        m &= m - 1;
+                        em(uint64_t(int64_t(base) + x * int64_t(kSPU) + bit), 1u);
+                    }
+                }
+            };
+            side(pv, int64_t(u) - 1);
+            side(nx, int64_t(u) + 1);
         }
         const uint32_t cnt = __popcll(pmask);
         found += cnt;
@@ -629,7 +762,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 constexpr int R = PZ::kProbeRound;
                 const uint32_t cur_pat = a.cur_code == 2 ? 1u : 3u;
                 uint32_t left = total;
-                for (int first = kBuPairs ? 1 : 0; first < PZ::kBranch && left; first += R) {
+                for (int first = kBuFlip3 ? 2 : kBuPairs ? 1 : 0; first < PZ::kBranch && left; first += R) {
                     uint32_t kept = 0;
                     for (uint32_t e0 = 0; e0 < left; e0 += 32) {
                         const uint32_t e = e0 + uint32_t(lane);
@@ -676,9 +809,9 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                     if constexpr (kPrefixed) {
                         uint32_t var;
                         const uint32_t r = split(p, var);
-                        PZ::template expand_from_prefixed<kPairs ? 1 : 0>(p, pref[var], r, em);
+                        PZ::template expand_from_prefixed<kFlip3 ? 2 : kPairs ? 1 : 0>(p, pref[var], r, em);
                     } else if constexpr (kPairs) {
-                        PZ::template expand_from<1>(p, a.pz, em);
+                        PZ::template expand_from<kFlip3 ? 2 : 1>(p, a.pz, em);
                     } else {
                         PZ::template expand<false>(p, 0u, a.pz, em);
                     }
