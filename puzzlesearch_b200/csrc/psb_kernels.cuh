@@ -43,6 +43,9 @@ enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 #ifndef PSB_PAIR_WORDS
 #define PSB_PAIR_WORDS 1
 #endif
+#ifndef PSB_PROBE_DESC
+#define PSB_PROBE_DESC 0
+#endif
 #ifndef PSB_FLIP3_WORDS
 #define PSB_FLIP3_WORDS 1
 #endif
@@ -774,7 +777,15 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 constexpr int R = PZ::kProbeRound;
                 const uint32_t cur_pat = a.cur_code == 2 ? 1u : 3u;
                 uint32_t left = total;
-                for (int first = kBuFlip3 ? 2 : kBuPairs ? 1 : 0; first < PZ::kBranch && left; first += R) {
+                constexpr int kFirst = kBuFlip3 ? 2 : kBuPairs ? 1 : 0;
+                constexpr int kRounds = (PZ::kBranch - kFirst + R - 1) / R;
+                for (int round = 0; round < kRounds && left; ++round) {
+                    // children [lo, hi) of this round: ascending from kFirst, or
+                    // (PSB_PROBE_DESC) descending from the last child
+                    const int lo = PSB_PROBE_DESC ? (PZ::kBranch - (round + 1) * R > kFirst ? PZ::kBranch - (round + 1) * R : kFirst)
+                                                  : kFirst + round * R;
+                    const int hi = PSB_PROBE_DESC ? PZ::kBranch - round * R
+                                                  : (lo + R < PZ::kBranch ? lo + R : PZ::kBranch);
                     uint32_t kept = 0;
                     for (uint32_t e0 = 0; e0 < left; e0 += 32) {
                         const uint32_t e = e0 + uint32_t(lane);
@@ -787,9 +798,9 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                             if constexpr (kPrefixed) {
                                 uint32_t var;
                                 const uint32_t r = split(base + o, var);
-                                PZ::probe_prefixed(base + o, pref[var], r, first, first + R, pr);
+                                PZ::probe_prefixed(base + o, pref[var], r, lo, hi, pr);
                             } else {
-                                PZ::probe_range(base + o, first, first + R, a.pz, pr);
+                                PZ::probe_range(base + o, lo, hi, a.pz, pr);
                             }
                             probes += pr.probes;
                             pbad |= pr.bad;
