@@ -43,6 +43,9 @@ enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 #ifndef PSB_PAIR_WORDS
 #define PSB_PAIR_WORDS 1
 #endif
+#ifndef PSB_PROBE_TWO_ROUNDS
+#define PSB_PROBE_TWO_ROUNDS 1
+#endif
 #ifndef PSB_PROBE_DESC
 #define PSB_PROBE_DESC 0
 #endif
@@ -774,7 +777,12 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 // states with a hit are marked, the rest are compacted in
                 // place (ballot) for the next round, so every round keeps all
                 // lanes busy whatever the hit pattern.
-                constexpr int R = PZ::kProbeRound;
+                // Pancake: the children left after the word-level flips in two
+                // rounds (each round re-unranks the states still listed; 13-pancake
+                // depth 12: 58 ms in 2 rounds of 5 against 65 ms in 3 rounds of 4).
+                constexpr int kLeftChildren = PZ::kBranch - (kBuFlip3 ? 2 : kBuPairs ? 1 : 0);
+                constexpr int R = (PSB_PROBE_TWO_ROUNDS && PZ::kPairOp0) ? (kLeftChildren > 1 ? (kLeftChildren + 1) / 2 : 1)
+                                                                         : PZ::kProbeRound;
                 const uint32_t cur_pat = a.cur_code == 2 ? 1u : 3u;
                 uint32_t left = total;
                 constexpr int kFirst = kBuFlip3 ? 2 : kBuPairs ? 1 : 0;
