@@ -49,6 +49,9 @@ enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 #ifndef PSB_PROBE_DESC
 #define PSB_PROBE_DESC 0
 #endif
+#ifndef PSB_FLIP4_WORDS
+#define PSB_FLIP4_WORDS 1
+#endif
 #ifndef PSB_FLIP3_WORDS
 #define PSB_FLIP3_WORDS 1
 #endif
@@ -117,6 +120,7 @@ struct PancakeK {
     static constexpr int kProbeRound = PSB_PROBE_ROUND < N - 1 ? PSB_PROBE_ROUND : N - 1;
     static constexpr bool kPairOp0 = true;
     static constexpr bool kFlip3Op1 = N >= 3;  // operator 1 permutes each aligned block of 6 (see flip3_push)
+    static constexpr bool kFlip4Op2 = N >= 4;  // operator 2 permutes each aligned block of 24 (see flip4_pull)
     static constexpr bool kChunkPrefix = true;
     static constexpr uint32_t kBlock = Pancake<N>::kBlock;
     using Prefix = typename Pancake<N>::Prefix;
@@ -150,6 +154,7 @@ struct SlidingK {
     static constexpr int kProbeRound = 4;  // one round: four cheap children
     static constexpr bool kPairOp0 = false;
     static constexpr bool kFlip3Op1 = false;
+    static constexpr bool kFlip4Op2 = false;
     static constexpr bool kChunkPrefix = false;
     static constexpr uint32_t kBlock = 1;
     struct Prefix { uint32_t unused; };
@@ -168,6 +173,7 @@ struct HanoiK {
     static constexpr int kProbeRound = 6;  // one round: six cheap children
     static constexpr bool kPairOp0 = false;
     static constexpr bool kFlip3Op1 = false;
+    static constexpr bool kFlip4Op2 = false;
     static constexpr bool kChunkPrefix = false;
     static constexpr uint32_t kBlock = 1;
     struct Prefix { uint32_t unused; };
@@ -371,6 +377,43 @@ __device__ __forceinline__ uint64_t flip3_pull(uint64_t prevF, uint64_t F, uint6
     return (m.m0 & up5) | (m.m12 & up2) | (m.m34 & dn2) | (m.m5 & dn5);
 }
 
+// Pancake operator 2 (flip of the last four values) changes the three lowest
+// Lehmer digits only: it maps index 24q + r to 24q + pi4(r), an involution
+// (pi4 below is the Lehmer rank of the reversed arrangement of rank r), and
+// n! is a multiple of 24 for n >= 4.  Bottom-up: the states of unit g whose
+// operator-2 partner is in the frontier.  The residue masks are bits
+// {0, 24, 48} of the unit shifted by (r - phase) mod 24.
+// pi4 = (23 17 21 11 15 9 22 16 19 5 13 3 20 10 18 4 7 1 14 8 12 2 6 0), five bits per entry.
+__host__ __device__ constexpr int pi4(int r) {
+    return int(((r < 12 ? 0x1b4b38592f5d637ull >> (5 * r) : 0x184c4382724954ull >> (5 * (r - 12)))) & 31u);
+}
+template <int UW>
+__device__ __forceinline__ uint64_t flip4_pull(uint64_t prevF, uint64_t F, uint64_t nextF, uint64_t g) {
+    // phase = (g * UW) mod 24 depends on g mod 3 only
+    constexpr int p1 = UW % 24, p2 = (2 * UW) % 24;
+    const uint32_t k = uint32_t(g % 3u);
+    const int phase = k == 0 ? 0 : k == 1 ? p1 : p2;
+    const int t = phase == 0 ? 0 : 24 - phase;
+    constexpr uint64_t kBase = UW == 64 ? 0x0001000001000001ull : 0x01000001ull;
+    constexpr uint64_t kLow = UW == 64 ? ~uint64_t(0) : 0xFFFFFFFFull;
+    uint64_t hit = 0;
+#pragma unroll
+    for (int r = 0; r < 24; ++r) {
+        const int d = pi4(r) - r;  // partner offset, compile-time after unrolling
+        int x = r + t;
+        if (x >= 24) x -= 24;
+        const uint64_t m = (kBase << x) & kLow;
+        uint64_t sh;  // bit b: frontier bit of state b + d
+        if constexpr (UW == 64) {
+            sh = d > 0 ? (F >> d) | (nextF << ((64 - d) & 63)) : (F << -d) | (prevF >> ((64 + d) & 63));
+        } else {
+            sh = d > 0 ? (((nextF << 32) | F) >> d) & kLow : ((((F << 32) | prevF) << -d) >> 32);
+        }
+        hit |= m & sh;
+    }
+    return hit;
+}
+
 template <int MODE>
 struct Emitter {
     uint64_t base;        // first state of the block's window
@@ -530,6 +573,8 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     // (flip3_push / flip3_pull); per-state expansion then starts at operator 2.
     constexpr bool kFlip3 = PSB_FLIP3_WORDS && kPairs && PZ::kFlip3Op1;
     constexpr bool kBuFlip3 = PSB_FLIP3_WORDS && kBuPairs && PZ::kFlip3Op1;
+    // Bottom-up also finds operator-2 hits per unit (flip4_pull).
+    constexpr bool kBuFlip4 = PSB_FLIP4_WORDS && kBuFlip3 && PZ::kFlip4Op2;
     constexpr int kThreads = KTHREADS;
     constexpr int kWarps = kThreads / 32;
     constexpr uint32_t kSPU = states_per_unit(MODE);
@@ -642,7 +687,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                     hits += __popcll(hit2);
                     pmask &= ~hit2;
                 }
-                if constexpr (kBuFlip3) {
+                if (kBuFlip3 && pmask) {
                     // neighbouring units' frontier states (stable during a bottom-up level)
                     const uint64_t g = (MODE == kTwoBit ? (base >> 5) : (base >> 6)) + u;
                     uint64_t pf = 0, nf = 0;
@@ -653,7 +698,9 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                         if (g > 0) pf = __ldg(a.probe + g - 1);
                         if (g + 1 < a.front_words) nf = __ldg(a.probe + g + 1);
                     }
-                    const uint64_t hit3 = pmask & flip3_pull<kSPU>(pf, fw, nf, g);
+                    uint64_t hit3 = flip3_pull<kSPU>(pf, fw, nf, g);
+                    if constexpr (kBuFlip4) hit3 |= flip4_pull<kSPU>(pf, fw, nf, g);
+                    hit3 &= pmask;
                     if (hit3) {
                         mark_unit(u, hit3);
                         hits += __popcll(hit3);
@@ -780,12 +827,12 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 // Pancake: the children left after the word-level flips in two
                 // rounds (each round re-unranks the states still listed; 13-pancake
                 // depth 12: 58 ms in 2 rounds of 5 against 65 ms in 3 rounds of 4).
-                constexpr int kLeftChildren = PZ::kBranch - (kBuFlip3 ? 2 : kBuPairs ? 1 : 0);
+                constexpr int kLeftChildren = PZ::kBranch - (kBuFlip4 ? 3 : kBuFlip3 ? 2 : kBuPairs ? 1 : 0);
                 constexpr int R = (PSB_PROBE_TWO_ROUNDS && PZ::kPairOp0) ? (kLeftChildren > 1 ? (kLeftChildren + 1) / 2 : 1)
                                                                          : PZ::kProbeRound;
                 const uint32_t cur_pat = a.cur_code == 2 ? 1u : 3u;
                 uint32_t left = total;
-                constexpr int kFirst = kBuFlip3 ? 2 : kBuPairs ? 1 : 0;
+                constexpr int kFirst = kBuFlip4 ? 3 : kBuFlip3 ? 2 : kBuPairs ? 1 : 0;
                 constexpr int kRounds = (PZ::kBranch - kFirst + R - 1) / R;
                 for (int round = 0; round < kRounds && left; ++round) {
                     // children [lo, hi) of this round: ascending from kFirst, or
