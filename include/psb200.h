@@ -121,7 +121,8 @@ typedef struct {
  * symmetry) makes every still unvisited state probe its neighbours for a
  * frontier state; on the last, dense levels of a search that is far less
  * work.  Counts and final arrays are the same either way.  Three-bit searches
- * that may go bottom-up keep one more bit per state (the visited set). */
+ * that may go bottom-up keep one more bit per state (the visited set) when
+ * device memory allows; otherwise every level runs top-down. */
 #define PSB_DIR_AUTO 0      /* top-down; bottom-up on dense levels once unvisited < ratio * frontier */
 #define PSB_DIR_TOP_DOWN 1  /* every level top-down (no visited array) */
 #define PSB_DIR_BOTTOM_UP 2 /* every level bottom-up where the search supports it (tests) */

@@ -986,8 +986,17 @@ int psb_bfs_session_create(const psb_puzzle* p, int algo, const psb_bfs_opts* op
     for (int i = 0; i < S->n_arr; i++)
         if (int rc = S->alloc(reinterpret_cast<void**>(&S->arr[i]), S->words[i] * 8)) return rc;
     S->bottom_up = supports_bottom_up(p, algo);
-    if (S->bottom_up && algo == PSB_THREE_BIT && !(opts && opts->direction == PSB_DIR_TOP_DOWN))
-        if (int rc = S->alloc(reinterpret_cast<void**>(&S->visited), S->words[0] * 8)) return rc;
+    if (S->bottom_up && algo == PSB_THREE_BIT && !(opts && opts->direction == PSB_DIR_TOP_DOWN)) {
+        // Optional: without room for the visited array the search runs every
+        // level top-down, in the reference's three arrays.
+        void* v = nullptr;
+        if (cudaMallocFromPoolAsync(&v, S->words[0] * 8, S->pool, S->stream) == cudaSuccess) {
+            S->visited = static_cast<uint64_t*>(v);
+            S->bytes += S->words[0] * 8;
+        } else {
+            cudaGetLastError();  // an allocation failure is not sticky; clear it
+        }
+    }
     S->n_windows = (p->n_states + (uint64_t(1) << S->window_bits) - 1) >> S->window_bits;
     for (auto& f : S->wflags)
         if (int rc = S->alloc(reinterpret_cast<void**>(&f), S->n_windows)) return rc;
