@@ -238,7 +238,8 @@ def batch_bench(args):
     total_states = sum(puzzles[t].IndexesCount() // (2 if t[0] == "sliding" else 1) for _, t, _ in items)
 
     def run_batched():
-        eng = psb.Engine(max_instances=args.instances, max_depths=128, pool_bytes=24 << 30)
+        eng = psb.Engine(max_instances=args.instances, max_depths=128, pool_bytes=24 << 30,
+                         direction="top_down" if args.direction == "top_down" else "auto")
         t0 = time.perf_counter()
         for i, t, st in items:
             assert eng.add(puzzles[t], st, i)
@@ -268,7 +269,7 @@ def batch_bench(args):
             "value": len(items) / b_dt, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": args.warmup,
             "higher_is_better": True, "dtype": "u64", "data": "seeded random solvable starts",
             "config": {"workload": "batch4096", "instances": len(items), "states": total_states,
-                       "engine_levels": levels},
+                       "engine_levels": levels, "direction": "top_down" if args.direction == "top_down" else "auto"},
             "batched": {"seconds": b_dt, "solves_per_s": len(items) / b_dt, "states_per_s": total_states / b_dt},
             "plain_one_per_launch": {"seconds": p_dt, "solves_per_s": len(items) / p_dt,
                                      "states_per_s": total_states / p_dt},

@@ -255,6 +255,8 @@ typedef struct {
     uint64_t pool_bytes;    /* device pool for the instances' two-bit arrays (admission limit) */
     int32_t blocks_per_sm;  /* persistent blocks per SM (0 = 2) */
     int32_t use_graph;      /* 1 = replay each step as a CUDA graph */
+    int32_t direction;      /* PSB_DIR_AUTO (0): each instance's dense late levels run bottom-up;
+                               PSB_DIR_TOP_DOWN: every level top-down */
 } psb_engine_opts;
 int psb_engine_create(const psb_engine_opts* opts, psb_engine** out);
 int psb_engine_destroy(psb_engine* e);

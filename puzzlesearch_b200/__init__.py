@@ -63,7 +63,7 @@ class BfsStats(ctypes.Structure):
 class EngineOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("max_instances", ctypes.c_uint32),
                 ("max_depths", ctypes.c_uint32), ("device", ctypes.c_int32), ("pool_bytes", ctypes.c_uint64),
-                ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32), ("direction", ctypes.c_int32)]
 
 
 class ServerOpts(ctypes.Structure):
@@ -362,8 +362,9 @@ class Engine:
     (batched solves, and continuous batching for serving)."""
 
     def __init__(self, max_instances=4096, max_depths=128, pool_bytes=8 << 30, blocks_per_sm=0, use_graph=True,
-                 device=-1):
+                 device=-1, direction="auto"):
         o = EngineOpts()
+        o.direction = DIRECTIONS[direction] if isinstance(direction, str) else int(direction)
         o.struct_size = ctypes.sizeof(EngineOpts)
         o.max_instances = max_instances
         o.max_depths = max_depths

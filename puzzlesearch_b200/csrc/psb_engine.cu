@@ -10,9 +10,14 @@
 //                counts -> the level's (instance, window) work queue
 //   batch_level  (persistent, #SM x k blocks): blocks pull work items and run
 //                the same per-window level pass as psb_bfs (level_window)
+//   retire       (persistent): CUR -> OLD and the depth count for the
+//                instances whose level ran bottom-up (see psb_bfs)
 //   epilogue     (1 block): each instance's count of CUR states becomes its
 //                next per-depth count; an instance whose count is 0 is done
-//                and its slot id is appended to a completion list
+//                and its slot id is appended to a completion list.  It also
+//                picks each instance's next direction with psb_bfs's rule:
+//                bottom-up once the frontier is dense (>= N/64) and larger
+//                than the unvisited states
 //
 // The three launches are captured once as a CUDA graph and replayed; all
 // per-level state lives in device tables, so instances added between
@@ -44,12 +49,15 @@ constexpr int kEMinBlocks = 2;
 constexpr uint32_t kEWindowBitsMax = 16;
 
 struct EngineSlot {
-    LevelArgs args;     // per-instance level arguments (front = marks = its codes)
+    LevelArgs args;     // per-instance level arguments (front = marks = probe = its codes)
     uint8_t* flags[2];  // active-window flags, windows bytes each (see psb_bfs)
     uint32_t type;      // EngineType
     uint32_t state;     // 0 free, 1 active, 2 done (waiting for the host to collect)
     uint32_t depth;     // counts recorded so far
     uint32_t windows;   // windows of this instance
+    uint32_t bu;        // this level runs bottom-up
+    uint32_t can_bu;    // the puzzle allows bottom-up levels (not Hanoi with symmetry)
+    uint64_t seen;      // states at depths below the current frontier's
 };
 
 struct EngineDev {
@@ -58,6 +66,7 @@ struct EngineDev {
     unsigned long long* counts;  // max_depths per slot
     uint32_t* item_start;        // n_slots + 1
     uint32_t* queue_head;
+    uint32_t* retire_head;       // work-queue counter of the retire pass
     uint32_t* n_items;
     uint32_t* done_list;         // slot ids, ring of n_slots
     uint32_t* done_count;        // monotonically increasing
@@ -106,6 +115,7 @@ __global__ void __launch_bounds__(1024) engine_build_queue(EngineDev d) {
         d.item_start[d.n_slots] = carry;
         *d.n_items = carry;
         *d.queue_head = 0;
+        *d.retire_head = 0;
     }
 }
 
@@ -124,6 +134,30 @@ __device__ __forceinline__ void engine_window(const LevelArgs& a, uint64_t windo
     if constexpr (T == kE_P11) level_window<PancakeK<11>, kTwoBit, kEThreads>(a, window, smem, sh);
     if constexpr (T == kE_P12) level_window<PancakeK<12>, kTwoBit, kEThreads>(a, window, smem, sh);
     if constexpr (T == kE_H) level_window<HanoiK, kTwoBit, kEThreads>(a, window, smem, sh);
+}
+
+template <int T>
+__device__ __forceinline__ void engine_window_bu(const LevelArgs& a, uint64_t window, unsigned long long* smem,
+                                                 WindowShared& sh) {
+    if constexpr (T == kE_S6) level_window<SlidingK<6>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_S8) level_window<SlidingK<8>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_S9) level_window<SlidingK<9>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_S10) level_window<SlidingK<10>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_S12) level_window<SlidingK<12>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_P7) level_window<PancakeK<7>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_P8) level_window<PancakeK<8>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_P9) level_window<PancakeK<9>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_P10) level_window<PancakeK<10>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_P11) level_window<PancakeK<11>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_P12) level_window<PancakeK<12>, kTwoBit, kEThreads, true>(a, window, smem, sh);
+    if constexpr (T == kE_H) level_window<HanoiK, kTwoBit, kEThreads, true>(a, window, smem, sh);
+}
+
+template <int T>
+__device__ __forceinline__ void engine_pass(bool bu, const LevelArgs& a, uint64_t window, unsigned long long* smem,
+                                            WindowShared& sh) {
+    if (bu) engine_window_bu<T>(a, window, smem, sh);
+    else engine_window<T>(a, window, smem, sh);
 }
 
 __global__ void __launch_bounds__(kEThreads, kEMinBlocks) engine_level(EngineDev d) {
@@ -145,21 +179,56 @@ __global__ void __launch_bounds__(kEThreads, kEMinBlocks) engine_level(EngineDev
         }
         const LevelArgs la = d.slots[lo].args;  // uniform loads: one copy per thread, broadcast by L1
         const uint32_t type = d.slots[lo].type;
+        const bool bu = d.slots[lo].bu != 0;
         const uint64_t window = item - d.item_start[lo];
         switch (type) {
-        case kE_S6: engine_window<kE_S6>(la, window, smem64, sh); break;
-        case kE_S8: engine_window<kE_S8>(la, window, smem64, sh); break;
-        case kE_S9: engine_window<kE_S9>(la, window, smem64, sh); break;
-        case kE_S10: engine_window<kE_S10>(la, window, smem64, sh); break;
-        case kE_S12: engine_window<kE_S12>(la, window, smem64, sh); break;
-        case kE_P7: engine_window<kE_P7>(la, window, smem64, sh); break;
-        case kE_P8: engine_window<kE_P8>(la, window, smem64, sh); break;
-        case kE_P9: engine_window<kE_P9>(la, window, smem64, sh); break;
-        case kE_P10: engine_window<kE_P10>(la, window, smem64, sh); break;
-        case kE_P11: engine_window<kE_P11>(la, window, smem64, sh); break;
-        case kE_P12: engine_window<kE_P12>(la, window, smem64, sh); break;
-        default: engine_window<kE_H>(la, window, smem64, sh); break;
+        case kE_S6: engine_pass<kE_S6>(bu, la, window, smem64, sh); break;
+        case kE_S8: engine_pass<kE_S8>(bu, la, window, smem64, sh); break;
+        case kE_S9: engine_pass<kE_S9>(bu, la, window, smem64, sh); break;
+        case kE_S10: engine_pass<kE_S10>(bu, la, window, smem64, sh); break;
+        case kE_S12: engine_pass<kE_S12>(bu, la, window, smem64, sh); break;
+        case kE_P7: engine_pass<kE_P7>(bu, la, window, smem64, sh); break;
+        case kE_P8: engine_pass<kE_P8>(bu, la, window, smem64, sh); break;
+        case kE_P9: engine_pass<kE_P9>(bu, la, window, smem64, sh); break;
+        case kE_P10: engine_pass<kE_P10>(bu, la, window, smem64, sh); break;
+        case kE_P11: engine_pass<kE_P11>(bu, la, window, smem64, sh); break;
+        case kE_P12: engine_pass<kE_P12>(bu, la, window, smem64, sh); break;
+        default: engine_pass<kE_H>(bu, la, window, smem64, sh); break;
         }
+    }
+}
+
+// After a bottom-up level: the instance's CUR codes become OLD and are
+// counted (the depth's count, stats[4]), window by window as in retire_two_bit.
+__global__ void __launch_bounds__(256) engine_retire(EngineDev d) {
+    __shared__ uint32_t s_item;
+    const uint32_t n_items = *d.n_items;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(d.retire_head, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        __syncthreads();
+        if (item >= n_items) break;
+        uint32_t lo = 0, hi = d.n_slots;  // item_start[lo] <= item < item_start[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (d.item_start[mid] <= item) lo = mid; else hi = mid;
+        }
+        const EngineSlot& slot = d.slots[lo];
+        if (!slot.bu) continue;  // uniform: the whole block skips the item
+        const LevelArgs& a = slot.args;
+        const uint64_t window = item - d.item_start[lo];
+        const uint64_t w0 = (window << a.window_bits) >> 5, nw = (uint64_t(1) << a.window_bits) >> 5;
+        unsigned long long* codes = reinterpret_cast<unsigned long long*>(a.front);
+        uint32_t c = 0;
+        for (uint64_t i = w0 + threadIdx.x; i < w0 + nw && i < a.front_words; i += blockDim.x) {
+            const uint64_t x = codes[i], hib = x & kEven, lob = (x >> 1) & kEven;
+            const uint64_t cur = hib & (a.cur_code == 3 ? lob : ~lob);
+            if (cur) codes[i] = x ^ (cur | (a.cur_code == 2 ? (cur << 1) : 0));
+            c += __popcll(cur);
+        }
+        c = __reduce_add_sync(0xFFFFFFFFu, c);
+        if ((threadIdx.x & 31) == 0 && c) atomicAdd(&a.stats[4], (unsigned long long)c);
     }
 }
 
@@ -171,7 +240,8 @@ __global__ void __launch_bounds__(1024) engine_epilogue(EngineDev d) {
         if (slot.state != 1) continue;
         unsigned long long* st = d.stats + 8ull * s;
         if (st[3]) atomicOr(d.err, 1ull);
-        const unsigned long long count = st[0];
+        const unsigned long long count = slot.bu ? st[4] : st[0];  // this depth's states
+        const unsigned long long next_est = st[5];                 // the next frontier (estimate)
         for (int k = 0; k < 8; k++) st[k] = 0;
         if (count == 0 || slot.depth >= d.max_depths) {
             if (count != 0) atomicOr(d.err, 2ull);  // more depths than the engine records
@@ -183,12 +253,16 @@ __global__ void __launch_bounds__(1024) engine_epilogue(EngineDev d) {
         d.counts[uint64_t(s) * d.max_depths + slot.depth] = count;
         slot.depth++;
         slot.args.cur_code = 5u - slot.args.cur_code;
+        slot.seen += count;
+        const uint64_t n = slot.args.n_states;
+        const uint64_t unvisited = n - (slot.seen + next_est < n ? slot.seen + next_est : n);
+        slot.bu = (slot.can_bu && next_est >= n / 64 && unvisited < next_est) ? 1u : 0u;
         // Active-window flags, the psb_bfs policy: the flags this level
         // recorded (if it recorded any) steer the next level's sweep, and the
         // next level records flags when this level's frontier is sparse.
         uint8_t* produced = slot.args.wflag_next;
         slot.args.wflag_cur = produced;
-        if (count < slot.args.n_states / 64) {
+        if (!slot.bu && count < slot.args.n_states / 64) {  // bottom-up levels record no flags
             uint8_t* other = produced == slot.flags[0] ? slot.flags[1] : slot.flags[0];
             uint4* z = reinterpret_cast<uint4*>(other);
             for (uint32_t i = 0; i < (slot.windows + 15) / 16; i++) z[i] = make_uint4(0, 0, 0, 0);
@@ -238,6 +312,7 @@ struct psb_engine {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool use_graph = true;
+    bool bottom_up = true;  // instances may run bottom-up levels
     unsigned grid = 0;
     size_t smem = 0;
     uint64_t levels_run = 0;
@@ -341,6 +416,7 @@ int record_step(psb_engine* e) {
     cudaStream_t s = e->stream;
     psb::engine_build_queue<<<1, 1024, 0, s>>>(e->d);
     psb::engine_level<<<e->grid, psb::kEThreads, e->smem, s>>>(e->d);
+    psb::engine_retire<<<e->grid, 256, 0, s>>>(e->d);
     psb::engine_epilogue<<<1, 1024, 0, s>>>(e->d);
     EN_CUDA(cudaGetLastError());
     return PSB_OK;
@@ -363,6 +439,7 @@ int psb_engine_create(const psb_engine_opts* opts, psb_engine** out) {
     e->max_depths = opts->max_depths;
     e->pool_words = opts->pool_bytes / 8;
     e->use_graph = opts->use_graph != 0;
+    e->bottom_up = opts->direction != PSB_DIR_TOP_DOWN;
     EN_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     EN_CUDA(cudaMalloc(&e->pool, e->pool_words * 8));
     e->free_space[0] = e->pool_words;
@@ -370,13 +447,14 @@ int psb_engine_create(const psb_engine_opts* opts, psb_engine** out) {
     EN_CUDA(cudaMalloc(&e->d.stats, 8 * 8ull * e->n_slots));
     EN_CUDA(cudaMalloc(&e->d.counts, 8ull * e->n_slots * e->max_depths));
     // small counters in one allocation
-    const size_t ints = size_t(e->n_slots + 1) + 4 + 2 * size_t(e->n_slots) + 2;  // + release scratch
+    const size_t ints = size_t(e->n_slots + 1) + 5 + 2 * size_t(e->n_slots) + 2;  // + release scratch
     uint32_t* ib = nullptr;
     EN_CUDA(cudaMalloc(&ib, ints * 4 + 16));
     e->d.item_start = ib;
     e->d.queue_head = ib + e->n_slots + 1;
     e->d.n_items = e->d.queue_head + 1;
-    e->d.done_count = e->d.n_items + 1;
+    e->d.retire_head = e->d.n_items + 1;
+    e->d.done_count = e->d.retire_head + 1;
     e->d.n_active = e->d.done_count + 1;
     e->d.done_list = e->d.n_active + 1;
     EN_CUDA(cudaMalloc(&e->d.err, 8));
@@ -458,6 +536,10 @@ int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial, uint
     slot.flags[1] = slot.flags[0] + flag_words * 4;
     psb::LevelArgs& la = slot.args;
     la.front = la.marks = e->pool + off;
+    la.probe = la.front;
+    slot.bu = 0;
+    slot.can_bu = (e->bottom_up && !(kind == PSB_HANOI4 && b)) ? 1u : 0u;
+    slot.seen = 0;
     la.n_states = p->n_states;
     la.front_words = la.mark_words = (2 * p->n_states + 63) / 64;
     la.window_bits = wb;
