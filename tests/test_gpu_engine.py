@@ -122,3 +122,22 @@ def test_without_graph_same_result():
     a = run_engine(psb.Engine(max_instances=32, pool_bytes=1 << 30, use_graph=True), items)
     b = run_engine(psb.Engine(max_instances=32, pool_bytes=1 << 30, use_graph=False), items)
     assert a == b and len(a) == 20
+
+
+def test_directions_agree_with_single_instance():
+    """Instances with bottom-up levels (the default) and with every level
+    top-down give the same counts as psb_bfs, including Hanoi with symmetry,
+    which never goes bottom-up."""
+    rng = random.Random(77)
+    items = {}
+    for tag in range(28):
+        kind, a, b = TYPES[tag % len(TYPES)]
+        if (kind, a) == ("sliding", 4):
+            continue
+        p = make(kind, a, b)
+        items[tag] = (p, random_start(rng, kind, a, b, p))
+    auto = run_engine(psb.Engine(max_instances=64, pool_bytes=2 << 30), items)
+    top = run_engine(psb.Engine(max_instances=64, pool_bytes=2 << 30, direction="top_down"), items)
+    assert auto == top and set(auto) == set(items)
+    for tag, (p, start) in items.items():
+        assert auto[tag] == psb.bfs(p, "two_bit", start, direction="top_down")["counts"], (tag, p.Name())
