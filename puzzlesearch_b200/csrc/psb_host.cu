@@ -807,7 +807,13 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             launches++;
         }
         PSB_CUDA(cudaEventRecord(S->ev[2], s));
-        if (S->algo == PSB_THREE_BIT || S->algo == PSB_CLASSIC) {
+        const bool bu_three = bu && S->algo == PSB_THREE_BIT;
+        if (bu_three) {
+            // The bottom-up flush already ORed the found states into `visited`,
+            // and they were all unvisited, so new &= ~old (& ~cur) changes
+            // nothing: only `old` must be zeroed for reuse (as finalize does).
+            if (!want_final) PSB_CUDA(cudaMemsetAsync(old_, 0, W1 * 8, s));
+        } else if (S->algo == PSB_THREE_BIT || S->algo == PSB_CLASSIC) {
             const unsigned fgrid = 148 * 8;
             const uint64_t n2 = (W1 + 1) / 2;
             if (S->algo == PSB_THREE_BIT && produce && flags_old != -1 && !want_final)
@@ -856,7 +862,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
 
         switch (S->algo) {
         case PSB_THREE_BIT:
-            count = S->h_stats[4];
+            count = bu_three ? S->h_stats[2] : S->h_stats[4];  // bottom-up: the states found
             if (first) { res.push_back(1); }
             if (count == 0) goto done;
             res.push_back(count);

@@ -934,7 +934,13 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                         ((unsigned long long)bytes_to_bits(smarks + 16 * i + 8) << 32);
                 else
                     v = smem64[i];
-                if (v && (base >> kShift) + i < a.mark_words) atomicOr(g + i, v);
+                if (v && (base >> kShift) + i < a.mark_words) {
+                    atomicOr(g + i, v);
+                    // three-bit bottom-up: the found states join the visited
+                    // array here (only this block writes this window's words),
+                    // so the level needs no finalize sweep
+                    if constexpr (BU && MODE == kThreeBit) a.front[(base >> kShift) + i] |= v;
+                }
             }
         }
     }
