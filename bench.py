@@ -223,7 +223,7 @@ def solvable_start(rng, kind, a, b, puzzle):
 
 
 def batch_bench(args):
-    """4096 independent two-bit searches drawn from a seed,
+    """Batched solves: 4096 independent two-bit searches drawn from a seed,
     uniform over sliding 2x3/2x4/3x3/2x5 and pancake 7..11, from random
     solvable starts; batched engine vs one search per launch, counts equal."""
     import random
@@ -265,7 +265,7 @@ def batch_bench(args):
     b_res, b_dt, levels = run_batched()
     p_res, p_dt = run_plain()
     assert b_res == p_res, "batched counts differ from the single-instance path"
-    line = {"metric": "batched solves/s (config 4: 4096 two-bit searches, sliding 2x3/2x4/3x3/2x5 + pancake 7..11)",
+    line = {"metric": "batched solves/s (4096 two-bit searches, sliding 2x3/2x4/3x3/2x5 + pancake 7..11)",
             "value": len(items) / b_dt, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": args.warmup,
             "higher_is_better": True, "dtype": "u64", "data": "seeded random solvable starts",
             "config": {"workload": "batch4096", "instances": len(items), "states": total_states,
@@ -283,7 +283,7 @@ SERVE_TYPES = [("sliding", 2, 4), ("sliding", 3, 3), ("sliding", 2, 5), ("slidin
 
 
 def serve_bench(args):
-    """seeded Poisson request streams (rates 10..2000 req/s),
+    """Served solves: seeded Poisson request streams (rates 10..2000 req/s),
     request type uniform over sliding 2x4/3x3/2x5/3x4, pancake 8..12 and Hanoi
     8..14 disks, random solvable starts.  The server (continuous batching,
     admission by HBM footprint) against plain sequential solves of the same
@@ -346,7 +346,7 @@ def serve_bench(args):
                      "plain": {"solves_per_s": n_req / plain_span, "p50_s": q(pl, 0.5), "p99_s": q(pl, 0.99)},
                      "mean_eccentricity": sum(len(done[k][1]) - 1 for k in tickets) / n_req})
         print(json.dumps({"progress": rows[-1]}), file=sys.stderr, flush=True)
-    line = {"metric": "served solves/s and p50/p99 latency (config 5: Poisson streams, continuous batching)",
+    line = {"metric": "served solves/s and p50/p99 latency (Poisson request streams, continuous batching)",
             "value": max(r["served"]["solves_per_s"] for r in rows), "unit": "solves/s", "n_gpus": 1,
             "higher_is_better": True, "dtype": "u64", "data": "seeded Poisson streams, random solvable starts",
             "config": {"workload": "serve", "types": len(SERVE_TYPES), "pool_gb": args.pool_gb},
