@@ -64,7 +64,7 @@ def test_legacy_sliding_vectors(golden):
 
 
 def test_sliding_3x4_equals_4x3_golden(golden):
-    """3x4 is the transpose of the reference's 4x3 golden
+    """The 3x4 board is the transpose of the reference's 4x3 golden
     (SlidingPuzzleTests/TestFrontierSearch.cpp:70-72): same per-depth counts."""
     v = [x for x in golden["legacy_sliding"] if x["puzzle"] == ["sliding", 4, 3]][0]
     p = psb.SlidingTilePuzzleSimple(3, 4)
