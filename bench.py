@@ -43,6 +43,10 @@ WORKLOADS = {
     # smaller cases of the same kernels, sized for ncu captures (arrays above L2, a few GB at most)
     "hanoi15-2bit": ("hanoi4", 15, 0, "two_bit", "15-disk 4-peg Hanoi in-memory two-bit BFS (profiling case)"),
     "pancake12-3bit": ("pancake", 12, 0, "three_bit", "12-pancake in-memory three-bit BFS (profiling case)"),
+    # the other two in-memory algorithms
+    "hanoi16-frontier": ("hanoi4", 16, 0, "frontier", "16-disk 4-peg Hanoi in-memory frontier search, full solve"),
+    "pancake12-classic": ("pancake", 12, 0, "classic", "12-pancake in-memory classic BFS, full solve from the identity"),
+    "sliding4x3-frontier": ("sliding", 4, 3, "frontier", "4x3 sliding-tile in-memory frontier search, full solve"),
 }
 REF_SAMPLE = ("pancake", 11, 0, "three_bit")  # CPU baseline sample (reference InMemoryThreeBitBFS)
 
@@ -265,7 +269,7 @@ def batch_bench(args):
     b_res, b_dt, levels = run_batched()
     p_res, p_dt = run_plain()
     assert b_res == p_res, "batched counts differ from the single-instance path"
-    line = {"metric": "batched solves/s (4096 two-bit searches, sliding 2x3/2x4/3x3/2x5 + pancake 7..11)",
+    line = {"metric": f"batched solves/s ({len(items)} two-bit searches, sliding 2x3/2x4/3x3/2x5 + pancake 7..11)",
             "value": len(items) / b_dt, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": args.warmup,
             "higher_is_better": True, "dtype": "u64", "data": "seeded random solvable starts",
             "config": {"workload": "batch4096", "instances": len(items), "states": total_states,
