@@ -366,8 +366,10 @@ def profile_once(args):
     kind, a, b, algo, desc = WORKLOADS[args.workload]
     puzzle = {"pancake": lambda: psb.PancakeSimple(a), "sliding": lambda: psb.SlidingTilePuzzleSimple(a, b),
               "hanoi4": lambda: psb.FourPegHanoiSimple(a, bool(b))}[kind]()
+    sink = psb.SPILL_FN(lambda *_: 0) if args.spill else None
     r = psb.bfs(puzzle, algo, 0, max_depth=args.max_depth, window_bits=args.window_bits, levels=True,
-                direction=args.direction, bottom_up_ratio=args.bottom_up_ratio)
+                direction=args.direction, bottom_up_ratio=args.bottom_up_ratio, spill=sink,
+                segment_bits=args.segment_bits)
     out = {"workload": args.workload, "counts": r["counts"], "level_ms": [round(x, 3) for x in r["level_ms"]],
            "level_children": r["level_children"], "stats": r["stats"]}
     print(json.dumps(out), flush=True)
@@ -387,6 +389,10 @@ def main():
                     help="level direction (PSB_DIR_*): auto switches to bottom-up on the last dense levels")
     ap.add_argument("--bottom-up-ratio", type=float, default=0.0,
                     help="auto: a level runs bottom-up when unvisited < ratio x frontier (0 = library default)")
+    ap.add_argument("--spill", action="store_true",
+                    help="encode every depth's frontier on the GPU (segment streams) and hand it over in pinned"
+                         " host memory during the timed searches")
+    ap.add_argument("--segment-bits", type=int, default=0, help="with --spill: 2^bits states per segment (0 = 32)")
     ap.add_argument("--profile-once", action="store_true",
                     help="run ONE search (no warm-up, no e2e, no CPU baseline) and print per-level times; for ncu")
     ap.add_argument("--max-depth", type=int, default=0, help="with --profile-once: stop after this depth")
@@ -426,12 +432,23 @@ def main():
     cap = 1 << 16
     counts = (ctypes.c_uint64 * cap)()
     nd = ctypes.c_uint32()
+    # Frontier spill sink: the streams arrive in the library's pinned host
+    # buffer; this caller only tallies them (a real caller stores them).
+    spilled = {"bytes": 0, "segments": 0, "states": 0}
+
+    def _sink(_user, depth, segment, data, n, states):
+        spilled["bytes"] += n
+        spilled["segments"] += 1
+        spilled["states"] += states
+        return 0
+
+    spill_fn = psb.SPILL_FN(_sink) if args.spill else None
 
     def run_once():
         st = psb.BfsStats()
         st.struct_size = ctypes.sizeof(psb.BfsStats)
         o = psb._opts(0, 0, local, stream.cuda_stream, direction=args.direction,
-                      bottom_up_ratio=args.bottom_up_ratio)
+                      bottom_up_ratio=args.bottom_up_ratio, spill=spill_fn, segment_bits=args.segment_bits)
         psb._check(psb.lib().psb_bfs_session_run(h, 0, ctypes.byref(o), counts, cap, ctypes.byref(nd), ctypes.byref(st)))
         return list(counts[:nd.value]), st
 
@@ -464,7 +481,8 @@ def main():
     # Untimed warm-up calls first, as for the device loop: the first call
     # grows the library's memory pool.
     for _ in range(args.warmup):
-        psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio)
+        psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
+                spill=spill_fn, segment_bits=args.segment_bits)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -472,7 +490,8 @@ def main():
     calls = []
     for _ in range(args.steps):
         tc = time.perf_counter()
-        r = psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio)
+        r = psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
+                    spill=spill_fn, segment_bits=args.segment_bits)
         calls.append(time.perf_counter() - tc)
         assert r["counts"] == ref_counts
         levels = r["stats"]["levels"]
@@ -504,7 +523,10 @@ def main():
     # level kernels + one finalize per level (three-bit, classic) or one
     # CUR -> OLD pass per bottom-up level (two-bit)
     launches_per_step = st.levels + (st.levels if algo in ("three_bit", "classic") else st.bottom_up_levels)
+    launches_per_step += st.spill_launches
 
+    if args.spill:
+        desc += "; every depth's frontier encoded on the GPU and spilled to pinned host memory"
     line = {
         "metric": f"BFS states/sec ({desc})", "value": value, "unit": "states/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
@@ -528,6 +550,16 @@ def main():
         "direction": {"mode": args.direction, "bottom_up_levels": st.bottom_up_levels, "levels": st.levels},
         "clocks": clk.summary(),
     }
+    if args.spill:
+        line["spill"] = {"segment_bits": args.segment_bits or 32, "bytes_per_step": st.spill_bytes,
+                         "segments_per_step": st.spill_segments,
+                         "ms_per_step": sum(s.spill_ms for s in stats) / len(stats),
+                         "encode_ms_per_step": sum(s.spill_encode_ms for s in stats) / len(stats),
+                         "copy_ms_per_step": sum(s.spill_copy_ms for s in stats) / len(stats),
+                         "copy_gbs": st.spill_bytes / max(st.spill_copy_ms, 1e-9) / 1e6,
+                         "bytes_per_state": st.spill_bytes / states_per_step,
+                         "d2h_bytes_per_step": st.spill_bytes}
+        line["e2e"]["d2h_bytes_per_step"] += st.spill_bytes
     if not args.no_cpu_baseline and world == 1:
         s, secs, ck = cpu_reference_sample()
         line["cpu_baseline"] = {"value": s / secs, "unit": "states/s", "cores": 1, "kind": ck,

@@ -37,7 +37,8 @@ enum {
     PSB_ERR_CAPACITY = -4,    /* an output buffer is too small */
     PSB_ERR_UNSUPPORTED = -5, /* combination not supported (e.g. frontier search with > 4 operators) */
     PSB_ERR_DEVICE = -6,      /* a kernel reported an internal error (index out of range) */
-    PSB_ERR_NO_DEVICE = -7    /* no CUDA device visible */
+    PSB_ERR_NO_DEVICE = -7,   /* no CUDA device visible */
+    PSB_ERR_ABORTED = -8      /* a callback (psb_spill_fn) returned non-zero */
 };
 
 /* Puzzle kinds (the reference's *Simple classes). */
@@ -100,6 +101,16 @@ int psb_expand(const psb_puzzle* p, const uint64_t* parents, const uint32_t* opb
 
 /* --- In-memory BFS (Common/InMemoryBFS.h:5-11) ----------------------------- */
 
+/* Frontier spill: receives one segment of one depth's frontier as the
+ * reference's compressed segment stream (see psb_frontier_encode), in pinned
+ * host memory that stays valid until the callback returns.  `states` =
+ * offsets in the stream; the segment holds states
+ * segment * 2^segment_bits ... (SegmentedOptions::GetSegIdx,
+ * Common/DiskBasedBFS.h:22-24).  Non-zero ends the search with
+ * PSB_ERR_ABORTED. */
+typedef int (*psb_spill_fn)(void* user, uint32_t depth, uint32_t segment, const uint8_t* stream, uint64_t bytes,
+                            uint64_t states);
+
 typedef struct {
     uint32_t struct_size;  /* sizeof(psb_bfs_opts) */
     uint32_t max_depth;    /* stop after this depth (0 = until the frontier is empty; PuzzleOptions::maxSteps, Common/DiskBasedBFS.h:10) */
@@ -113,7 +124,28 @@ typedef struct {
                               (two-bit writes one more entry, for its final empty sweep, when it fits) */
     int32_t direction;     /* PSB_DIR_AUTO (0), PSB_DIR_TOP_DOWN or PSB_DIR_BOTTOM_UP; see below */
     float bottom_up_ratio; /* PSB_DIR_AUTO: a dense level runs bottom-up when unvisited < ratio * frontier (0 = 1.0) */
+    psb_spill_fn spill;    /* optional: every depth's frontier, encoded on the GPU segment by segment (below) */
+    void* spill_user;      /* first argument of spill */
+    int32_t segment_bits;  /* states per spilled segment = 2^segment_bits, 6..32 (0 = 32, the reference's largest) */
 } psb_bfs_opts;
+
+/* With opts->spill set, the states at each depth d = 0, 1, ... (every depth
+ * the counts report) are encoded on the GPU, segment by segment, into the
+ * reference's CompressedSegmentWriter stream (Common/CompressedFrontier.cpp:
+ * 103-140) and copied to pinned host memory; spill(user, d, segment, ...)
+ * then receives each one, on the calling thread.  Calls come in ascending
+ * (depth, segment) order, all before psb_bfs returns; empty segments are
+ * skipped, as the reference writes nothing for them.  Depth d is encoded on
+ * the GPU before the level that expands it; its copies to the host and its
+ * callbacks run while that level is on the GPU.
+ * This replaces SegmentWriter's files with pinned host buffers: the caller
+ * keeps, writes or drops each stream.  The spill's memory (an extracted
+ * segment bitmap for two-bit and frontier searches, the encoder's offset
+ * list, about 7 bytes per frontier state of a segment, a device arena for
+ * one depth's streams and two pinned host buffers of one segment's stream)
+ * is allocated on first use, kept for the
+ * device's next searches and freed by psb_release_cached_memory; it is not
+ * part of psb_bfs_footprint. */
 
 /* Level direction.  A top-down level expands every frontier state and marks
  * its children, as the reference does.  A bottom-up level (three-bit,
@@ -141,6 +173,13 @@ typedef struct {
     uint64_t expand_launches; /* level-kernel launches (one per level) */
     uint64_t device_bytes;    /* device memory held by the search */
     uint64_t bottom_up_levels; /* levels that ran bottom-up (their "children" are probes) */
+    double spill_ms;          /* host time in the spill: encoding plus handing over (the latter overlaps the
+                                 level that follows) */
+    uint64_t spill_bytes;     /* stream bytes passed to the spill callback */
+    uint64_t spill_segments;  /* callback calls */
+    uint64_t spill_launches;  /* kernels the spill launched (extraction and encoding) */
+    double spill_encode_ms;   /* host time encoding depths (the search waits for it) */
+    double spill_copy_ms;     /* device time of the copies to pinned host memory */
 } psb_bfs_stats;
 
 /* Size in 64-bit words of the final arrays that psb_bfs copies out:
@@ -173,7 +212,8 @@ int psb_bfs_session_destroy(psb_bfs_session* s);
 /* Search arrays (psb_bfs and sessions) come from a per-device memory pool
  * that keeps freed memory reserved for the next search instead of returning
  * it to the driver after every call.  This returns the reserved memory of
- * `device` (-1 = current) to the driver; it waits for the device first. */
+ * `device` (-1 = current) to the driver, and frees the frontier spill's
+ * cached buffers; it waits for the device first. */
 int psb_release_cached_memory(int device);
 
 /* --- Device bit arrays (Common/BitArray.h:69-169) -------------------------

@@ -45,6 +45,7 @@ def lib():
         L.orc_bfs.argtypes = [P, ctypes.c_int, ctypes.c_uint64, u64p, ctypes.c_int, u64p, ctypes.c_uint64]
         L.orc_final_words.restype = ctypes.c_uint64
         L.orc_final_words.argtypes = [P, ctypes.c_int]
+        L.orc_depths.argtypes = [P, ctypes.c_uint64, ctypes.c_void_p]
         L.orc_perm_rank.restype = ctypes.c_uint64
         L.orc_perm_rank.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.orc_perm_unrank.argtypes = [ctypes.c_uint64, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
@@ -118,6 +119,18 @@ def bfs(spec, algo, initial=0, final=False):
     if n < 0:
         raise RuntimeError(f"orc_bfs failed {n}")
     return list(counts[:n]), (list(fin) if final else None)
+
+
+def depths(spec, initial=0):
+    """Distance of every state from initial as a numpy uint8 array (255 = not
+    reached), and the number of depths."""
+    import numpy as np
+    n = info(spec)["indexes"]
+    d = np.empty(n, dtype=np.uint8)
+    k = lib().orc_depths(_p(spec), initial, d.ctypes.data)
+    if k < 0:
+        raise RuntimeError(f"orc_depths failed {k}")
+    return d, k
 
 
 def perm_rank(perm):

@@ -492,6 +492,30 @@ int orc_bfs(const orc_puzzle* p, int algo, uint64_t initial, uint64_t* counts, i
     return -1;
 }
 
+/* Distance of every state from `initial` (255 = not reached), by the level
+ * sweep of InMemoryClassicBFS.cpp:4-45 over the same expander: the set of
+ * states at each depth, which a spilled frontier is checked against.
+ * Returns the number of depths, or <0 on error (-2: more than 254 depths). */
+int orc_depths(const orc_puzzle* p, uint64_t initial, uint8_t* depth) {
+    uint64_t N; int ops, odd;
+    if (orc_info(p, &N, &ops, 0, &odd) || initial >= N) return -1;
+    memset(depth, 255, N);
+    depth[initial] = 0;
+    uint64_t ch[ORC_MAXBR]; uint32_t chops[ORC_MAXBR];
+    for (int d = 0;; d++) {
+        if (d >= 254) return -2;
+        uint64_t found = 0;
+        for (uint64_t i = 0; i < N; i++) {
+            if (depth[i] != d) continue;
+            emitter e = { ch, chops, ORC_MAXBR, 0, 0 };
+            expand_one(p, i, 0, &e);
+            for (uint64_t k = 0; k < e.n; k++)
+                if (depth[ch[k]] == 255) { depth[ch[k]] = (uint8_t)(d + 1); found++; }
+        }
+        if (!found) return d + 1;
+    }
+}
+
 /* ------------------------------------------------------------------------- */
 /* StreamVInt: Common/StreamVInt.cpp                                           */
 /* ------------------------------------------------------------------------- */

@@ -62,6 +62,9 @@ int64_t orc_expand(const orc_puzzle* p, const uint64_t* parents, const uint32_t*
 int orc_bfs(const orc_puzzle* p, int algo, uint64_t initial, uint64_t* counts, int counts_cap,
             uint64_t* final_words, uint64_t final_words_cap);
 uint64_t orc_final_words(const orc_puzzle* p, int algo);
+/* Distance of every state from initial (depth[N]; 255 = not reached).
+ * Returns the number of depths, <0 on error. */
+int orc_depths(const orc_puzzle* p, uint64_t initial, uint8_t* depth);
 
 /* StreamVInt (Common/StreamVInt.cpp) -- byte-exact format. */
 int orc_svi_encode_tuple(const uint32_t* v4, uint8_t* out);       /* returns bytes (5..17) */

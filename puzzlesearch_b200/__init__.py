@@ -39,12 +39,18 @@ class PsbError(RuntimeError):
         self.code = code
 
 
+# psb_spill_fn(user, depth, segment, stream, bytes, states)
+SPILL_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                            ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, ctypes.c_uint64)
+
+
 class BfsOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
                 ("window_bits", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("stream", ctypes.c_void_p), ("final_words", u64p), ("final_cap", ctypes.c_uint64),
                 ("level_ms", ctypes.POINTER(ctypes.c_float)), ("level_children", u64p),
-                ("direction", ctypes.c_int32), ("bottom_up_ratio", ctypes.c_float)]
+                ("direction", ctypes.c_int32), ("bottom_up_ratio", ctypes.c_float),
+                ("spill", SPILL_FN), ("spill_user", ctypes.c_void_p), ("segment_bits", ctypes.c_int32)]
 
 
 class BfsStats(ctypes.Structure):
@@ -54,7 +60,10 @@ class BfsStats(ctypes.Structure):
                 ("finalize_ms", ctypes.c_double), ("expanded", ctypes.c_uint64),
                 ("children", ctypes.c_uint64), ("local_children", ctypes.c_uint64),
                 ("expand_launches", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64),
-                ("bottom_up_levels", ctypes.c_uint64)]
+                ("bottom_up_levels", ctypes.c_uint64), ("spill_ms", ctypes.c_double),
+                ("spill_bytes", ctypes.c_uint64), ("spill_segments", ctypes.c_uint64),
+                ("spill_launches", ctypes.c_uint64), ("spill_encode_ms", ctypes.c_double),
+                ("spill_copy_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}
@@ -275,9 +284,24 @@ def _algo(algo):
 DIRECTIONS = {"auto": 0, "top_down": 1, "bottom_up": 2}
 
 
+def _spill_fn(spill):
+    """Wraps spill(depth, segment, stream_bytes, states) -> stop (truthy ends
+    the search with PSB_ERR_ABORTED) as a psb_spill_fn.  The stream is copied
+    out of the pinned staging buffer before spill is called."""
+    def fn(_user, depth, segment, data, n, states):
+        try:
+            return 1 if spill(depth, segment, ctypes.string_at(data, n), states) else 0
+        except Exception:  # an exception cannot cross the C ABI: stop the search
+            return 1
+    return SPILL_FN(fn)
+
+
 def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_ms=None, level_children=None,
-          direction="auto", bottom_up_ratio=0.0):
+          direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0):
     o = BfsOpts()
+    if spill is not None:
+        o.spill = spill  # a SPILL_FN the caller keeps alive for the call
+        o.segment_bits = segment_bits
     o.struct_size = ctypes.sizeof(BfsOpts)
     o.direction = DIRECTIONS[direction] if isinstance(direction, str) else int(direction)
     o.bottom_up_ratio = bottom_up_ratio
@@ -296,10 +320,14 @@ def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_
 
 
 def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels=False, device=-1,
-        direction="auto", bottom_up_ratio=0.0):
+        direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0):
     """Runs psb_bfs.  Returns a dict with counts, stats and optionally the final
     arrays (list of 64-bit words in the reference's layout) and per-level data.
-    direction: "auto", "top_down" or "bottom_up" (PSB_DIR_*)."""
+    direction: "auto", "top_down" or "bottom_up" (PSB_DIR_*).
+    spill: optional callable(depth, segment, stream_bytes, states) receiving
+    every depth's frontier as compressed segment streams (2^segment_bits
+    states per segment, 0 = 2^32); a truthy return stops the search.  A
+    SPILL_FN is passed through as is (it sees the pinned buffer itself)."""
     if isinstance(initial, str):
         initial = puzzle.Parse(initial)
     cap = 1 << 16
@@ -310,7 +338,8 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
         fin = (ctypes.c_uint64 * puzzle.final_words(algo))()
     lm = (ctypes.c_float * cap)() if levels else None
     lc = (ctypes.c_uint64 * cap)() if levels else None
-    o = _opts(max_depth, window_bits, device, None, fin, lm, lc, direction, bottom_up_ratio)
+    fn = spill if isinstance(spill, SPILL_FN) or spill is None else _spill_fn(spill)
+    o = _opts(max_depth, window_bits, device, None, fin, lm, lc, direction, bottom_up_ratio, fn, segment_bits)
     st = BfsStats()
     st.struct_size = ctypes.sizeof(BfsStats)
     _check(lib().psb_bfs(puzzle.handle, _algo(algo), initial, ctypes.byref(o), counts, cap, ctypes.byref(nd),
@@ -338,11 +367,13 @@ class BfsSession:
         self._cap = 1 << 16
         self._counts = (ctypes.c_uint64 * self._cap)()
 
-    def run(self, initial=0, max_depth=0, bottom_up_ratio=0.0):
+    def run(self, initial=0, max_depth=0, bottom_up_ratio=0.0, spill=None, segment_bits=0):
         nd = ctypes.c_uint32()
         st = BfsStats()
         st.struct_size = ctypes.sizeof(BfsStats)
-        o = _opts(max_depth, direction=self.direction, bottom_up_ratio=bottom_up_ratio)
+        fn = _spill_fn(spill) if spill is not None else None
+        o = _opts(max_depth, direction=self.direction, bottom_up_ratio=bottom_up_ratio, spill=fn,
+                  segment_bits=segment_bits)
         _check(lib().psb_bfs_session_run(self._h, initial, ctypes.byref(o), self._counts, self._cap,
                                          ctypes.byref(nd), ctypes.byref(st)))
         return list(self._counts[:nd.value]), st.as_dict()

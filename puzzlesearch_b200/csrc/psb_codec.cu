@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -124,9 +125,25 @@ __global__ void k_group_scan(unsigned long long* v, uint64_t n, const unsigned l
     }
 }
 
-// Writes the ascending offsets of all set bits: offset list position = rank.
+__device__ __forceinline__ uint32_t vbytes(uint32_t x) { return x >> 24 ? 4 : x >> 16 ? 3 : x >> 8 ? 2 : 1; }
+
+struct BlockInfo {
+    unsigned long long out_off;  // byte offset of the block in the stream
+    uint32_t count, first, last, is_bitmap;
+    unsigned long long bytes;
+};
+
+// A StreamVInt block in tuple order: its first tuple and its block number.
+struct SviRef {
+    unsigned long long tuple0;
+    uint32_t block, pad;
+};
+
+// Writes the ascending offsets of the set bits that fall in StreamVInt
+// blocks, at their rank (offset list position = rank; bitmap blocks need no
+// list: their words are copied from the bitmap).
 __global__ void k_compact(const uint64_t* bits, uint64_t n_words, uint64_t n_bits, const unsigned long long* bsum,
-                          uint32_t* idx) {
+                          const BlockInfo* blocks, uint32_t* idx) {
     // Recompute the per-word exclusive rank inside the block (16 words per thread, interleaved).
     __shared__ uint32_t s[kT];
     const uint64_t base = uint64_t(blockIdx.x) * kT * 16;
@@ -144,11 +161,15 @@ __global__ void k_compact(const uint64_t* bits, uint64_t n_words, uint64_t n_bit
             __syncthreads();
         }
         unsigned long long r = run + s[threadIdx.x] - c;
-        uint64_t m = word;
-        while (m) {
-            const uint32_t j = __ffsll((long long)m) - 1;
-            m &= m - 1;
-            idx[r++] = uint32_t(w * 64 + j);
+        // c <= 64 < kBlock: the word's offsets lie in at most two blocks
+        if (c && !(blocks[r / kBlock].is_bitmap && blocks[(r + c - 1) / kBlock].is_bitmap)) {
+            uint64_t m = word;
+            while (m) {
+                const uint32_t j = __ffsll((long long)m) - 1;
+                m &= m - 1;
+                if (!blocks[r / kBlock].is_bitmap) idx[r] = uint32_t(w * 64 + j);
+                r++;
+            }
         }
         const uint32_t tot = s[kT - 1];
         __syncthreads();
@@ -156,14 +177,67 @@ __global__ void k_compact(const uint64_t* bits, uint64_t n_words, uint64_t n_bit
     }
 }
 
-__device__ __forceinline__ uint32_t vbytes(uint32_t x) { return x >> 24 ? 4 : x >> 16 ? 3 : x >> 8 ? 2 : 1; }
+// First and last offset of every block (ranks b * kBlock and the block's
+// last rank), by select: the chunk holding the rank from the chunk prefix
+// sums (bsum, chunks of kT * 16 words), then a warp scan of that chunk's
+// words.  One warp per (block, end); warps 2b and 2b + 1 serve block b.
+__global__ void k_select_blocks(const uint64_t* bits, uint64_t n_words, uint64_t n_bits,
+                                const unsigned long long* bsum, uint64_t nbs, uint64_t count, BlockInfo* blocks,
+                                uint32_t nb) {
+    const uint64_t gw = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) / 32;  // uniform in a warp
+    const int lane = threadIdx.x & 31;
+    if (gw >= 2ull * nb) return;
+    const uint32_t b = uint32_t(gw / 2);
+    const bool last = gw & 1;
+    const uint64_t end = (uint64_t(b) + 1) * kBlock < count ? (uint64_t(b) + 1) * kBlock : count;
+    const uint64_t r = last ? end - 1 : uint64_t(b) * kBlock;
+    uint64_t lo = 0, hi = nbs;  // largest chunk lo with bsum[lo] <= r (bsum[0] = 0)
+    while (hi - lo > 1) {
+        const uint64_t mid = (lo + hi) / 2;
+        if (bsum[mid] <= r) lo = mid; else hi = mid;
+    }
+    uint64_t rem = r - bsum[lo];
+    const uint64_t w_end = (lo + 1) * kT * 16 < n_words ? (lo + 1) * kT * 16 : n_words;
+    for (uint64_t w0 = lo * kT * 16; w0 < w_end; w0 += 32) {
+        const uint64_t w = w0 + lane;
+        const uint64_t v = w < w_end ? masked_word(bits, w, n_words, n_bits) : 0;
+        const uint32_t c = __popcll(v);
+        uint32_t inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
+        if (rem < total) {
+            const uint32_t exc = inc - c;
+            if (rem >= exc && rem < inc) {  // exactly one lane
+                uint64_t x = v;
+                for (uint64_t i = exc; i < rem; ++i) x &= x - 1;
+                const uint32_t pos = uint32_t(w * 64 + (__ffsll((long long)x) - 1));
+                if (last) blocks[b].last = pos; else blocks[b].first = pos;
+            }
+            return;
+        }
+        rem -= total;
+    }
+}
 
-struct BlockInfo {
-    unsigned long long out_off;  // byte offset of the block in the stream
-    uint32_t count, first, last, is_bitmap;
-    unsigned long long bytes;
-    unsigned long long tuple0;   // first tuple (StreamVInt blocks)
-};
+// FrontierCompression::Encode (FrontierCompression.cpp:92-102): a block is a
+// bitmap block when it holds more than 128 offsets and its bitmap is smaller
+// than 10 bits per offset.
+__global__ void k_block_decide(uint64_t count, BlockInfo* blocks, uint32_t nb) {
+    const uint32_t b = blockIdx.x * kT + threadIdx.x;
+    if (b >= nb) return;
+    BlockInfo& bi = blocks[b];
+    const uint64_t r0 = uint64_t(b) * kBlock;
+    const uint32_t n = uint32_t(count - r0 < kBlock ? count - r0 : kBlock);
+    bi.count = n;
+    const uint64_t bm_bytes = (uint64_t(bi.last) - bi.first + 63) / 64 * 8 + 8;
+    bi.is_bitmap = (n > 128 && bm_bytes * 8 < uint64_t(n) * 10 - 8) ? 1 : 0;
+    bi.bytes = bi.is_bitmap ? bm_bytes : 0;
+    bi.out_off = 0;
+}
 
 // Value of rank position k (0-based) of block b after the in-place delta, 0 past the count.
 __device__ __forceinline__ uint32_t delta_at(const uint32_t* idx, uint64_t r0, uint32_t count, uint32_t k) {
@@ -172,44 +246,49 @@ __device__ __forceinline__ uint32_t delta_at(const uint32_t* idx, uint64_t r0, u
     return k == 0 ? v : v - idx[r0 + k - 1];
 }
 
-// Tuple lengths of every StreamVInt block (bitmap blocks contribute zero).
-__global__ void k_tuple_len(const uint32_t* idx, const BlockInfo* blocks, uint32_t nb, uint64_t tuples,
-                            unsigned long long* tlen) {
+// The StreamVInt block that holds tuple t (the last ref with tuple0 <= t).
+__device__ __forceinline__ uint32_t svi_of(const SviRef* refs, uint32_t n_refs, uint64_t t) {
+    uint32_t lo = 0, hi = n_refs;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (refs[mid].tuple0 <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Tuple lengths of the StreamVInt blocks: 1 descriptor byte + 1..4 bytes per value.
+__global__ void k_tuple_len(const uint32_t* idx, const BlockInfo* blocks, const SviRef* refs, uint32_t n_refs,
+                            uint64_t tuples, unsigned long long* tlen) {
     const uint64_t t = blockIdx.x * uint64_t(kT) + threadIdx.x;
     if (t >= tuples) return;
-    const uint32_t b = uint32_t(t / (kBlock / 4));
-    const uint32_t k = uint32_t(t % (kBlock / 4)) * 4;
-    const BlockInfo bi = blocks[b];
-    const uint32_t padded = (bi.count + 7) / 8 * 8;
-    if (bi.is_bitmap || k >= padded) { tlen[t] = 0; return; }
-    const uint64_t r0 = uint64_t(b) * kBlock;
+    const SviRef ref = refs[svi_of(refs, n_refs, t)];
+    const uint32_t k = uint32_t(t - ref.tuple0) * 4;
+    const uint32_t count = blocks[ref.block].count;
+    const uint64_t r0 = uint64_t(ref.block) * kBlock;
     uint32_t len = 1;
-    for (int q = 0; q < 4; ++q) len += vbytes(delta_at(idx, r0, bi.count, k + q));
+    for (int q = 0; q < 4; ++q) len += vbytes(delta_at(idx, r0, count, k + q));
     tlen[t] = len;
 }
 
-__global__ void k_block_bytes(BlockInfo* blocks, uint32_t nb, const unsigned long long* tscan, uint64_t tuples,
-                              unsigned long long total) {
-    const uint32_t b = blockIdx.x * kT + threadIdx.x;
-    if (b >= nb) return;
-    BlockInfo& bi = blocks[b];
-    if (bi.is_bitmap) return;
-    const uint64_t t0 = bi.tuple0, t1 = t0 + (bi.count + 7) / 8 * 2;
+__global__ void k_block_bytes(BlockInfo* blocks, const SviRef* refs, uint32_t n_refs,
+                              const unsigned long long* tscan, uint64_t tuples, unsigned long long total) {
+    const uint32_t j = blockIdx.x * kT + threadIdx.x;
+    if (j >= n_refs) return;
+    BlockInfo& bi = blocks[refs[j].block];
+    const uint64_t t0 = refs[j].tuple0, t1 = j + 1 < n_refs ? refs[j + 1].tuple0 : tuples;
     const unsigned long long end = t1 < tuples ? tscan[t1] : total;
     bi.bytes = 4 + (end - tscan[t0]);
 }
 
-__global__ void k_write_svi(const uint32_t* idx, const BlockInfo* blocks, uint64_t tuples,
-                            const unsigned long long* tscan, uint8_t* out) {
+__global__ void k_write_svi(const uint32_t* idx, const BlockInfo* blocks, const SviRef* refs, uint32_t n_refs,
+                            uint64_t tuples, const unsigned long long* tscan, uint8_t* out) {
     const uint64_t t = blockIdx.x * uint64_t(kT) + threadIdx.x;
     if (t >= tuples) return;
-    const uint32_t b = uint32_t(t / (kBlock / 4));
-    const uint32_t k = uint32_t(t % (kBlock / 4)) * 4;
-    const BlockInfo bi = blocks[b];
-    const uint32_t padded = (bi.count + 7) / 8 * 8;
-    if (bi.is_bitmap || k >= padded) return;
-    const uint64_t r0 = uint64_t(b) * kBlock;
-    uint8_t* p = out + bi.out_off + 4 + (tscan[t] - tscan[bi.tuple0]);
+    const SviRef ref = refs[svi_of(refs, n_refs, t)];
+    const uint32_t k = uint32_t(t - ref.tuple0) * 4;
+    const BlockInfo bi = blocks[ref.block];
+    const uint64_t r0 = uint64_t(ref.block) * kBlock;
+    uint8_t* p = out + bi.out_off + 4 + (tscan[t] - tscan[ref.tuple0]);
     if (k == 0) {
         uint8_t* h = out + bi.out_off;
         h[0] = uint8_t(bi.count); h[1] = uint8_t(bi.count >> 8); h[2] = uint8_t(bi.count >> 16); h[3] = uint8_t(bi.count >> 24);
@@ -249,23 +328,6 @@ __global__ void k_write_bitmap(const uint64_t* bits, uint64_t n_words, uint64_t 
         v &= keep >= 64 ? ~uint64_t(0) : ((uint64_t(1) << keep) - 1);
     }
     for (int q = 0; q < 8; ++q) p[8 + 8 * i + q] = uint8_t(v >> (8 * q));
-}
-
-__global__ void k_block_info(const uint32_t* idx, uint64_t count, BlockInfo* blocks, uint32_t nb) {
-    const uint32_t b = blockIdx.x * kT + threadIdx.x;
-    if (b >= nb) return;
-    const uint64_t r0 = uint64_t(b) * kBlock;
-    const uint32_t n = uint32_t(count - r0 < kBlock ? count - r0 : kBlock);
-    BlockInfo bi{};
-    bi.count = n;
-    bi.first = idx[r0];
-    bi.last = idx[r0 + n - 1];
-    // FrontierCompression::Encode (FrontierCompression.cpp:92-102)
-    const uint64_t bm_bytes = (uint64_t(bi.last) - bi.first + 63) / 64 * 8 + 8;
-    bi.is_bitmap = (n > 128 && bm_bytes * 8 < uint64_t(n) * 10 - 8) ? 1 : 0;
-    bi.bytes = bi.is_bitmap ? bm_bytes : 0;
-    bi.tuple0 = uint64_t(b) * (kBlock / 4);
-    blocks[b] = bi;
 }
 
 // Decode: one warp per block; StreamVInt blocks are walked by lane 0 (the
@@ -312,7 +374,243 @@ __global__ void k_decode(const uint8_t* in, const psb_codec_block* blocks, uint3
     }
 }
 
+// Device scratch of the encoder, grown on demand and kept between segments
+// (a search that spills every level's frontier encodes many segments).
+struct Scratch {
+    unsigned long long *bsum = nullptr, *tot = nullptr, *tlen = nullptr, *gsum = nullptr;
+    uint32_t* idx = nullptr;
+    BlockInfo* blocks = nullptr;
+    SviRef* refs = nullptr;
+    size_t cap_bsum = 0, cap_tot = 0, cap_tlen = 0, cap_gsum = 0, cap_idx = 0, cap_blocks = 0, cap_refs = 0;
+};
+
+template <class T>
+int grow(T** p, size_t* cap, size_t need) {
+    if (need <= *cap) return PSB_OK;
+    const size_t want = need + need / 4;
+    CD_CUDA(cudaFree(*p));
+    *p = nullptr;
+    *cap = 0;
+    CD_CUDA(cudaMalloc(reinterpret_cast<void**>(p), want));
+    *cap = want;
+    return PSB_OK;
+}
+
 }  // namespace
+
+namespace psb {
+
+struct SegmentEncoder {
+    Scratch x;
+    std::vector<BlockInfo> hb;
+    std::vector<SviRef> hrefs;
+    // The planned segment.
+    const uint64_t* bits = nullptr;
+    uint64_t n_bits = 0, n_words = 0, count = 0, tuples = 0, bytes = 0, max_words = 1;
+    uint32_t nb = 0, n_refs = 0;
+    bool any_bitmap = false;
+    uint64_t launches = 0;  // kernels launched since the last encoder_take_launches
+
+    ~SegmentEncoder() {
+        cudaFree(x.bsum); cudaFree(x.tot); cudaFree(x.tlen); cudaFree(x.gsum);
+        cudaFree(x.idx); cudaFree(x.blocks); cudaFree(x.refs);
+    }
+
+    // First half: counts the set bits (chunk prefix sums), cuts them into
+    // blocks of kBlock offsets, finds each block's first and last offset by
+    // select and picks its coding; only StreamVInt blocks get an offset list
+    // and tuple lengths.  Afterwards `count` = offsets, `nb` = blocks,
+    // `bytes` = stream size and hb[b].out_off = block b's offset.
+    int plan(const uint64_t* b, uint64_t n, cudaStream_t s) {
+        bits = b;
+        n_bits = n;
+        count = tuples = bytes = 0;
+        nb = n_refs = 0;
+        any_bitmap = false;
+        max_words = 1;
+        n_words = (n + 63) / 64;
+        if (n == 0) return PSB_OK;
+        const uint64_t nbs = (n_words + kT * 16 - 1) / (kT * 16);
+        if (int rc = grow(&x.bsum, &x.cap_bsum, (nbs + 1) * 8)) return rc;
+        if (int rc = grow(&x.tot, &x.cap_tot, 8)) return rc;
+        k_block_sums<<<unsigned(nbs), kT, 0, s>>>(bits, n_words, n_bits, x.bsum);
+        k_scan_small<<<1, kT, 0, s>>>(x.bsum, nbs, x.tot);
+        launches += 2;
+        CD_CUDA(cudaGetLastError());
+        unsigned long long c = 0;
+        CD_CUDA(cudaMemcpyAsync(&c, x.tot, 8, cudaMemcpyDeviceToHost, s));
+        CD_CUDA(cudaStreamSynchronize(s));
+        count = c;
+        if (count == 0) return PSB_OK;  // an empty segment writes nothing (CompressedSegmentWriter)
+        nb = uint32_t((count + kBlock - 1) / kBlock);
+        if (int rc = grow(&x.blocks, &x.cap_blocks, size_t(nb) * sizeof(BlockInfo))) return rc;
+        const uint64_t sel_threads = 2ull * nb * 32;
+        k_select_blocks<<<unsigned((sel_threads + kT - 1) / kT), kT, 0, s>>>(bits, n_words, n_bits, x.bsum, nbs,
+                                                                            count, x.blocks, nb);
+        k_block_decide<<<(nb + kT - 1) / kT, kT, 0, s>>>(count, x.blocks, nb);
+        launches += 2;
+        CD_CUDA(cudaGetLastError());
+        hb.resize(nb);
+        CD_CUDA(cudaMemcpyAsync(hb.data(), x.blocks, size_t(nb) * sizeof(BlockInfo), cudaMemcpyDeviceToHost, s));
+        CD_CUDA(cudaStreamSynchronize(s));
+        // StreamVInt blocks in order: 2 tuples per 8 values (count padded to a multiple of 8).
+        hrefs.clear();
+        for (uint32_t k = 0; k < nb; k++) {
+            if (hb[k].is_bitmap) {
+                any_bitmap = true;
+                max_words = std::max<uint64_t>(max_words, (uint64_t(hb[k].last) - hb[k].first + 63) / 64);
+                continue;
+            }
+            hrefs.push_back(SviRef{tuples, k, 0});
+            tuples += (uint64_t(hb[k].count) + 7) / 8 * 2;
+        }
+        n_refs = uint32_t(hrefs.size());
+        if (tuples) {
+            if (int rc = grow(&x.refs, &x.cap_refs, size_t(n_refs) * sizeof(SviRef))) return rc;
+            CD_CUDA(cudaMemcpyAsync(x.refs, hrefs.data(), size_t(n_refs) * sizeof(SviRef), cudaMemcpyHostToDevice, s));
+            if (int rc = grow(&x.idx, &x.cap_idx, count * 4)) return rc;
+            k_compact<<<unsigned(nbs), kT, 0, s>>>(bits, n_words, n_bits, x.bsum, x.blocks, x.idx);
+            if (int rc = grow(&x.tlen, &x.cap_tlen, (tuples + 1) * 8)) return rc;
+            k_tuple_len<<<unsigned((tuples + kT - 1) / kT), kT, 0, s>>>(x.idx, x.blocks, x.refs, n_refs, tuples,
+                                                                       x.tlen);
+            CD_CUDA(cudaGetLastError());
+            // Tuple offsets: exclusive scan of the tuple lengths (two levels: groups of 4096).
+            const uint64_t groups = (tuples + kT * 16 - 1) / (kT * 16);
+            if (int rc = grow(&x.gsum, &x.cap_gsum, (groups + 1) * 8)) return rc;
+            k_group_sums<<<unsigned(groups), kT, 0, s>>>(x.tlen, tuples, x.gsum);
+            k_scan_small<<<1, kT, 0, s>>>(x.gsum, groups, x.tot);
+            k_group_scan<<<unsigned(groups), kT, 0, s>>>(x.tlen, tuples, x.gsum);
+            unsigned long long svi_total = 0;
+            CD_CUDA(cudaMemcpyAsync(&svi_total, x.tot, 8, cudaMemcpyDeviceToHost, s));
+            CD_CUDA(cudaStreamSynchronize(s));
+            k_block_bytes<<<(n_refs + kT - 1) / kT, kT, 0, s>>>(x.blocks, x.refs, n_refs, x.tlen, tuples, svi_total);
+            launches += 6;
+            CD_CUDA(cudaGetLastError());
+            CD_CUDA(cudaMemcpyAsync(hb.data(), x.blocks, size_t(nb) * sizeof(BlockInfo), cudaMemcpyDeviceToHost, s));
+            CD_CUDA(cudaStreamSynchronize(s));
+        }
+        unsigned long long off = 0;
+        for (uint32_t k = 0; k < nb; k++) {
+            hb[k].out_off = off;
+            off += hb[k].bytes;
+        }
+        bytes = off;
+        return PSB_OK;
+    }
+
+    // Second half: writes the planned stream (`bytes` bytes) to d_out.
+    int write(uint8_t* d_out, cudaStream_t s) {
+        if (count == 0) return PSB_OK;
+        CD_CUDA(cudaMemcpyAsync(x.blocks, hb.data(), size_t(nb) * sizeof(BlockInfo), cudaMemcpyHostToDevice, s));
+        if (tuples) {
+            k_write_svi<<<unsigned((tuples + kT - 1) / kT), kT, 0, s>>>(x.idx, x.blocks, x.refs, n_refs, tuples, x.tlen,
+                                                                       d_out);
+            launches++;
+        }
+        if (any_bitmap) {
+            k_write_bitmap<<<dim3(unsigned((max_words + kT - 1) / kT), nb), kT, 0, s>>>(bits, n_words, n_bits,
+                                                                                        x.blocks, d_out);
+            launches++;
+        }
+        CD_CUDA(cudaGetLastError());
+        return PSB_OK;
+    }
+};
+
+// Bit t of the result = bit 2t of x (t < 32): the even bits, packed.
+__device__ __forceinline__ uint64_t even_bits(uint64_t x) {
+    x &= 0x5555555555555555ull;
+    x = (x | (x >> 1)) & 0x3333333333333333ull;
+    x = (x | (x >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x >> 4)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x >> 8)) & 0x0000FFFF0000FFFFull;
+    return (x | (x >> 16)) & 0x00000000FFFFFFFFull;
+}
+
+// Bit t of the result = bit 4t of x (t < 16).
+__device__ __forceinline__ uint64_t every_fourth_bit(uint64_t x) {
+    x &= 0x1111111111111111ull;
+    x = (x | (x >> 3)) & 0x0303030303030303ull;
+    x = (x | (x >> 6)) & 0x000F000F000F000Full;
+    x = (x | (x >> 12)) & 0x000000FF000000FFull;
+    return (x | (x >> 24)) & 0x000000000000FFFFull;
+}
+
+// Frontier bitmap of a two-bit array segment: states whose code is `code`
+// (InMemoryTwoBitBFS.cpp:6-20 layout: bit 2i = code / 2, bit 2i+1 = code % 2).
+// Out word j covers states first + 64 j .. + 63, i.e. code words 2 (first/64 + j) + {0, 1}.
+__global__ void __launch_bounds__(kT) k_frontier_two_bit(const uint64_t* __restrict__ codes, uint64_t first,
+                                                          uint64_t n_out, uint32_t code, uint64_t* __restrict__ out) {
+    const uint64_t hi_sel = (code & 2) ? 0 : ~uint64_t(0), lo_sel = (code & 1) ? 0 : ~uint64_t(0);
+    for (uint64_t j = blockIdx.x * uint64_t(kT) + threadIdx.x; j < n_out; j += uint64_t(gridDim.x) * kT) {
+        const uint64_t w = 2 * (first / 64 + j);
+        const uint64_t a = codes[w], b = codes[w + 1];
+        const uint64_t ma = (a ^ hi_sel) & ((a >> 1) ^ lo_sel);
+        const uint64_t mb = (b ^ hi_sel) & ((b >> 1) ^ lo_sel);
+        out[j] = even_bits(ma) | (even_bits(mb) << 32);
+    }
+}
+
+// Frontier bitmap of a frontier-search segment: states whose four operator
+// bits are not all zero (InMemoryFrontierSearch.cpp:57-112), less the states
+// of `excl` (the previous level's, on puzzles with odd cycles; may be NULL).
+__global__ void __launch_bounds__(kT) k_frontier_nibbles(const uint64_t* __restrict__ nib,
+                                                          const uint64_t* __restrict__ excl, uint64_t first,
+                                                          uint64_t n_out, uint64_t* __restrict__ out) {
+    for (uint64_t j = blockIdx.x * uint64_t(kT) + threadIdx.x; j < n_out; j += uint64_t(gridDim.x) * kT) {
+        const uint64_t w = 4 * (first / 64 + j);
+        uint64_t v = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint64_t x = nib[w + q];
+            v |= every_fourth_bit(x | (x >> 1) | (x >> 2) | (x >> 3)) << (16 * q);
+        }
+        if (excl) v &= ~excl[first / 64 + j];
+        out[j] = v;
+    }
+}
+
+unsigned extract_grid(uint64_t n_out) {
+    const uint64_t g = (n_out + kT - 1) / kT;
+    return unsigned(g < 148 * 8 ? (g ? g : 1) : 148 * 8);
+}
+
+int frontier_bits_two_bit(const uint64_t* codes, uint64_t first_state, uint64_t n_states, uint32_t code,
+                          uint64_t* out, cudaStream_t s) {
+    const uint64_t n_out = (n_states + 63) / 64;
+    k_frontier_two_bit<<<extract_grid(n_out), kT, 0, s>>>(codes, first_state, n_out, code, out);
+    CD_CUDA(cudaGetLastError());
+    return PSB_OK;
+}
+
+int frontier_bits_nibbles(const uint64_t* nibbles, const uint64_t* excl, uint64_t first_state, uint64_t n_states,
+                          uint64_t* out, cudaStream_t s) {
+    const uint64_t n_out = (n_states + 63) / 64;
+    k_frontier_nibbles<<<extract_grid(n_out), kT, 0, s>>>(nibbles, excl, first_state, n_out, out);
+    CD_CUDA(cudaGetLastError());
+    return PSB_OK;
+}
+
+SegmentEncoder* encoder_create() { return new (std::nothrow) SegmentEncoder(); }
+void encoder_destroy(SegmentEncoder* e) { delete e; }
+
+int encoder_plan(SegmentEncoder* e, const uint64_t* d_bits, uint64_t n_bits, cudaStream_t s, uint64_t* bytes,
+                 uint64_t* count) {
+    if (int rc = e->plan(d_bits, n_bits, s)) return rc;
+    *bytes = e->bytes;
+    *count = e->count;
+    return PSB_OK;
+}
+
+int encoder_write(SegmentEncoder* e, uint8_t* d_out, cudaStream_t s) { return e->write(d_out, s); }
+
+uint64_t encoder_take_launches(SegmentEncoder* e) {
+    const uint64_t n = e->launches;
+    e->launches = 0;
+    return n;
+}
+
+}  // namespace psb
 
 extern "C" int psb_frontier_encode(const uint64_t* d_bits, uint64_t first_bit, uint64_t n_bits, uint8_t* d_out,
                                    uint64_t out_cap, uint64_t* out_bytes, psb_codec_block* blocks,
@@ -323,70 +621,19 @@ extern "C" int psb_frontier_encode(const uint64_t* d_bits, uint64_t first_bit, u
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     *out_bytes = 0;
     *n_blocks = 0;
-    if (n_bits == 0) return PSB_OK;
-    const uint64_t* bits = d_bits + first_bit / 64;
-    const uint64_t n_words = (n_bits + 63) / 64;
-    const uint64_t nbs = (n_words + kT * 16 - 1) / (kT * 16);
-
-    unsigned long long *d_bsum = nullptr, *d_tot = nullptr, *d_tlen = nullptr;
-    uint32_t* d_idx = nullptr;
-    BlockInfo* d_blocks = nullptr;
-    struct Guard {
-        std::vector<void*> p;
-        ~Guard() { for (void* x : p) cudaFree(x); }
-    } g;
-    CD_CUDA(cudaMalloc(&d_bsum, (nbs + 1) * 8)); g.p.push_back(d_bsum);
-    CD_CUDA(cudaMalloc(&d_tot, 8)); g.p.push_back(d_tot);
-    k_block_sums<<<unsigned(nbs), kT, 0, s>>>(bits, n_words, n_bits, d_bsum);
-    k_scan_small<<<1, kT, 0, s>>>(d_bsum, nbs, d_tot);
-    CD_CUDA(cudaGetLastError());
-    unsigned long long count = 0;
-    CD_CUDA(cudaMemcpyAsync(&count, d_tot, 8, cudaMemcpyDeviceToHost, s));
-    CD_CUDA(cudaStreamSynchronize(s));
-    if (count == 0) return PSB_OK;  // an empty segment writes nothing (CompressedSegmentWriter)
-    const uint32_t nb = uint32_t((count + kBlock - 1) / kBlock);
-    CD_CUDA(cudaMalloc(&d_idx, count * 4)); g.p.push_back(d_idx);
-    k_compact<<<unsigned(nbs), kT, 0, s>>>(bits, n_words, n_bits, d_bsum, d_idx);
-    CD_CUDA(cudaMalloc(&d_blocks, size_t(nb) * sizeof(BlockInfo))); g.p.push_back(d_blocks);
-    k_block_info<<<(nb + kT - 1) / kT, kT, 0, s>>>(d_idx, count, d_blocks, nb);
-    const uint64_t tuples = uint64_t(nb) * (kBlock / 4);
-    CD_CUDA(cudaMalloc(&d_tlen, (tuples + 1) * 8)); g.p.push_back(d_tlen);
-    k_tuple_len<<<unsigned((tuples + kT - 1) / kT), kT, 0, s>>>(d_idx, d_blocks, nb, tuples, d_tlen);
-    CD_CUDA(cudaGetLastError());
-    // Tuple offsets: exclusive scan of the tuple lengths (two levels: groups of 4096).
-    const uint64_t groups = (tuples + kT * 16 - 1) / (kT * 16);
-    unsigned long long* d_gsum = nullptr;
-    CD_CUDA(cudaMalloc(&d_gsum, (groups + 1) * 8)); g.p.push_back(d_gsum);
-    k_group_sums<<<unsigned(groups), kT, 0, s>>>(d_tlen, tuples, d_gsum);
-    k_scan_small<<<1, kT, 0, s>>>(d_gsum, groups, d_tot);
-    k_group_scan<<<unsigned(groups), kT, 0, s>>>(d_tlen, tuples, d_gsum);
-    unsigned long long svi_total = 0;
-    CD_CUDA(cudaMemcpyAsync(&svi_total, d_tot, 8, cudaMemcpyDeviceToHost, s));
-    CD_CUDA(cudaStreamSynchronize(s));
-    k_block_bytes<<<(nb + kT - 1) / kT, kT, 0, s>>>(d_blocks, nb, d_tlen, tuples, svi_total);
-    CD_CUDA(cudaGetLastError());
-    std::vector<BlockInfo> hb(nb);
-    CD_CUDA(cudaMemcpyAsync(hb.data(), d_blocks, size_t(nb) * sizeof(BlockInfo), cudaMemcpyDeviceToHost, s));
-    CD_CUDA(cudaStreamSynchronize(s));
-    unsigned long long off = 0;
-    uint64_t max_words = 1;
-    for (uint32_t b = 0; b < nb; b++) {
-        hb[b].out_off = off;
-        off += hb[b].bytes;
-        if (hb[b].is_bitmap) max_words = std::max<uint64_t>(max_words, (uint64_t(hb[b].last) - hb[b].first + 63) / 64);
-    }
-    *out_bytes = off;
-    *n_blocks = nb;
+    psb::SegmentEncoder E;
+    if (int rc = E.plan(d_bits + first_bit / 64, n_bits, s)) return rc;
+    *out_bytes = E.bytes;
+    *n_blocks = E.nb;
+    if (E.count == 0) return PSB_OK;
     if (blocks) {
-        if (blocks_cap < nb) return psb_set_error(PSB_ERR_CAPACITY, "blocks table too small");
-        for (uint32_t b = 0; b < nb; b++)
-            blocks[b] = psb_codec_block{hb[b].out_off, hb[b].count, uint32_t(hb[b].bytes), hb[b].first, hb[b].is_bitmap};
+        if (blocks_cap < E.nb) return psb_set_error(PSB_ERR_CAPACITY, "blocks table too small");
+        for (uint32_t b = 0; b < E.nb; b++)
+            blocks[b] = psb_codec_block{E.hb[b].out_off, E.hb[b].count, uint32_t(E.hb[b].bytes), E.hb[b].first,
+                                        E.hb[b].is_bitmap};
     }
-    if (!d_out || out_cap < off) return psb_set_error(PSB_ERR_CAPACITY, "output needs more bytes (see *out_bytes)");
-    CD_CUDA(cudaMemcpyAsync(d_blocks, hb.data(), size_t(nb) * sizeof(BlockInfo), cudaMemcpyHostToDevice, s));
-    k_write_svi<<<unsigned((tuples + kT - 1) / kT), kT, 0, s>>>(d_idx, d_blocks, tuples, d_tlen, d_out);
-    k_write_bitmap<<<dim3(unsigned((max_words + kT - 1) / kT), nb), kT, 0, s>>>(bits, n_words, n_bits, d_blocks, d_out);
-    CD_CUDA(cudaGetLastError());
+    if (!d_out || out_cap < E.bytes) return psb_set_error(PSB_ERR_CAPACITY, "output needs more bytes (see *out_bytes)");
+    if (int rc = E.write(d_out, s)) return rc;
     CD_CUDA(cudaStreamSynchronize(s));
     return PSB_OK;
 }

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -574,6 +575,94 @@ int session_pool(int device, cudaMemPool_t* out) {
     return PSB_OK;
 }
 
+// Frontier spill resources: the segment encoder (its device scratch), one
+// segment's extracted bitmap, an arena holding one depth's encoded segments
+// back to back, a copy stream and two pinned host slots.  A depth is encoded
+// into the arena before its level runs; while the level kernel runs, the
+// calling thread moves the segments through the host slots (copy on the copy
+// stream, then the callback) in order.  They are kept per device between
+// searches (a search allocates them on first use);
+// psb_release_cached_memory frees them.
+struct SpillSeg {
+    uint32_t depth, segment;
+    uint64_t off, bytes, states;
+};
+
+struct SpillSlot {
+    uint8_t* host = nullptr;
+    uint64_t host_cap = 0;
+    cudaEvent_t start = nullptr, done = nullptr;
+};
+
+struct SpillRes {
+    int device = -1;
+    psb::SegmentEncoder* enc = nullptr;
+    uint64_t* bits = nullptr;
+    uint64_t bits_cap = 0;  // bytes
+    uint8_t* arena = nullptr;
+    uint64_t arena_cap = 0;  // bytes
+    std::vector<SpillSeg> segs;  // the depth in the arena
+    std::vector<uint8_t> flags;  // host copy of the depth's active-window flags
+    size_t issued = 0, delivered = 0;
+    SpillSlot slot[2];  // segment i goes through slot i % 2
+    cudaStream_t copy = nullptr;
+    cudaEvent_t encoded = nullptr;
+
+    ~SpillRes() {
+        if (copy) cudaStreamSynchronize(copy);
+        for (auto& sl : slot) {
+            if (sl.host) cudaFreeHost(sl.host);
+            if (sl.start) cudaEventDestroy(sl.start);
+            if (sl.done) cudaEventDestroy(sl.done);
+        }
+        cudaFree(bits);
+        cudaFree(arena);
+        if (enc) psb::encoder_destroy(enc);
+        if (encoded) cudaEventDestroy(encoded);
+        if (copy) cudaStreamDestroy(copy);
+    }
+
+    // Waits for copies in flight and drops their segments (a search that
+    // failed part-way leaves them behind).
+    void reset() {
+        if (copy) cudaStreamSynchronize(copy);
+        segs.clear();
+        issued = delivered = 0;
+    }
+};
+
+std::mutex g_spill_mu;
+std::vector<SpillRes*> g_spill_cache[kMaxPoolDevices];
+
+int spill_acquire(int device, SpillRes** out) {
+    {
+        std::lock_guard<std::mutex> lock(g_spill_mu);
+        if (device >= 0 && device < kMaxPoolDevices && !g_spill_cache[device].empty()) {
+            *out = g_spill_cache[device].back();
+            g_spill_cache[device].pop_back();
+            return PSB_OK;
+        }
+    }
+    std::unique_ptr<SpillRes> R(new (std::nothrow) SpillRes());
+    if (!R || !(R->enc = psb::encoder_create())) return fail(PSB_ERR_NOMEM, "spill resources");
+    R->device = device;
+    PSB_CUDA(cudaStreamCreateWithFlags(&R->copy, cudaStreamNonBlocking));
+    PSB_CUDA(cudaEventCreateWithFlags(&R->encoded, cudaEventDisableTiming));
+    for (auto& sl : R->slot) {
+        PSB_CUDA(cudaEventCreate(&sl.start));
+        PSB_CUDA(cudaEventCreate(&sl.done));
+    }
+    *out = R.release();
+    return PSB_OK;
+}
+
+void spill_return(SpillRes* R) {
+    R->reset();
+    std::lock_guard<std::mutex> lock(g_spill_mu);
+    if (R->device >= 0 && R->device < kMaxPoolDevices) g_spill_cache[R->device].push_back(R);
+    else delete R;
+}
+
 }  // namespace
 
 struct psb_bfs_session {
@@ -593,6 +682,7 @@ struct psb_bfs_session {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t bytes = 0;
     cudaMemPool_t pool = nullptr;
+    SpillRes* spill = nullptr;  // frontier spill resources, taken from the device's cache on first use
 
     int alloc(void** ptr, size_t size) {  // stream-ordered, from the device's session pool
         PSB_CUDA(cudaMallocFromPoolAsync(ptr, size, pool, stream));
@@ -605,6 +695,7 @@ struct psb_bfs_session {
         if (visited) cudaFreeAsync(visited, stream);
         if (d_stats) cudaFreeAsync(d_stats, stream);
         for (auto* f : wflags) if (f) cudaFreeAsync(f, stream);
+        if (spill) spill_return(spill);
         if (h_stats) cudaFreeHost(h_stats);
         for (auto& e : ev) if (e) cudaEventDestroy(e);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -674,6 +765,156 @@ int set_bit(uint64_t* d_word_base, uint64_t bit, cudaStream_t s) {
     return PSB_OK;
 }
 
+// Where one depth's frontier lives when it is spilled: a one-bit array
+// (three-bit `cur`, classic `open`), two-bit codes equal to `code`, the
+// frontier search's operator nibbles less `excl`, or the single initial state.
+struct SpillSource {
+    const uint64_t* bitmap = nullptr;
+    const uint64_t* codes = nullptr;
+    uint32_t code = 0;
+    const uint64_t* nibbles = nullptr;
+    const uint64_t* excl = nullptr;
+    uint64_t single = PSB_INVALID_INDEX;
+    // Active-window flags of this depth (one byte per 2^window_bits states,
+    // a superset of the windows holding its states), or NULL: segments with
+    // no flagged window are empty and skipped without touching the array.
+    const uint8_t* flags = nullptr;
+    int window_bits = 0;
+    uint64_t n_windows = 0;
+};
+
+struct SpillTotals {
+    double encode_ms = 0, drain_ms = 0, copy_ms = 0;
+    uint64_t bytes = 0, segments = 0, launches = 0;
+};
+
+// Grows a device buffer to at least `need` bytes (*cap is its size in bytes).
+template <class T>
+int grow_device(T** p, uint64_t* cap, uint64_t need) {
+    if (need <= *cap) return PSB_OK;
+    PSB_CUDA(cudaFree(*p));
+    *p = nullptr;
+    *cap = 0;
+    const uint64_t want = need + need / 4;
+    PSB_CUDA(cudaMalloc(reinterpret_cast<void**>(p), want));
+    *cap = want;
+    return PSB_OK;
+}
+
+// Starts the copies of arena segments to free host slots (at most two in
+// flight; segment i uses slot i % 2).
+int spill_issue(SpillRes* R) {
+    while (R->issued < R->segs.size() && R->issued < R->delivered + 2) {
+        const SpillSeg& g = R->segs[R->issued];
+        SpillSlot& sl = R->slot[R->issued & 1];
+        if (sl.host_cap < g.bytes) {  // the slot is idle: its last segment was delivered
+            if (sl.host) PSB_CUDA(cudaFreeHost(sl.host));
+            sl.host = nullptr;
+            sl.host_cap = 0;
+            const uint64_t want = g.bytes + g.bytes / 4;
+            PSB_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&sl.host), want, cudaHostAllocDefault));
+            sl.host_cap = want;
+        }
+        PSB_CUDA(cudaEventRecord(sl.start, R->copy));
+        PSB_CUDA(cudaMemcpyAsync(sl.host, R->arena + g.off, g.bytes, cudaMemcpyDeviceToHost, R->copy));
+        PSB_CUDA(cudaEventRecord(sl.done, R->copy));
+        R->issued++;
+    }
+    return PSB_OK;
+}
+
+// Hands every segment of the arena's depth to the callback, in order, as its
+// copy lands.  The search calls this right after launching a level, so the
+// copies and callbacks run while that level is on the GPU.
+int spill_drain(SpillRes* R, const psb_bfs_opts* o, SpillTotals* t) {
+    const auto t0 = std::chrono::steady_clock::now();
+    while (R->delivered < R->segs.size()) {
+        if (int rc = spill_issue(R)) return rc;
+        const SpillSeg& g = R->segs[R->delivered];
+        SpillSlot& sl = R->slot[R->delivered & 1];
+        PSB_CUDA(cudaEventSynchronize(sl.done));
+        float ms = 0;
+        PSB_CUDA(cudaEventElapsedTime(&ms, sl.start, sl.done));
+        t->copy_ms += ms;
+        R->delivered++;
+        if (o->spill(o->spill_user, g.depth, g.segment, sl.host, g.bytes, g.states))
+            return fail(PSB_ERR_ABORTED, "spill callback stopped the search at depth %u, segment %u", g.depth,
+                        g.segment);
+        t->bytes += g.bytes;
+        t->segments++;
+    }
+    t->drain_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return PSB_OK;
+}
+
+// Encodes the states at `depth` into the arena, segment by segment (the
+// segment's frontier bitmap is the array itself, or one extracted into the
+// spill scratch), and starts the first copies.  The previous depth must be
+// drained.  This takes SegmentWriter's place (Common/CompressedFrontier.cpp:
+// 103-140 writes the same stream per segment).  The arrays may change as
+// soon as this returns: the arena holds everything still to be copied.
+int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const SpillSource& src, SpillTotals* t) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const uint64_t N = S->p.n_states;
+    const uint64_t seg = uint64_t(1) << (o->segment_bits ? o->segment_bits : 32);
+    cudaStream_t s = S->stream;
+    SpillRes* R = S->spill;
+    R->segs.clear();
+    R->issued = R->delivered = 0;
+    if (src.flags) {
+        R->flags.resize(src.n_windows);
+        PSB_CUDA(cudaMemcpyAsync(R->flags.data(), src.flags, src.n_windows, cudaMemcpyDeviceToHost, s));
+        PSB_CUDA(cudaStreamSynchronize(s));
+    }
+    uint64_t off = 0;
+    for (uint64_t g = 0; g * seg < N; g++) {
+        const uint64_t first = g * seg, n = std::min(seg, N - first);
+        if (src.flags) {
+            const uint64_t w0 = first >> src.window_bits, w1 = std::min(src.n_windows, ((first + n - 1) >> src.window_bits) + 1);
+            if (std::find_if(R->flags.begin() + w0, R->flags.begin() + w1, [](uint8_t f) { return f != 0; }) ==
+                R->flags.begin() + w1)
+                continue;
+        }
+        if (!src.bitmap) {
+            if (src.single != PSB_INVALID_INDEX && (src.single < first || src.single - first >= n)) continue;
+            const uint64_t words = (n + 63) / 64;
+            if (int rc = grow_device(&R->bits, &R->bits_cap, words * 8)) return rc;
+            if (src.single != PSB_INVALID_INDEX) {
+                PSB_CUDA(cudaMemsetAsync(R->bits, 0, words * 8, s));
+                if (int rc = set_bit(R->bits, src.single - first, s)) return rc;
+            } else {
+                t->launches++;
+                const int rc = src.codes ? psb::frontier_bits_two_bit(src.codes, first, n, src.code, R->bits, s)
+                                         : psb::frontier_bits_nibbles(src.nibbles, src.excl, first, n, R->bits, s);
+                if (rc) return rc;
+            }
+        }
+        const uint64_t* bits = src.bitmap ? src.bitmap + first / 64 : R->bits;  // after the scratch exists
+        uint64_t bytes = 0, count = 0;
+        if (int rc = psb::encoder_plan(R->enc, bits, n, s, &bytes, &count)) return rc;
+        if (count == 0) continue;
+        if (R->arena_cap < off + bytes) {  // grow, keeping this depth's segments written so far
+            const uint64_t want = (off + bytes) + (off + bytes) / 4;
+            uint8_t* bigger = nullptr;
+            PSB_CUDA(cudaMalloc(reinterpret_cast<void**>(&bigger), want));
+            if (off) PSB_CUDA(cudaMemcpyAsync(bigger, R->arena, off, cudaMemcpyDeviceToDevice, s));
+            PSB_CUDA(cudaStreamSynchronize(s));
+            PSB_CUDA(cudaFree(R->arena));
+            R->arena = bigger;
+            R->arena_cap = want;
+        }
+        if (int rc = psb::encoder_write(R->enc, R->arena + off, s)) return rc;
+        R->segs.push_back(SpillSeg{depth, uint32_t(g), off, bytes, count});
+        off += bytes;
+    }
+    t->launches += psb::encoder_take_launches(R->enc);
+    PSB_CUDA(cudaEventRecord(R->encoded, s));
+    PSB_CUDA(cudaStreamWaitEvent(R->copy, R->encoded, 0));
+    if (int rc = spill_issue(R)) return rc;
+    t->encode_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return PSB_OK;
+}
+
 int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, uint64_t* counts, uint32_t cap,
                 uint32_t* n_depths, psb_bfs_stats* stats) {
     const psb_puzzle& P = S->p;
@@ -681,7 +922,16 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     if (initial >= N) return fail(PSB_ERR_ARG, "initial index %llu >= IndexesCount()", (unsigned long long)initial);
     if (!counts || !n_depths || cap == 0) return fail(PSB_ERR_ARG, "counts buffer missing");
     const uint32_t max_depth = opts ? opts->max_depth : 0;
+    const bool spill = opts && opts->spill;
+    if (spill && opts->segment_bits && (opts->segment_bits < 6 || opts->segment_bits > 32))
+        return fail(PSB_ERR_ARG, "segment_bits %d outside 6..32", opts->segment_bits);
+    SpillTotals spilled;
+    uint32_t spilled_depths = 0;
     cudaStream_t s = S->stream;
+    if (spill) {
+        if (!S->spill) if (int rc = spill_acquire(S->device, &S->spill)) return rc;
+        S->spill->reset();
+    }
     if (S->device >= 0) PSB_CUDA(cudaSetDevice(S->device));
     for (int i = 0; i < S->n_arr; i++) PSB_CUDA(cudaMemsetAsync(S->arr[i], 0, S->words[i] * 8, s));
     if (S->visited) PSB_CUDA(cudaMemsetAsync(S->visited, 0, S->words[0] * 8, s));
@@ -759,6 +1009,25 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     uint32_t iteration = 0;
     for (;;) {
         if (max_depth && res.size() >= size_t(max_depth) + 1) break;
+        if (spill) {  // the states at depth `iteration`, before its level changes the arrays
+            SpillSource src;
+            switch (S->algo) {
+            case PSB_THREE_BIT: src.bitmap = cur; break;
+            case PSB_CLASSIC: src.bitmap = open; break;
+            case PSB_TWO_BIT: src.codes = codes; src.code = cur_code; break;
+            case PSB_FRONTIER:
+                if (first) src.single = initial;
+                else { src.nibbles = fcur; src.excl = P.odd ? cex : nullptr; }
+                break;
+            }
+            if (flags_valid >= 0) {
+                src.flags = S->wflags[flags_valid];
+                src.window_bits = S->window_bits;
+                src.n_windows = S->n_windows;
+            }
+            if (int rc = spill_depth(S, opts, iteration, src, &spilled)) return rc;
+            spilled_depths = iteration + 1;
+        }
         PSB_CUDA(cudaMemsetAsync(S->d_stats, 0, 8 * sizeof(unsigned long long), s));
         // Direction of this level: bottom-up once the unvisited states are
         // fewer than ratio x the frontier (they probe until a round hits; the
@@ -845,6 +1114,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             PSB_CUDA(cudaGetLastError());
         }
         PSB_CUDA(cudaEventRecord(S->ev[3], s));
+        if (spill) if (int rc = spill_drain(S->spill, opts, &spilled)) return rc;  // overlaps this level
         PSB_CUDA(cudaMemcpyAsync(S->h_stats, S->d_stats, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         PSB_CUDA(cudaStreamSynchronize(s));
         if (S->h_stats[3]) return fail(PSB_ERR_DEVICE, "level kernel produced a child index >= IndexesCount()");
@@ -907,6 +1177,14 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         if (res.size() > cap) return fail(PSB_ERR_CAPACITY, "more than %u depths", cap);
     }
 done:
+    if (spill && spilled_depths < res.size()) {
+        // Three-bit and classic searches stopped by max_depth hold their
+        // last depth, which no level expanded, in cur / open.
+        SpillSource src;
+        src.bitmap = S->algo == PSB_THREE_BIT ? cur : open;
+        if (int rc = spill_depth(S, opts, spilled_depths, src, &spilled)) return rc;
+    }
+    if (spill) if (int rc = spill_drain(S->spill, opts, &spilled)) return rc;
     PSB_CUDA(cudaEventRecord(S->ev[3], s));
     PSB_CUDA(cudaEventSynchronize(S->ev[3]));
     float total = 0;
@@ -948,6 +1226,12 @@ done:
         stats->expand_launches = launches;
         stats->device_bytes = S->bytes;
         stats->bottom_up_levels = bu_levels;
+        stats->spill_ms = spilled.encode_ms + spilled.drain_ms;
+        stats->spill_encode_ms = spilled.encode_ms;
+        stats->spill_copy_ms = spilled.copy_ms;
+        stats->spill_bytes = spilled.bytes;
+        stats->spill_segments = spilled.segments;
+        stats->spill_launches = spilled.launches;
     }
     return PSB_OK;
 }
@@ -1034,6 +1318,12 @@ int psb_release_cached_memory(int device) {
         std::lock_guard<std::mutex> lock(g_pool_mu);
         pool = g_pools[device];
     }
+    std::vector<SpillRes*> cached;
+    {
+        std::lock_guard<std::mutex> lock(g_spill_mu);
+        cached.swap(g_spill_cache[device]);
+    }
+    for (SpillRes* R : cached) delete R;
     if (!pool) return PSB_OK;
     PSB_CUDA(cudaDeviceSynchronize());  // frees still queued on streams return first
     PSB_CUDA(cudaMemPoolTrimTo(pool, 0));

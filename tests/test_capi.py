@@ -1,6 +1,7 @@
 """CPU tests of the C ABI (include/psb200.h): the library loads, exports every
 declared function, and its host-side logic (puzzle info, Parse, ToString,
 argument checks) matches the oracle.  No kernels are launched."""
+import ctypes
 import math
 import os
 import random
@@ -131,3 +132,26 @@ def test_no_device_error_without_gpu():
     with pytest.raises(psb.PsbError) as e:
         psb.bfs(psb.PancakeSimple(5), "three_bit")
     assert e.value.code == -7
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of the ABI structs have the header's size and field
+    offsets (a C program compiled against include/psb200.h prints them)."""
+    mirrors = {"psb_bfs_opts": psb.BfsOpts, "psb_bfs_stats": psb.BfsStats, "psb_engine_opts": psb.EngineOpts,
+               "psb_server_opts": psb.ServerOpts, "psb_codec_block": psb.CodecBlock}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "psb200.h"', "int main(void) {"]
+    for cname, cls in mirrors.items():
+        lines.append(f'    printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in cls._fields_:
+            lines.append(f'    printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                               text=True).stdout.splitlines())
+    for cname, cls in mirrors.items():
+        assert int(out[cname]) == ctypes.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            assert int(out[f"{cname}.{f}"]) == getattr(cls, f).offset, (cname, f)

@@ -100,3 +100,50 @@ def test_bfs_frontier_spill_roundtrip():
     pos = np.nonzero(np.unpackbits(cur.view(np.uint8), bitorder="little"))[0].astype(np.uint32)
     assert bytes(host.numpy().tobytes()) == O.segment_stream(pos)
     assert sum(blocks[i].count for i in range(nb)) == r["counts"][-1]
+
+
+def mixed_bits(n_bits, pieces, seed):
+    """A bitmap whose density changes along it: pieces = [(fraction, density)]."""
+    rng = np.random.default_rng(seed)
+    bits = np.zeros(n_bits, dtype=bool)
+    at = 0
+    for frac, dens in pieces:
+        n = int(n_bits * frac)
+        bits[at:at + n] = rng.random(n) < dens
+        at += n
+    words = np.zeros((n_bits + 63) // 64, dtype=np.uint64)
+    pos = np.nonzero(bits)[0].astype(np.uint64)
+    np.bitwise_or.at(words, (pos >> 6).astype(np.int64), np.left_shift(np.uint64(1), pos & np.uint64(63)))
+    return words, pos.astype(np.uint32)
+
+
+MIXED = [
+    (1 << 24, [(0.3, 0.5), (0.4, 0.004), (0.3, 0.9)]),
+    (1 << 24, [(0.5, 0.001), (0.1, 0.6), (0.4, 0.03)]),
+    (12_000_001, [(0.2, 0.0), (0.2, 0.15), (0.4, 0.06), (0.2, 1.0)]),
+    (1 << 23, [(0.05, 1.0), (0.95, 0.0002)]),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(MIXED)))
+def test_encode_mixed_density_segments(case):
+    """Segments whose blocks are partly bitmap and partly StreamVInt coded,
+    with block boundaries where the density changes."""
+    torch = pytest.importorskip("torch")
+    n_bits, pieces = MIXED[case]
+    words, offsets = mixed_bits(n_bits, pieces, 100 + case)
+    expected = O.segment_stream(offsets)
+    d_bits = torch.from_numpy(words.view(np.int64)).cuda()
+    size, _, _ = psb.frontier_encode(d_bits.data_ptr(), 0, n_bits)
+    assert size == len(expected)
+    d_out = torch.zeros(size, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    _, blocks, nb = psb.frontier_encode(d_bits.data_ptr(), 0, n_bits, d_out.data_ptr(), size)
+    assert bytes(d_out.cpu().numpy().tobytes()) == expected
+    kinds = {bool(blocks[i].is_bitmap) for i in range(nb)}
+    assert len(kinds) == 2
+    d_back = torch.zeros_like(d_bits)
+    torch.cuda.synchronize()
+    psb.frontier_decode(d_out.data_ptr(), blocks, nb, d_back.data_ptr(), 0, n_bits)
+    assert torch.equal(d_back.cpu(), d_bits.cpu())

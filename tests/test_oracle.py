@@ -120,6 +120,22 @@ def test_reference_runs(golden):
         assert counts == run["counts"], (spec, run["algo"], run["start"])
 
 
+def test_depths_match_reference_runs(golden):
+    """orc_depths (the per-state distances a spilled frontier is checked
+    against) gives the reference's own per-depth counts."""
+    import numpy as np
+    ran = 0
+    for run in golden["ref_runs"]:
+        spec = run["puzzle"]
+        if O.info(spec)["indexes"] > 4_000_000 or run["algo"] != "two_bit":
+            continue
+        d, k = O.depths(spec, O.parse(spec, run["start"]))
+        hist = np.bincount(d[d != 255], minlength=k)
+        assert hist.tolist() == run["counts"], (spec, run["start"])
+        ran += 1
+    assert ran >= 10
+
+
 def test_sum_invariants():
     """Every pancake and Hanoi state is reachable; half of the sliding states are."""
     assert sum(O.bfs(["pancake", 8, 0], "three_bit")[0]) == math.factorial(8)
