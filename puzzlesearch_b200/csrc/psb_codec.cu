@@ -66,25 +66,49 @@ __global__ void k_block_sums(const uint64_t* bits, uint64_t n_words, uint64_t n_
     }
 }
 
-// Exclusive scan of n u64 values in place by one block (n is small: block sums, tuple groups).
-__global__ void k_scan_small(unsigned long long* v, uint64_t n, unsigned long long* total) {
-    __shared__ unsigned long long s[kT];
+// Exclusive scan of n u64 values in place by one CTA of kScanT threads
+// (chunk sums, tuple-group sums: at most a few hundred thousand values), in
+// tiles of kScanT * 16 values: thread t sums values 16 t .. 16 t + 15 of a
+// tile, warp shuffles and one pass over the warp totals rank them.
+constexpr int kScanT = 1024;
+__global__ void __launch_bounds__(kScanT) k_scan_small(unsigned long long* v, uint64_t n, unsigned long long* total) {
+    __shared__ unsigned long long warp_tot[kScanT / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long carry = 0;
-    for (uint64_t base = 0; base < n; base += kT) {
-        const uint64_t i = base + threadIdx.x;
-        const unsigned long long x = i < n ? v[i] : 0;
-        s[threadIdx.x] = x;
-        __syncthreads();
-        for (int o = 1; o < kT; o <<= 1) {
-            const unsigned long long y = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
-            __syncthreads();
-            s[threadIdx.x] += y;
-            __syncthreads();
+    for (uint64_t base = 0; base < n; base += uint64_t(kScanT) * 16) {
+        const uint64_t i0 = base + uint64_t(threadIdx.x) * 16;
+        unsigned long long x[16], c = 0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            x[k] = i0 + k < n ? v[i0 + k] : 0;
+            c += x[k];
         }
-        if (i < n) v[i] = carry + s[threadIdx.x] - x;
-        const unsigned long long blk = s[kT - 1];
+        unsigned long long inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) warp_tot[warp] = inc;
         __syncthreads();
-        carry += blk;
+        if (warp == 0) {
+            unsigned long long t = warp_tot[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t;  // inclusive over warps
+        }
+        __syncthreads();
+        unsigned long long run = carry + (warp ? warp_tot[warp - 1] : 0) + inc - c;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            if (i0 + k < n) v[i0 + k] = run;
+            run += x[k];
+        }
+        carry += warp_tot[kScanT / 32 - 1];
+        __syncthreads();
     }
     if (threadIdx.x == 0) *total = carry;
 }
@@ -125,6 +149,35 @@ __global__ void k_group_scan(unsigned long long* v, uint64_t n, const unsigned l
     }
 }
 
+// Inclusive block-wide sum scan of one value per thread (kT threads).
+__device__ __forceinline__ uint32_t block_inclusive_scan(uint32_t v, uint32_t* warp_tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= o) v += y;
+    }
+    if (lane == 31) warp_tot[warp] = v;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += warp_tot[w];
+    __syncthreads();
+    return before + v;
+}
+
+// Sum of one value per thread over the CTA, written by thread 0.
+__device__ __forceinline__ void chunk_total(uint32_t c, unsigned long long* out) {
+    __shared__ uint32_t warp_tot[kT / 32];
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0) warp_tot[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < kT / 32; ++i) t += warp_tot[i];
+        *out = t;
+    }
+}
+
 __device__ __forceinline__ uint32_t vbytes(uint32_t x) { return x >> 24 ? 4 : x >> 16 ? 3 : x >> 8 ? 2 : 1; }
 
 struct BlockInfo {
@@ -141,54 +194,48 @@ struct SviRef {
 
 // Writes the ascending offsets of the set bits that fall in StreamVInt
 // blocks, at their rank (offset list position = rank; bitmap blocks need no
-// list: their words are copied from the bitmap).
-__global__ void k_compact(const uint64_t* bits, uint64_t n_words, uint64_t n_bits, const unsigned long long* bsum,
-                          const BlockInfo* blocks, uint32_t* idx) {
-    // Recompute the per-word exclusive rank inside the block (16 words per thread, interleaved).
-    __shared__ uint32_t s[kT];
-    const uint64_t base = uint64_t(blockIdx.x) * kT * 16;
-    unsigned long long run = bsum[blockIdx.x];
+// list: their words are copied from the bitmap).  One CTA per chunk of
+// kT * 16 words; thread t takes the chunk's words 16 t .. 16 t + 15, so one
+// block scan of the per-thread counts ranks them all.
+__global__ void __launch_bounds__(kT) k_compact(const uint64_t* bits, uint64_t n_words, uint64_t n_bits,
+                                                const unsigned long long* bsum, const BlockInfo* blocks,
+                                                uint32_t* idx) {
+    __shared__ uint32_t warp_tot[kT / 32];
+    const uint64_t w0 = uint64_t(blockIdx.x) * kT * 16 + uint64_t(threadIdx.x) * 16;
+    uint64_t v[16];
+    uint32_t c = 0;
+#pragma unroll
     for (int k = 0; k < 16; ++k) {
-        const uint64_t w = base + uint64_t(k) * kT + threadIdx.x;
-        const uint64_t word = w < n_words ? masked_word(bits, w, n_words, n_bits) : 0;
-        const uint32_t c = __popcll(word);
-        s[threadIdx.x] = c;
-        __syncthreads();
-        for (int o = 1; o < kT; o <<= 1) {
-            const uint32_t y = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
-            __syncthreads();
-            s[threadIdx.x] += y;
-            __syncthreads();
+        v[k] = w0 + k < n_words ? masked_word(bits, w0 + k, n_words, n_bits) : 0;
+        c += __popcll(v[k]);
+    }
+    const uint32_t inc = block_inclusive_scan(c, warp_tot);
+    if (c == 0) return;
+    unsigned long long r = bsum[blockIdx.x] + inc - c;
+    // c <= 1024 < kBlock: the thread's offsets lie in at most two blocks
+    if (blocks[r / kBlock].is_bitmap && blocks[(r + c - 1) / kBlock].is_bitmap) return;
+    for (int k = 0; k < 16; ++k) {
+        uint64_t m = v[k];
+        while (m) {
+            const uint32_t j = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            if (!blocks[r / kBlock].is_bitmap) idx[r] = uint32_t((w0 + k) * 64 + j);
+            r++;
         }
-        unsigned long long r = run + s[threadIdx.x] - c;
-        // c <= 64 < kBlock: the word's offsets lie in at most two blocks
-        if (c && !(blocks[r / kBlock].is_bitmap && blocks[(r + c - 1) / kBlock].is_bitmap)) {
-            uint64_t m = word;
-            while (m) {
-                const uint32_t j = __ffsll((long long)m) - 1;
-                m &= m - 1;
-                if (!blocks[r / kBlock].is_bitmap) idx[r] = uint32_t(w * 64 + j);
-                r++;
-            }
-        }
-        const uint32_t tot = s[kT - 1];
-        __syncthreads();
-        run += tot;
     }
 }
 
 // First and last offset of every block (ranks b * kBlock and the block's
 // last rank), by select: the chunk holding the rank from the chunk prefix
-// sums (bsum, chunks of kT * 16 words), then a warp scan of that chunk's
-// words.  One warp per (block, end); warps 2b and 2b + 1 serve block b.
-__global__ void k_select_blocks(const uint64_t* bits, uint64_t n_words, uint64_t n_bits,
-                                const unsigned long long* bsum, uint64_t nbs, uint64_t count, BlockInfo* blocks,
-                                uint32_t nb) {
-    const uint64_t gw = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) / 32;  // uniform in a warp
-    const int lane = threadIdx.x & 31;
-    if (gw >= 2ull * nb) return;
-    const uint32_t b = uint32_t(gw / 2);
-    const bool last = gw & 1;
+// sums (bsum, chunks of kT * 16 words), then a block scan of that chunk's
+// per-thread counts (thread t: words 16 t .. 16 t + 15).  CTAs 2b and 2b + 1
+// serve block b.
+__global__ void __launch_bounds__(kT) k_select_blocks(const uint64_t* bits, uint64_t n_words, uint64_t n_bits,
+                                                      const unsigned long long* bsum, uint64_t nbs, uint64_t count,
+                                                      BlockInfo* blocks, uint32_t nb) {
+    __shared__ uint32_t warp_tot[kT / 32];
+    const uint32_t b = blockIdx.x / 2;
+    const bool last = blockIdx.x & 1;
     const uint64_t end = (uint64_t(b) + 1) * kBlock < count ? (uint64_t(b) + 1) * kBlock : count;
     const uint64_t r = last ? end - 1 : uint64_t(b) * kBlock;
     uint64_t lo = 0, hi = nbs;  // largest chunk lo with bsum[lo] <= r (bsum[0] = 0)
@@ -196,30 +243,29 @@ __global__ void k_select_blocks(const uint64_t* bits, uint64_t n_words, uint64_t
         const uint64_t mid = (lo + hi) / 2;
         if (bsum[mid] <= r) lo = mid; else hi = mid;
     }
-    uint64_t rem = r - bsum[lo];
-    const uint64_t w_end = (lo + 1) * kT * 16 < n_words ? (lo + 1) * kT * 16 : n_words;
-    for (uint64_t w0 = lo * kT * 16; w0 < w_end; w0 += 32) {
-        const uint64_t w = w0 + lane;
-        const uint64_t v = w < w_end ? masked_word(bits, w, n_words, n_bits) : 0;
-        const uint32_t c = __popcll(v);
-        uint32_t inc = c;
+    const uint64_t rem = r - bsum[lo];
+    const uint64_t w0 = lo * kT * 16 + uint64_t(threadIdx.x) * 16;
+    uint64_t v[16];
+    uint32_t c = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
-        if (rem < total) {
-            const uint32_t exc = inc - c;
-            if (rem >= exc && rem < inc) {  // exactly one lane
-                uint64_t x = v;
-                for (uint64_t i = exc; i < rem; ++i) x &= x - 1;
-                const uint32_t pos = uint32_t(w * 64 + (__ffsll((long long)x) - 1));
-                if (last) blocks[b].last = pos; else blocks[b].first = pos;
-            }
+    for (int k = 0; k < 16; ++k) {
+        v[k] = w0 + k < n_words ? masked_word(bits, w0 + k, n_words, n_bits) : 0;
+        c += __popcll(v[k]);
+    }
+    const uint32_t inc = block_inclusive_scan(c, warp_tot);
+    const uint32_t exc = inc - c;
+    if (rem < exc || rem >= inc) return;  // exactly one thread holds the rank
+    uint64_t left = rem - exc;
+    for (int k = 0; k < 16; ++k) {
+        const uint32_t ck = __popcll(v[k]);
+        if (left < ck) {
+            uint64_t x = v[k];
+            for (uint64_t i = 0; i < left; ++i) x &= x - 1;
+            const uint32_t pos = uint32_t((w0 + k) * 64 + (__ffsll((long long)x) - 1));
+            if (last) blocks[b].last = pos; else blocks[b].first = pos;
             return;
         }
-        rem -= total;
+        left -= ck;
     }
 }
 
@@ -421,7 +467,16 @@ struct SegmentEncoder {
     // select and picks its coding; only StreamVInt blocks get an offset list
     // and tuple lengths.  Afterwards `count` = offsets, `nb` = blocks,
     // `bytes` = stream size and hb[b].out_off = block b's offset.
-    int plan(const uint64_t* b, uint64_t n, cudaStream_t s) {
+    // Device buffer for the chunk sums of an n-bit segment (one per kT * 16
+    // words), for a producer that computes them itself (plan(.., true)).
+    int chunk_sums(uint64_t n, unsigned long long** out) {
+        const uint64_t nbs = ((n + 63) / 64 + kT * 16 - 1) / (kT * 16);
+        if (int rc = grow(&x.bsum, &x.cap_bsum, (nbs + 1) * 8)) return rc;
+        *out = x.bsum;
+        return PSB_OK;
+    }
+
+    int plan(const uint64_t* b, uint64_t n, cudaStream_t s, bool sums_ready) {
         bits = b;
         n_bits = n;
         count = tuples = bytes = 0;
@@ -433,9 +488,12 @@ struct SegmentEncoder {
         const uint64_t nbs = (n_words + kT * 16 - 1) / (kT * 16);
         if (int rc = grow(&x.bsum, &x.cap_bsum, (nbs + 1) * 8)) return rc;
         if (int rc = grow(&x.tot, &x.cap_tot, 8)) return rc;
-        k_block_sums<<<unsigned(nbs), kT, 0, s>>>(bits, n_words, n_bits, x.bsum);
-        k_scan_small<<<1, kT, 0, s>>>(x.bsum, nbs, x.tot);
-        launches += 2;
+        if (!sums_ready) {
+            k_block_sums<<<unsigned(nbs), kT, 0, s>>>(bits, n_words, n_bits, x.bsum);
+            launches++;
+        }
+        k_scan_small<<<1, kScanT, 0, s>>>(x.bsum, nbs, x.tot);
+        launches++;
         CD_CUDA(cudaGetLastError());
         unsigned long long c = 0;
         CD_CUDA(cudaMemcpyAsync(&c, x.tot, 8, cudaMemcpyDeviceToHost, s));
@@ -444,9 +502,7 @@ struct SegmentEncoder {
         if (count == 0) return PSB_OK;  // an empty segment writes nothing (CompressedSegmentWriter)
         nb = uint32_t((count + kBlock - 1) / kBlock);
         if (int rc = grow(&x.blocks, &x.cap_blocks, size_t(nb) * sizeof(BlockInfo))) return rc;
-        const uint64_t sel_threads = 2ull * nb * 32;
-        k_select_blocks<<<unsigned((sel_threads + kT - 1) / kT), kT, 0, s>>>(bits, n_words, n_bits, x.bsum, nbs,
-                                                                            count, x.blocks, nb);
+        k_select_blocks<<<2 * nb, kT, 0, s>>>(bits, n_words, n_bits, x.bsum, nbs, count, x.blocks, nb);
         k_block_decide<<<(nb + kT - 1) / kT, kT, 0, s>>>(count, x.blocks, nb);
         launches += 2;
         CD_CUDA(cudaGetLastError());
@@ -478,7 +534,7 @@ struct SegmentEncoder {
             const uint64_t groups = (tuples + kT * 16 - 1) / (kT * 16);
             if (int rc = grow(&x.gsum, &x.cap_gsum, (groups + 1) * 8)) return rc;
             k_group_sums<<<unsigned(groups), kT, 0, s>>>(x.tlen, tuples, x.gsum);
-            k_scan_small<<<1, kT, 0, s>>>(x.gsum, groups, x.tot);
+            k_scan_small<<<1, kScanT, 0, s>>>(x.gsum, groups, x.tot);
             k_group_scan<<<unsigned(groups), kT, 0, s>>>(x.tlen, tuples, x.gsum);
             unsigned long long svi_total = 0;
             CD_CUDA(cudaMemcpyAsync(&svi_total, x.tot, 8, cudaMemcpyDeviceToHost, s));
@@ -538,55 +594,74 @@ __device__ __forceinline__ uint64_t every_fourth_bit(uint64_t x) {
 
 // Frontier bitmap of a two-bit array segment: states whose code is `code`
 // (InMemoryTwoBitBFS.cpp:6-20 layout: bit 2i = code / 2, bit 2i+1 = code % 2).
-// Out word j covers states first + 64 j .. + 63, i.e. code words 2 (first/64 + j) + {0, 1}.
+// Out word j covers states first + 64 j .. + 63, i.e. code words
+// 2 (first/64 + j) + {0, 1}.  One CTA per chunk of kT * 16 out words, whose
+// popcount goes to sums[chunk] (the encoder's chunk sums); codes past the
+// last state are 0 and never match.
 __global__ void __launch_bounds__(kT) k_frontier_two_bit(const uint64_t* __restrict__ codes, uint64_t first,
-                                                          uint64_t n_out, uint32_t code, uint64_t* __restrict__ out) {
+                                                          uint64_t n_out, uint32_t code, uint64_t* __restrict__ out,
+                                                          unsigned long long* __restrict__ sums) {
     const uint64_t hi_sel = (code & 2) ? 0 : ~uint64_t(0), lo_sel = (code & 1) ? 0 : ~uint64_t(0);
-    for (uint64_t j = blockIdx.x * uint64_t(kT) + threadIdx.x; j < n_out; j += uint64_t(gridDim.x) * kT) {
-        const uint64_t w = 2 * (first / 64 + j);
-        const uint64_t a = codes[w], b = codes[w + 1];
-        const uint64_t ma = (a ^ hi_sel) & ((a >> 1) ^ lo_sel);
-        const uint64_t mb = (b ^ hi_sel) & ((b >> 1) ^ lo_sel);
-        out[j] = even_bits(ma) | (even_bits(mb) << 32);
+    const uint64_t base = uint64_t(blockIdx.x) * kT * 16;
+    uint32_t c = 0;
+#pragma unroll 4
+    for (int k = 0; k < 16; ++k) {
+        const uint64_t j = base + uint64_t(k) * kT + threadIdx.x;
+        if (j < n_out) {
+            const uint64_t w = 2 * (first / 64 + j);
+            const uint64_t a = codes[w], b = codes[w + 1];
+            const uint64_t ma = (a ^ hi_sel) & ((a >> 1) ^ lo_sel);
+            const uint64_t mb = (b ^ hi_sel) & ((b >> 1) ^ lo_sel);
+            const uint64_t v = even_bits(ma) | (even_bits(mb) << 32);
+            out[j] = v;
+            c += __popcll(v);
+        }
     }
+    chunk_total(c, sums + blockIdx.x);
 }
 
 // Frontier bitmap of a frontier-search segment: states whose four operator
 // bits are not all zero (InMemoryFrontierSearch.cpp:57-112), less the states
 // of `excl` (the previous level's, on puzzles with odd cycles; may be NULL).
+// Same CTA layout and chunk sums as k_frontier_two_bit.
 __global__ void __launch_bounds__(kT) k_frontier_nibbles(const uint64_t* __restrict__ nib,
                                                           const uint64_t* __restrict__ excl, uint64_t first,
-                                                          uint64_t n_out, uint64_t* __restrict__ out) {
-    for (uint64_t j = blockIdx.x * uint64_t(kT) + threadIdx.x; j < n_out; j += uint64_t(gridDim.x) * kT) {
-        const uint64_t w = 4 * (first / 64 + j);
-        uint64_t v = 0;
+                                                          uint64_t n_out, uint64_t* __restrict__ out,
+                                                          unsigned long long* __restrict__ sums) {
+    const uint64_t base = uint64_t(blockIdx.x) * kT * 16;
+    uint32_t c = 0;
+    for (int k = 0; k < 16; ++k) {
+        const uint64_t j = base + uint64_t(k) * kT + threadIdx.x;
+        if (j < n_out) {
+            const uint64_t w = 4 * (first / 64 + j);
+            uint64_t v = 0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const uint64_t x = nib[w + q];
-            v |= every_fourth_bit(x | (x >> 1) | (x >> 2) | (x >> 3)) << (16 * q);
+            for (int q = 0; q < 4; ++q) {
+                const uint64_t x = nib[w + q];
+                v |= every_fourth_bit(x | (x >> 1) | (x >> 2) | (x >> 3)) << (16 * q);
+            }
+            if (excl) v &= ~excl[first / 64 + j];
+            out[j] = v;
+            c += __popcll(v);
         }
-        if (excl) v &= ~excl[first / 64 + j];
-        out[j] = v;
     }
+    chunk_total(c, sums + blockIdx.x);
 }
 
-unsigned extract_grid(uint64_t n_out) {
-    const uint64_t g = (n_out + kT - 1) / kT;
-    return unsigned(g < 148 * 8 ? (g ? g : 1) : 148 * 8);
-}
+unsigned chunks_of(uint64_t n_out) { return unsigned((n_out + kT * 16 - 1) / (kT * 16)); }
 
 int frontier_bits_two_bit(const uint64_t* codes, uint64_t first_state, uint64_t n_states, uint32_t code,
-                          uint64_t* out, cudaStream_t s) {
+                          uint64_t* out, unsigned long long* sums, cudaStream_t s) {
     const uint64_t n_out = (n_states + 63) / 64;
-    k_frontier_two_bit<<<extract_grid(n_out), kT, 0, s>>>(codes, first_state, n_out, code, out);
+    k_frontier_two_bit<<<chunks_of(n_out), kT, 0, s>>>(codes, first_state, n_out, code, out, sums);
     CD_CUDA(cudaGetLastError());
     return PSB_OK;
 }
 
 int frontier_bits_nibbles(const uint64_t* nibbles, const uint64_t* excl, uint64_t first_state, uint64_t n_states,
-                          uint64_t* out, cudaStream_t s) {
+                          uint64_t* out, unsigned long long* sums, cudaStream_t s) {
     const uint64_t n_out = (n_states + 63) / 64;
-    k_frontier_nibbles<<<extract_grid(n_out), kT, 0, s>>>(nibbles, excl, first_state, n_out, out);
+    k_frontier_nibbles<<<chunks_of(n_out), kT, 0, s>>>(nibbles, excl, first_state, n_out, out, sums);
     CD_CUDA(cudaGetLastError());
     return PSB_OK;
 }
@@ -594,9 +669,13 @@ int frontier_bits_nibbles(const uint64_t* nibbles, const uint64_t* excl, uint64_
 SegmentEncoder* encoder_create() { return new (std::nothrow) SegmentEncoder(); }
 void encoder_destroy(SegmentEncoder* e) { delete e; }
 
-int encoder_plan(SegmentEncoder* e, const uint64_t* d_bits, uint64_t n_bits, cudaStream_t s, uint64_t* bytes,
-                 uint64_t* count) {
-    if (int rc = e->plan(d_bits, n_bits, s)) return rc;
+int encoder_chunk_sums(SegmentEncoder* e, uint64_t n_bits, unsigned long long** sums) {
+    return e->chunk_sums(n_bits, sums);
+}
+
+int encoder_plan(SegmentEncoder* e, const uint64_t* d_bits, uint64_t n_bits, cudaStream_t s, bool sums_ready,
+                 uint64_t* bytes, uint64_t* count) {
+    if (int rc = e->plan(d_bits, n_bits, s, sums_ready)) return rc;
     *bytes = e->bytes;
     *count = e->count;
     return PSB_OK;
@@ -622,7 +701,7 @@ extern "C" int psb_frontier_encode(const uint64_t* d_bits, uint64_t first_bit, u
     *out_bytes = 0;
     *n_blocks = 0;
     psb::SegmentEncoder E;
-    if (int rc = E.plan(d_bits + first_bit / 64, n_bits, s)) return rc;
+    if (int rc = E.plan(d_bits + first_bit / 64, n_bits, s, false)) return rc;
     *out_bytes = E.bytes;
     *n_blocks = E.nb;
     if (E.count == 0) return PSB_OK;

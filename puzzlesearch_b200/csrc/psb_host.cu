@@ -875,6 +875,7 @@ int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const
                 R->flags.begin() + w1)
                 continue;
         }
+        bool sums_ready = false;  // the extraction kernels also count
         if (!src.bitmap) {
             if (src.single != PSB_INVALID_INDEX && (src.single < first || src.single - first >= n)) continue;
             const uint64_t words = (n + 63) / 64;
@@ -883,15 +884,19 @@ int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const
                 PSB_CUDA(cudaMemsetAsync(R->bits, 0, words * 8, s));
                 if (int rc = set_bit(R->bits, src.single - first, s)) return rc;
             } else {
+                unsigned long long* sums = nullptr;
+                if (int rc = psb::encoder_chunk_sums(R->enc, n, &sums)) return rc;
                 t->launches++;
-                const int rc = src.codes ? psb::frontier_bits_two_bit(src.codes, first, n, src.code, R->bits, s)
-                                         : psb::frontier_bits_nibbles(src.nibbles, src.excl, first, n, R->bits, s);
+                const int rc =
+                    src.codes ? psb::frontier_bits_two_bit(src.codes, first, n, src.code, R->bits, sums, s)
+                              : psb::frontier_bits_nibbles(src.nibbles, src.excl, first, n, R->bits, sums, s);
                 if (rc) return rc;
+                sums_ready = true;
             }
         }
         const uint64_t* bits = src.bitmap ? src.bitmap + first / 64 : R->bits;  // after the scratch exists
         uint64_t bytes = 0, count = 0;
-        if (int rc = psb::encoder_plan(R->enc, bits, n, s, &bytes, &count)) return rc;
+        if (int rc = psb::encoder_plan(R->enc, bits, n, s, sums_ready, &bytes, &count)) return rc;
         if (count == 0) continue;
         if (R->arena_cap < off + bytes) {  // grow, keeping this depth's segments written so far
             const uint64_t want = (off + bytes) + (off + bytes) / 4;

@@ -48,17 +48,21 @@ void encoder_destroy(SegmentEncoder* e);
 // Plans the reference's segment stream of the set bits of d_bits[0, n_bits)
 // (n_bits <= 2^32): *count offsets in *bytes bytes; encoder_write then
 // writes it to d_out (device, >= *bytes).  d_bits must stay unchanged
-// until the write has run (both are ordered on stream s).
-int encoder_plan(SegmentEncoder* e, const uint64_t* d_bits, uint64_t n_bits, cudaStream_t s, uint64_t* bytes,
-                 uint64_t* count);
+// until the write has run (both are ordered on stream s).  sums_ready: the
+// chunk popcounts are already in encoder_chunk_sums' buffer.
+int encoder_plan(SegmentEncoder* e, const uint64_t* d_bits, uint64_t n_bits, cudaStream_t s, bool sums_ready,
+                 uint64_t* bytes, uint64_t* count);
 int encoder_write(SegmentEncoder* e, uint8_t* d_out, cudaStream_t s);
+// The encoder's chunk-sum buffer sized for an n_bits segment.
+int encoder_chunk_sums(SegmentEncoder* e, uint64_t n_bits, unsigned long long** sums);
 // Kernels the encoder launched since the last call.
 uint64_t encoder_take_launches(SegmentEncoder* e);
 // One-bit frontier bitmaps (ceil(n_states/64) words at out; first_state a
 // multiple of 64) of a two-bit array (states with code `code`) and of a
-// frontier-search array (states with an operator bit set, less `excl`).
+// frontier-search array (states with an operator bit set, less `excl`),
+// with their chunk popcounts in `sums` (from encoder_chunk_sums).
 int frontier_bits_two_bit(const uint64_t* codes, uint64_t first_state, uint64_t n_states, uint32_t code,
-                          uint64_t* out, cudaStream_t s);
+                          uint64_t* out, unsigned long long* sums, cudaStream_t s);
 int frontier_bits_nibbles(const uint64_t* nibbles, const uint64_t* excl, uint64_t first_state, uint64_t n_states,
-                          uint64_t* out, cudaStream_t s);
+                          uint64_t* out, unsigned long long* sums, cudaStream_t s);
 }  // namespace psb
