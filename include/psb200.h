@@ -126,7 +126,8 @@ typedef struct {
     float bottom_up_ratio; /* PSB_DIR_AUTO: a dense level runs bottom-up when unvisited < ratio * frontier (0 = 1.0) */
     psb_spill_fn spill;    /* optional: every depth's frontier, encoded on the GPU segment by segment (below) */
     void* spill_user;      /* first argument of spill */
-    int32_t segment_bits;  /* states per spilled segment = 2^segment_bits, 6..32 (0 = 32, the reference's largest) */
+    int32_t segment_bits;  /* states per spilled segment = 2^segment_bits, 6..32 (0 = 32, the default of
+                              PuzzleOptions::segmentBits, Common/DiskBasedBFS.h:11) */
 } psb_bfs_opts;
 
 /* With opts->spill set, the states at each depth d = 0, 1, ... (every depth

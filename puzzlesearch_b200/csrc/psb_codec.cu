@@ -198,9 +198,17 @@ struct SviRef {
 // kT * 16 words; thread t takes the chunk's words 16 t .. 16 t + 15, so one
 // block scan of the per-thread counts ranks them all.
 __global__ void __launch_bounds__(kT) k_compact(const uint64_t* bits, uint64_t n_words, uint64_t n_bits,
-                                                const unsigned long long* bsum, const BlockInfo* blocks,
-                                                uint32_t* idx) {
+                                                const unsigned long long* bsum, uint64_t nbs, uint64_t count,
+                                                const BlockInfo* blocks, uint32_t* idx) {
     __shared__ uint32_t warp_tot[kT / 32];
+    // Chunks with no offsets, or whose offsets all fall in bitmap blocks,
+    // have nothing to list (uniform over the CTA: the chunk's rank range).
+    const unsigned long long r_lo = bsum[blockIdx.x];
+    const unsigned long long r_hi = blockIdx.x + 1 < nbs ? bsum[blockIdx.x + 1] : count;
+    if (r_hi == r_lo) return;
+    bool all_bitmap = true;
+    for (uint64_t b = r_lo / kBlock; b <= (r_hi - 1) / kBlock; ++b) all_bitmap = all_bitmap && blocks[b].is_bitmap;
+    if (all_bitmap) return;
     const uint64_t w0 = uint64_t(blockIdx.x) * kT * 16 + uint64_t(threadIdx.x) * 16;
     uint64_t v[16];
     uint32_t c = 0;
@@ -525,7 +533,7 @@ struct SegmentEncoder {
             if (int rc = grow(&x.refs, &x.cap_refs, size_t(n_refs) * sizeof(SviRef))) return rc;
             CD_CUDA(cudaMemcpyAsync(x.refs, hrefs.data(), size_t(n_refs) * sizeof(SviRef), cudaMemcpyHostToDevice, s));
             if (int rc = grow(&x.idx, &x.cap_idx, count * 4)) return rc;
-            k_compact<<<unsigned(nbs), kT, 0, s>>>(bits, n_words, n_bits, x.bsum, x.blocks, x.idx);
+            k_compact<<<unsigned(nbs), kT, 0, s>>>(bits, n_words, n_bits, x.bsum, nbs, count, x.blocks, x.idx);
             if (int rc = grow(&x.tlen, &x.cap_tlen, (tuples + 1) * 8)) return rc;
             k_tuple_len<<<unsigned((tuples + kT - 1) / kT), kT, 0, s>>>(x.idx, x.blocks, x.refs, n_refs, tuples,
                                                                        x.tlen);
