@@ -359,8 +359,21 @@ __global__ void k_write_svi(const uint32_t* idx, const BlockInfo* blocks, const 
 }
 
 // Bitmap block: bit j of output word i is state first + 1 + 64 i + j (<= last).
+// A chunk (kT * 16 words) with no set bits; its words may be stale scratch
+// (an extraction skips chunks of windows that hold no frontier state).
+__device__ __forceinline__ bool chunk_empty(const unsigned long long* bsum, uint64_t nbs, uint64_t count,
+                                            uint64_t w) {
+    const uint64_t k = w / (kT * 16);
+    return (k + 1 < nbs ? bsum[k + 1] : count) == bsum[k];
+}
+
+__device__ __forceinline__ uint64_t live_word(const uint64_t* bits, uint64_t w, uint64_t n_words, uint64_t n_bits,
+                                              const unsigned long long* bsum, uint64_t nbs, uint64_t count) {
+    return chunk_empty(bsum, nbs, count, w) ? 0 : masked_word(bits, w, n_words, n_bits);
+}
+
 __global__ void k_write_bitmap(const uint64_t* bits, uint64_t n_words, uint64_t n_bits, const BlockInfo* blocks,
-                               uint8_t* out) {
+                               const unsigned long long* bsum, uint64_t nbs, uint64_t count, uint8_t* out) {
     const BlockInfo bi = blocks[blockIdx.y];
     if (!bi.is_bitmap) return;
     const uint64_t words = (uint64_t(bi.last) - bi.first + 63) / 64;
@@ -374,8 +387,8 @@ __global__ void k_write_bitmap(const uint64_t* bits, uint64_t n_words, uint64_t 
     if (i >= words) return;
     const uint64_t start = uint64_t(bi.first) + 1 + 64 * i;  // first state of this output word
     const uint64_t w0 = start >> 6, sh = start & 63;
-    uint64_t v = masked_word(bits, w0, n_words, n_bits) >> sh;
-    if (sh && w0 + 1 < n_words) v |= masked_word(bits, w0 + 1, n_words, n_bits) << (64 - sh);
+    uint64_t v = live_word(bits, w0, n_words, n_bits, bsum, nbs, count) >> sh;
+    if (sh && w0 + 1 < n_words) v |= live_word(bits, w0 + 1, n_words, n_bits, bsum, nbs, count) << (64 - sh);
     const uint64_t hi = start + 63;  // last state this word covers
     if (hi > bi.last) {
         const uint64_t keep = uint64_t(bi.last) - start + 1;  // 0..63
@@ -572,8 +585,8 @@ struct SegmentEncoder {
             launches++;
         }
         if (any_bitmap) {
-            k_write_bitmap<<<dim3(unsigned((max_words + kT - 1) / kT), nb), kT, 0, s>>>(bits, n_words, n_bits,
-                                                                                        x.blocks, d_out);
+            k_write_bitmap<<<dim3(unsigned((max_words + kT - 1) / kT), nb), kT, 0, s>>>(
+                bits, n_words, n_bits, x.blocks, x.bsum, (n_words + kT * 16 - 1) / (kT * 16), count, d_out);
             launches++;
         }
         CD_CUDA(cudaGetLastError());
@@ -606,11 +619,32 @@ __device__ __forceinline__ uint64_t every_fourth_bit(uint64_t x) {
 // 2 (first/64 + j) + {0, 1}.  One CTA per chunk of kT * 16 out words, whose
 // popcount goes to sums[chunk] (the encoder's chunk sums); codes past the
 // last state are 0 and never match.
+// With active-window flags (one byte per 2^wb states, a superset of the
+// windows holding the depth's states), a chunk none of whose windows is
+// flagged is empty: it counts 0 and its words are left unwritten.
+__device__ __forceinline__ bool chunk_flagged(const uint8_t* flags, int wb, uint64_t n_windows, uint64_t first,
+                                              uint64_t n_out, uint64_t base) {
+    if (!flags) return true;
+    const uint64_t s0 = first + base * 64;
+    const uint64_t end_out = base + kT * 16 < n_out ? base + kT * 16 : n_out;
+    const uint64_t s1 = first + end_out * 64 - 1;
+    const uint64_t w0 = s0 >> wb, w1 = (s1 >> wb) < n_windows ? (s1 >> wb) : n_windows - 1;
+    int any = 0;
+    for (uint64_t w = w0 + threadIdx.x; w <= w1; w += kT) any |= flags[w];
+    return __syncthreads_or(any) != 0;
+}
+
 __global__ void __launch_bounds__(kT) k_frontier_two_bit(const uint64_t* __restrict__ codes, uint64_t first,
                                                           uint64_t n_out, uint32_t code, uint64_t* __restrict__ out,
-                                                          unsigned long long* __restrict__ sums) {
+                                                          unsigned long long* __restrict__ sums,
+                                                          const uint8_t* __restrict__ flags, int wb,
+                                                          uint64_t n_windows) {
     const uint64_t hi_sel = (code & 2) ? 0 : ~uint64_t(0), lo_sel = (code & 1) ? 0 : ~uint64_t(0);
     const uint64_t base = uint64_t(blockIdx.x) * kT * 16;
+    if (!chunk_flagged(flags, wb, n_windows, first, n_out, base)) {
+        if (threadIdx.x == 0) sums[blockIdx.x] = 0;
+        return;
+    }
     uint32_t c = 0;
 #pragma unroll 4
     for (int k = 0; k < 16; ++k) {
@@ -659,9 +693,11 @@ __global__ void __launch_bounds__(kT) k_frontier_nibbles(const uint64_t* __restr
 unsigned chunks_of(uint64_t n_out) { return unsigned((n_out + kT * 16 - 1) / (kT * 16)); }
 
 int frontier_bits_two_bit(const uint64_t* codes, uint64_t first_state, uint64_t n_states, uint32_t code,
-                          uint64_t* out, unsigned long long* sums, cudaStream_t s) {
+                          uint64_t* out, unsigned long long* sums, const uint8_t* flags, int window_bits,
+                          uint64_t n_windows, cudaStream_t s) {
     const uint64_t n_out = (n_states + 63) / 64;
-    k_frontier_two_bit<<<chunks_of(n_out), kT, 0, s>>>(codes, first_state, n_out, code, out, sums);
+    k_frontier_two_bit<<<chunks_of(n_out), kT, 0, s>>>(codes, first_state, n_out, code, out, sums, flags,
+                                                        window_bits, n_windows);
     CD_CUDA(cudaGetLastError());
     return PSB_OK;
 }

@@ -888,7 +888,8 @@ int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const
                 if (int rc = psb::encoder_chunk_sums(R->enc, n, &sums)) return rc;
                 t->launches++;
                 const int rc =
-                    src.codes ? psb::frontier_bits_two_bit(src.codes, first, n, src.code, R->bits, sums, s)
+                    src.codes ? psb::frontier_bits_two_bit(src.codes, first, n, src.code, R->bits, sums, src.flags,
+                                                           src.window_bits, src.n_windows, s)
                               : psb::frontier_bits_nibbles(src.nibbles, src.excl, first, n, R->bits, sums, s);
                 if (rc) return rc;
                 sums_ready = true;

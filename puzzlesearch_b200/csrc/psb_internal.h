@@ -60,9 +60,12 @@ uint64_t encoder_take_launches(SegmentEncoder* e);
 // One-bit frontier bitmaps (ceil(n_states/64) words at out; first_state a
 // multiple of 64) of a two-bit array (states with code `code`) and of a
 // frontier-search array (states with an operator bit set, less `excl`),
-// with their chunk popcounts in `sums` (from encoder_chunk_sums).
+// with their chunk popcounts in `sums` (from encoder_chunk_sums).  Two-bit
+// extraction may be given the depth's active-window flags (NULL = none):
+// chunks of unflagged windows count 0 and are not written.
 int frontier_bits_two_bit(const uint64_t* codes, uint64_t first_state, uint64_t n_states, uint32_t code,
-                          uint64_t* out, unsigned long long* sums, cudaStream_t s);
+                          uint64_t* out, unsigned long long* sums, const uint8_t* flags, int window_bits,
+                          uint64_t n_windows, cudaStream_t s);
 int frontier_bits_nibbles(const uint64_t* nibbles, const uint64_t* excl, uint64_t first_state, uint64_t n_states,
                           uint64_t* out, unsigned long long* sums, cudaStream_t s);
 }  // namespace psb
