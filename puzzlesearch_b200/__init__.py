@@ -284,16 +284,43 @@ def _algo(algo):
 DIRECTIONS = {"auto": 0, "top_down": 1, "bottom_up": 2}
 
 
-def _spill_fn(spill):
+class _Spill:
     """Wraps spill(depth, segment, stream_bytes, states) -> stop (truthy ends
     the search with PSB_ERR_ABORTED) as a psb_spill_fn.  The stream is copied
-    out of the pinned staging buffer before spill is called."""
-    def fn(_user, depth, segment, data, n, states):
-        try:
-            return 1 if spill(depth, segment, ctypes.string_at(data, n), states) else 0
-        except Exception:  # an exception cannot cross the C ABI: stop the search
-            return 1
-    return SPILL_FN(fn)
+    out of the pinned staging buffer before spill is called.  An exception
+    cannot cross the C ABI: it stops the search and is raised again by
+    run() once the library has returned."""
+
+    def __init__(self, spill):
+        self.error = None
+
+        def fn(_user, depth, segment, data, n, states):
+            try:
+                return 1 if spill(depth, segment, ctypes.string_at(data, n), states) else 0
+            except Exception as e:
+                self.error = e
+                return 1
+
+        self.fn = SPILL_FN(fn)
+
+    def run(self, call):
+        rc = call()
+        if rc < 0 and self.error is not None:
+            raise self.error
+        _check(rc)
+
+
+def _spill_fn(spill):
+    """(SPILL_FN or None, runner) for a spill argument: a SPILL_FN passes
+    through as is (it sees the pinned buffer itself)."""
+    if spill is None or isinstance(spill, SPILL_FN):
+        return spill, _check_call
+    w = _Spill(spill)
+    return w.fn, w.run
+
+
+def _check_call(call):
+    _check(call())
 
 
 def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_ms=None, level_children=None,
@@ -338,12 +365,12 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
         fin = (ctypes.c_uint64 * puzzle.final_words(algo))()
     lm = (ctypes.c_float * cap)() if levels else None
     lc = (ctypes.c_uint64 * cap)() if levels else None
-    fn = spill if isinstance(spill, SPILL_FN) or spill is None else _spill_fn(spill)
+    fn, runner = _spill_fn(spill)
     o = _opts(max_depth, window_bits, device, None, fin, lm, lc, direction, bottom_up_ratio, fn, segment_bits)
     st = BfsStats()
     st.struct_size = ctypes.sizeof(BfsStats)
-    _check(lib().psb_bfs(puzzle.handle, _algo(algo), initial, ctypes.byref(o), counts, cap, ctypes.byref(nd),
-                         ctypes.byref(st)))
+    runner(lambda: lib().psb_bfs(puzzle.handle, _algo(algo), initial, ctypes.byref(o), counts, cap,
+                                 ctypes.byref(nd), ctypes.byref(st)))
     out = {"counts": list(counts[:nd.value]), "stats": st.as_dict()}
     if final:
         out["final"] = list(fin)
@@ -371,11 +398,11 @@ class BfsSession:
         nd = ctypes.c_uint32()
         st = BfsStats()
         st.struct_size = ctypes.sizeof(BfsStats)
-        fn = _spill_fn(spill) if spill is not None else None
+        fn, runner = _spill_fn(spill)
         o = _opts(max_depth, direction=self.direction, bottom_up_ratio=bottom_up_ratio, spill=fn,
                   segment_bits=segment_bits)
-        _check(lib().psb_bfs_session_run(self._h, initial, ctypes.byref(o), self._counts, self._cap,
-                                         ctypes.byref(nd), ctypes.byref(st)))
+        runner(lambda: lib().psb_bfs_session_run(self._h, initial, ctypes.byref(o), self._counts, self._cap,
+                                                 ctypes.byref(nd), ctypes.byref(st)))
         return list(self._counts[:nd.value]), st.as_dict()
 
     def close(self):

@@ -155,3 +155,27 @@ def test_struct_layouts_match_header(tmp_path):
         assert int(out[cname]) == ctypes.sizeof(cls), cname
         for f, _ in cls._fields_:
             assert int(out[f"{cname}.{f}"]) == getattr(cls, f).offset, (cname, f)
+
+
+def test_spill_wrapper_host_logic():
+    """The Python spill wrapper: the callback sees a copy of the stream, a
+    truthy return or an exception stops the search (non-zero to the C side),
+    and the exception is raised again after the library call returns."""
+    seen = []
+    fn, runner = psb._spill_fn(lambda d, g, data, st: seen.append((d, g, data, st)) or d == 4)
+    buf = (ctypes.c_uint8 * 5)(1, 2, 3, 4, 5)
+    assert fn(None, 3, 1, buf, 5, 9) == 0 and fn(None, 4, 0, buf, 2, 1) == 1
+    assert seen == [(3, 1, b"\x01\x02\x03\x04\x05", 9), (4, 0, b"\x01\x02", 1)]
+    runner(lambda: 0)
+    with pytest.raises(psb.PsbError):
+        runner(lambda: -8)
+
+    def boom(*a):
+        raise ValueError("disk full")
+
+    fn, runner = psb._spill_fn(boom)
+    assert fn(None, 0, 0, buf, 1, 1) == 1
+    with pytest.raises(ValueError):
+        runner(lambda: -8)
+    raw = psb.SPILL_FN(lambda *a: 0)
+    assert psb._spill_fn(raw)[0] is raw and psb._spill_fn(None)[0] is None

@@ -124,6 +124,14 @@ def test_spill_callback_stops_search():
         psb.bfs(psb.PancakeSimple(9), "three_bit", 0, spill=sink)
     assert e.value.code == -8
 
+    def failing(depth, segment, data, states):
+        if depth == 2:
+            raise KeyError("sink full")
+
+    with pytest.raises(KeyError):  # the callback's own exception, once the search has stopped
+        psb.bfs(psb.PancakeSimple(9), "two_bit", 0, spill=failing)
+    assert psb.bfs(psb.PancakeSimple(9), "two_bit", 0)["counts"][:3] == [1, 8, 56]
+
 
 def test_bad_segment_bits():
     with pytest.raises(psb.PsbError) as e:
