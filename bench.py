@@ -240,10 +240,23 @@ def batch_bench(args):
         t = BATCH_TYPES[rng.randrange(len(BATCH_TYPES))]
         items.append((i, t, solvable_start(rng, *t, puzzles[t])))
     total_states = sum(puzzles[t].IndexesCount() // (2 if t[0] == "sliding" else 1) for _, t, _ in items)
+    direction = "top_down" if args.direction == "top_down" else "auto"
+    blocks_per_sm, tuning = 0, None
+    if args.autotune:  # persistent grid picked on a separate calibration batch (another seed)
+        from puzzlesearch_b200 import autotune
+        crng = random.Random(77)
+        calib = []
+        for _ in range(min(1024, args.instances)):
+            t = BATCH_TYPES[crng.randrange(len(BATCH_TYPES))]
+            calib.append((puzzles[t], solvable_start(crng, *t, puzzles[t])))
+        blocks_per_sm, timings = autotune.tune_engine(calib, candidates=(1, 2, 3, 4), pool_bytes=24 << 30,
+                                                      direction=direction)
+        tuning = {"blocks_per_sm": blocks_per_sm, "calibration_instances": len(calib),
+                  "seconds": {str(k): round(v, 4) for k, v in timings.items()}}
 
     def run_batched():
         eng = psb.Engine(max_instances=args.instances, max_depths=128, pool_bytes=24 << 30,
-                         direction="top_down" if args.direction == "top_down" else "auto")
+                         blocks_per_sm=blocks_per_sm, direction=direction)
         t0 = time.perf_counter()
         for i, t, st in items:
             assert eng.add(puzzles[t], st, i)
@@ -273,7 +286,8 @@ def batch_bench(args):
             "value": len(items) / b_dt, "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": args.warmup,
             "higher_is_better": True, "dtype": "u64", "data": "seeded random solvable starts",
             "config": {"workload": "batch4096", "instances": len(items), "states": total_states,
-                       "engine_levels": levels, "direction": "top_down" if args.direction == "top_down" else "auto"},
+                       "engine_levels": levels, "direction": direction,
+                       "blocks_per_sm": blocks_per_sm or 2, "autotune": tuning},
             "batched": {"seconds": b_dt, "solves_per_s": len(items) / b_dt, "states_per_s": total_states / b_dt},
             "plain_one_per_launch": {"seconds": p_dt, "solves_per_s": len(items) / p_dt,
                                      "states_per_s": total_states / p_dt},
@@ -393,6 +407,9 @@ def main():
                     help="encode every depth's frontier on the GPU (segment streams) and hand it over in pinned"
                          " host memory during the timed searches")
     ap.add_argument("--segment-bits", type=int, default=0, help="with --spill: 2^bits states per segment (0 = 32)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the level window (single searches) or the engine's blocks per SM (batch4096) by"
+                         " timing the candidates first")
     ap.add_argument("--profile-once", action="store_true",
                     help="run ONE search (no warm-up, no e2e, no CPU baseline) and print per-level times; for ncu")
     ap.add_argument("--max-depth", type=int, default=0, help="with --profile-once: stop after this depth")
@@ -424,6 +441,11 @@ def main():
     puzzle = {"pancake": lambda: psb.PancakeSimple(a), "sliding": lambda: psb.SlidingTilePuzzleSimple(a, b),
               "hanoi4": lambda: psb.FourPegHanoiSimple(a, bool(b))}[kind]()
     N = puzzle.IndexesCount()
+    tuning = None
+    if args.autotune and not args.window_bits:
+        from puzzlesearch_b200 import autotune
+        args.window_bits, timings = autotune.tune_window_bits(puzzle, algo, 0, direction=args.direction)
+        tuning = {"window_bits": args.window_bits, "search_ms": {str(k): round(v, 2) for k, v in timings.items()}}
     stream = torch.cuda.Stream()
     # Session on torch's stream so the CUDA events below bracket exactly the searches.
     opts = psb._opts(0, args.window_bits, local, stream.cuda_stream, direction=args.direction)
@@ -482,7 +504,7 @@ def main():
     # grows the library's memory pool.
     for _ in range(args.warmup):
         psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
-                spill=spill_fn, segment_bits=args.segment_bits)
+                spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -491,7 +513,7 @@ def main():
     for _ in range(args.steps):
         tc = time.perf_counter()
         r = psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
-                    spill=spill_fn, segment_bits=args.segment_bits)
+                    spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits)
         calls.append(time.perf_counter() - tc)
         assert r["counts"] == ref_counts
         levels = r["stats"]["levels"]
@@ -550,6 +572,8 @@ def main():
         "direction": {"mode": args.direction, "bottom_up_levels": st.bottom_up_levels, "levels": st.levels},
         "clocks": clk.summary(),
     }
+    if tuning:
+        line["config"]["autotune"] = tuning
     if args.spill:
         line["spill"] = {"segment_bits": args.segment_bits or 32, "bytes_per_step": st.spill_bytes,
                          "segments_per_step": st.spill_segments,

@@ -65,6 +65,9 @@ const char* psb_version(void);
 int psb_last_error(char* buf, int cap);
 /* Number of visible CUDA devices (0 when none). */
 int psb_device_count(int* count);
+/* Name, compute capability and SM count of `device` (-1 = current), e.g. for
+ * keying tuning results. */
+int psb_device_name(int device, char* buf, int cap);
 
 /* --- Puzzle (Common/Puzzle.h:16-48) --------------------------------------- */
 

@@ -99,6 +99,7 @@ def lib():
         L.psb_version.restype = ctypes.c_char_p
         L.psb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int]
         L.psb_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
+        L.psb_device_name.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
         L.psb_puzzle_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
         L.psb_puzzle_destroy.argtypes = [P]
         L.psb_puzzle_info.argtypes = [P, u64p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
@@ -154,6 +155,13 @@ def _check(rc):
         lib().psb_last_error(buf, 512)
         raise PsbError(rc, buf.value.decode(errors="replace"))
     return rc
+
+
+def device_name(device=-1):
+    """psb_device_name: e.g. "NVIDIA B200 (sm_100, 148 SMs)"."""
+    buf = ctypes.create_string_buffer(256)
+    _check(lib().psb_device_name(device, buf, 256))
+    return buf.value.decode()
 
 
 def device_count():

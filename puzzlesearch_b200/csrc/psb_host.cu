@@ -351,6 +351,16 @@ int psb_device_count(int* count) {
     return PSB_OK;
 }
 
+int psb_device_name(int device, char* buf, int cap) {
+    if (!buf || cap <= 0) return fail(PSB_ERR_ARG, "bad argument");
+    if (int rc = ensure_device(device)) return rc;
+    if (device < 0) PSB_CUDA(cudaGetDevice(&device));
+    cudaDeviceProp prop{};
+    PSB_CUDA(cudaGetDeviceProperties(&prop, device));
+    snprintf(buf, size_t(cap), "%s (sm_%d%d, %d SMs)", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
+    return PSB_OK;
+}
+
 int psb_puzzle_create(int kind, int a, int b, psb_puzzle** out) {
     if (!out) return fail(PSB_ERR_ARG, "out is NULL");
     auto p = std::make_unique<psb_puzzle>();

@@ -1,0 +1,44 @@
+"""The autotuner on the GPU: every candidate launch shape gives the same
+counts (the tuner checks it), the pick is one of the candidates, and a
+cached pick is reused without timing again."""
+import random
+
+import pytest
+
+import puzzlesearch_b200 as psb
+from puzzlesearch_b200 import autotune
+
+pytestmark = pytest.mark.gpu
+
+
+def test_engine_blocks_per_sm(tmp_path):
+    rng = random.Random(3)
+    items = []
+    for _ in range(96):
+        p = [psb.PancakeSimple(8), psb.PancakeSimple(9), psb.SlidingTilePuzzleSimple(3, 3)][rng.randrange(3)]
+        start = rng.randrange(p.IndexesCount()) if p.Name().startswith("Pancake") else 0
+        items.append((p, start))
+    cache = autotune.Cache(str(tmp_path / "tune.json"))
+    best, timings = autotune.tune_engine(items, candidates=(1, 2, 4), pool_bytes=1 << 30, cache=cache, key="mix")
+    assert best in (1, 2, 4) and set(timings) == {1, 2, 4}
+    again, t2 = autotune.tune_engine(items, candidates=(1, 2, 4), pool_bytes=1 << 30, cache=cache, key="mix")
+    assert again == best and t2 == {}
+    # the tuned grid gives the single-instance counts
+    eng = psb.Engine(max_instances=8, pool_bytes=1 << 30, blocks_per_sm=best)
+    for tag, (p, s) in enumerate(items[:8]):
+        assert eng.add(p, s, tag)
+    done = {}
+    while len(done) < 8:
+        eng.step(8)
+        done.update(eng.poll())
+    eng.close()
+    for tag, (p, s) in enumerate(items[:8]):
+        assert done[tag] == psb.bfs(p, "two_bit", s)["counts"]
+
+
+def test_window_bits():
+    p = psb.PancakeSimple(10)
+    best, timings = autotune.tune_window_bits(p, "three_bit", candidates=[10, 12, 14])
+    assert best in (10, 12, 14) and set(timings) == {10, 12, 14}
+    assert all(ms > 0 for ms in timings.values())
+    assert psb.device_name().startswith("NVIDIA")
