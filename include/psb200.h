@@ -352,10 +352,15 @@ int psb_server_stop(psb_server* s);
  * device array of 4 MiB + 256 bytes that every GPU loading the library holds
  * until exit; searches needing more than 2^21 windows (more than ~1.4e11
  * states) return PSB_ERR_CAPACITY.  All calls share that array: calls whose
- * GPU work overlaps race, so run them one after the other.  The first call on
- * a device looks the array's address up; make it before any stream capture.
- * For PSB_TWO_BIT the final code array is d_arrays[0 .. ceil(2N/64)) on
- * return, in the reference's layout. */
+ * GPU work overlaps race, so run them one after the other.  d_arrays must be
+ * 256-byte aligned (PSB_ERR_ARG otherwise, before the device is touched).
+ * The first call on a device loads the library's kernels and the static
+ * array (lazy module loading takes device memory from the driver then), so a
+ * caller that reserves all device memory for its arena makes one small call
+ * first.  Every call synchronizes `stream` once per level, so it must not be
+ * called while that stream is being captured.  For PSB_TWO_BIT the final
+ * code array is d_arrays[0 .. ceil(2N/64)) on return, in the reference's
+ * layout. */
 int psb_bfs_noalloc(const psb_puzzle* p, int algo, uint64_t initial_index, uint64_t* d_arrays,
                     uint64_t d_array_words, uint32_t max_depth, void* stream, uint64_t* depth_counts,
                     uint32_t counts_cap, uint32_t* n_depths);

@@ -12,12 +12,19 @@
 #   * a generated <intrin.h> mapping the MSVC intrinsics to GCC builtins, and
 #     the AVX-512VL byte load/store intrinsics to their SSE2 equivalents so the
 #     library runs on any x86-64-v3 host.
-# Outputs: oracle/_ref/libpsbref.so (C ABI from oracle/ref_capi.cpp) and
-#          oracle/_ref/psbref (CLI used for the CPU baseline timing).
+# Outputs: oracle/_ref/libpsbref.so (C ABI from oracle/ref_capi.cpp),
+#          oracle/_ref/psbref (CLI used for the CPU baseline timing) and
+#          oracle/_ref/psbref_mt (multi-threaded level loop over the reference's
+#          own expanders, for the large per-depth count fixtures).
 set -euo pipefail
-REF="${PSB_REFERENCE:-/root/reference}"
+# The reference's source tree: the first argument, else $PSB_REFERENCE.
+REF="${1:-${PSB_REFERENCE:-}}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
+if [ -z "$REF" ]; then
+    echo "usage: build_ref.sh <reference source tree> (or set PSB_REFERENCE); keeping any prebuilt $OUT" >&2
+    exit 0
+fi
 if [ ! -d "$REF/Common" ]; then
     echo "build_ref: reference sources not found at $REF; keeping any prebuilt $OUT" >&2
     exit 0
@@ -74,4 +81,5 @@ for f in $COMMON $PUZZLES; do case "$f" in *.cpp)
     d=Common; [ -f "$SRC/Puzzles/$f" ] && d=Puzzles; SOURCES="$SOURCES $SRC/$d/$f";; esac; done
 $CXX $FLAGS -shared -o "$OUT/libpsbref.so" "$HERE/ref_capi.cpp" $SOURCES
 $CXX $FLAGS -o "$OUT/psbref" "$HERE/ref_main.cpp" "$HERE/ref_capi.cpp" $SOURCES
-echo "build_ref: built $OUT/libpsbref.so and $OUT/psbref"
+$CXX $FLAGS -pthread -o "$OUT/psbref_mt" "$HERE/ref_mt_bfs.cpp" $SOURCES
+echo "build_ref: built $OUT/libpsbref.so, $OUT/psbref and $OUT/psbref_mt"

@@ -18,7 +18,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.environ.get("PSB_BUILD_DIR") or os.path.join(HERE, "_build")
 LIB = os.environ.get("PSB_LIB_OUT") or os.path.join(HERE, "libpsb200.so")
-EXTRA = os.environ.get("PSB_EXTRA_NVCC_FLAGS", "").split()  # e.g. -DPSB_THREADS=512 for tuning builds
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -35,7 +34,7 @@ def host_compiler():
 
 def flags(verbose):
     f = GENCODE + ["-O3", "-lineinfo", "-std=c++17", "-ccbin", host_compiler(),
-                   "-Xcompiler", "-fPIC,-O3", "-I" + os.path.join(HERE, "..", "include")] + EXTRA
+                   "-Xcompiler", "-fPIC,-O3", "-I" + os.path.join(HERE, "..", "include")]
     if verbose:
         f += ["-Xptxas", "-v"]
     return f

@@ -40,51 +40,15 @@ constexpr int kThreads = 256;  // finalize and batched-expand kernels
 
 enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 
-#ifndef PSB_PAIR_WORDS
-#define PSB_PAIR_WORDS 1
-#endif
-#ifndef PSB_PROBE_TWO_ROUNDS
-#define PSB_PROBE_TWO_ROUNDS 1
-#endif
-#ifndef PSB_PROBE_DESC
-#define PSB_PROBE_DESC 0
-#endif
-#ifndef PSB_FLIP4_WORDS
-#define PSB_FLIP4_WORDS 1
-#endif
-#ifndef PSB_FLIP3_WORDS
-#define PSB_FLIP3_WORDS 1
-#endif
-#ifndef PSB_TD_MIN_BLOCKS
-#define PSB_TD_MIN_BLOCKS 1
-#endif
-#ifndef PSB_TD2_MIN_BLOCKS
-#define PSB_TD2_MIN_BLOCKS 4
-#endif
-#ifndef PSB_BU_MIN_BLOCKS
-#define PSB_BU_MIN_BLOCKS 4
-#endif
-
 // Block shape of the level kernel per mode, chosen by a sweep on B200:
-// two-bit reads the target's code before each long-range mark, so it wants
-// more resident warps (four 256-thread blocks per SM); three-bit's marks are
-// fire-and-forget, and it runs fastest without a register cap.
-// PSB_THREADS / PSB_MIN_BLOCKS override every mode (tuning builds only).
+// two-bit top-down wants more resident warps (four 256-thread blocks per SM);
+// three-bit's marks are fire-and-forget, and it runs fastest without a
+// register cap.  Bottom-up levels wait on their probe loads, so they want
+// resident warps too (four blocks per SM).
 template <int MODE, bool BU = false>
 struct Shape {
-#ifdef PSB_THREADS
-    static constexpr int threads = PSB_THREADS;
-#else
     static constexpr int threads = 256;
-#endif
-#ifdef PSB_MIN_BLOCKS
-    static constexpr int min_blocks = PSB_MIN_BLOCKS;
-#else
-    // Bottom-up levels wait on their probe loads, so they want resident warps
-    // too, but not at the price of spills (two-bit's 64-register cap spills).
-    static constexpr int min_blocks = BU ? PSB_BU_MIN_BLOCKS : MODE == kTwoBit ? PSB_TD2_MIN_BLOCKS
-                                        : MODE == kFrontier ? 2 : PSB_TD_MIN_BLOCKS;
-#endif
+    static constexpr int min_blocks = BU ? 4 : MODE == kTwoBit ? 4 : MODE == kFrontier ? 2 : 1;
 };
 
 __host__ __device__ constexpr int level_threads(int mode) {
@@ -103,9 +67,6 @@ struct PuzzleArgs {
 // Adapters giving the three puzzles one device interface.  probe_range
 // generates the children of one bottom-up probe round: the round starting at
 // child `first` covers children first .. first+kProbeRound-1 in expansion order.
-#ifndef PSB_PROBE_ROUND
-#define PSB_PROBE_ROUND 4
-#endif
 // kPairOp0: operator 0 maps state i to i ^ 1 (the pancake flip of the last
 // two values only toggles the lowest Lehmer digit, of weight 1!), so a level
 // kernel can mark those children for a whole frontier word at once and expand
@@ -117,7 +78,7 @@ template <int N>
 struct PancakeK {
     static constexpr int kBranch = N - 1;
     static constexpr int kOps = N - 1;
-    static constexpr int kProbeRound = PSB_PROBE_ROUND < N - 1 ? PSB_PROBE_ROUND : N - 1;
+    static constexpr int kProbeRound = 4 < N - 1 ? 4 : N - 1;
     static constexpr bool kPairOp0 = true;
     static constexpr bool kFlip3Op1 = N >= 3;  // operator 1 permutes each aligned block of 6 (see flip3_push)
     static constexpr bool kFlip4Op2 = N >= 4;  // operator 2 permutes each aligned block of 24 (see flip4_pull)
@@ -245,60 +206,35 @@ __device__ __forceinline__ uint32_t nibble_flags(uint64_t x) {
 // are never reused, so they are marked evict-first: they no longer displace
 // the region that the flips of 9..12 keep hitting (a flip of m stays inside
 // its aligned block of m! states).  13-pancake depth 11: 79 -> 72 ms.
-#ifndef PSB_FAR_HINT
-#define PSB_FAR_HINT 1
-#endif
 __device__ __forceinline__ uint64_t l2_evict_first() {
     uint64_t p;
     asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
     return p;
 }
 __device__ __forceinline__ void red_or_far(unsigned int* a, unsigned int v) {
-    if constexpr (PSB_FAR_HINT)
-        asm volatile("red.global.or.b32.L2::cache_hint [%0], %1, %2;" ::"l"(a), "r"(v), "l"(l2_evict_first())
-                     : "memory");
-    else
-        atomicOr(a, v);
+    asm volatile("red.global.or.b32.L2::cache_hint [%0], %1, %2;" ::"l"(a), "r"(v), "l"(l2_evict_first())
+                 : "memory");
 }
 __device__ __forceinline__ uint64_t ld_cg_far(const unsigned long long* a) {
-    if constexpr (PSB_FAR_HINT) {
-        uint64_t v;
-        asm volatile("ld.global.cg.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
-        return v;
-    } else {
-        return __ldcg(a);
-    }
+    uint64_t v;
+    asm volatile("ld.global.cg.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
+    return v;
 }
 __device__ __forceinline__ uint64_t ld_nc_far(const uint64_t* a) {
-    if constexpr (PSB_FAR_HINT) {
-        uint64_t v;
-        asm("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
-        return v;
-    } else {
-        return __ldg(a);
-    }
+    uint64_t v;
+    asm("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
+    return v;
 }
 __device__ __forceinline__ uint64_t ld_far(const uint64_t* a) {
-    if constexpr (PSB_FAR_HINT) {
-        uint64_t v;
-        asm volatile("ld.global.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
-        return v;
-    } else {
-        return *a;
-    }
+    uint64_t v;
+    asm volatile("ld.global.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(l2_evict_first()));
+    return v;
 }
 
 // Shared-memory marks: one bit per state (1-bit modes) or four operator bits
-// per state (frontier search).  PSB_BYTE_MARKS (tuning builds) keeps one byte
-// per state for the 1-bit modes and marks with plain stores instead of atomics.
-#ifdef PSB_BYTE_MARKS
-constexpr bool kByteMarks = true;
-#else
-constexpr bool kByteMarks = false;
-#endif
-
+// per state (frontier search).
 __host__ __device__ constexpr size_t mark_bytes(int mode, size_t window_states) {
-    return mode == kFrontier ? window_states / 2 : kByteMarks ? window_states : window_states / 8;
+    return mode == kFrontier ? window_states / 2 : window_states / 8;
 }
 
 // Warp chunk: 32 lanes x one unit each (64 states; 32 for two-bit codes).
@@ -443,8 +379,6 @@ struct Emitter {
         ++local;
         if constexpr (MODE == kFrontier) {
             atomicOr(&smarks[o >> 3], 1u << (4 * (o & 7u) + op));
-        } else if constexpr (kByteMarks) {
-            reinterpret_cast<uint8_t*>(smarks)[o] = 1;
         } else {
             atomicOr(&smarks[o >> 5], 1u << (o & 31u));
         }
@@ -529,14 +463,6 @@ struct Probe {
     __device__ __forceinline__ void far(uint64_t c, uint32_t) { probe<true>(c); }
 };
 
-// 32 marks held as bytes (0/1) -> 32-bit mask.
-__device__ __forceinline__ uint32_t bytes_to_bits(const uint32_t* b8) {
-    uint32_t r = 0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) r |= (((b8[k] & 0x01010101u) * 0x01020408u) >> 24 & 15u) << (4 * k);
-    return r;
-}
-
 // Shared variables of one window pass (a kernel's static shared memory).
 struct WindowShared {
     uint32_t any;         // some warp found a frontier state in the window
@@ -565,16 +491,16 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     // Operator-0 children marked per frontier word in the sweep (see PancakeK);
     // bottom-up: unvisited states whose operator-0 neighbour is in the
     // frontier, found per word before any probing.
-    constexpr bool kPairs = PSB_PAIR_WORDS && PZ::kPairOp0 && MODE != kFrontier && !BU && !kByteMarks;
-    constexpr bool kBuPairs = PSB_PAIR_WORDS && PZ::kPairOp0 && BU && !kByteMarks;
+    constexpr bool kPairs = PZ::kPairOp0 && MODE != kFrontier && !BU;
+    constexpr bool kBuPairs = PZ::kPairOp0 && BU;
     // three-bit / classic bottom-up pairs also read the unit's frontier word
     constexpr bool kProbeWord = kBuPairs && MODE != kTwoBit;
     // Operator-1 children (top-down) and hits (bottom-up) per unit as well
     // (flip3_push / flip3_pull); per-state expansion then starts at operator 2.
-    constexpr bool kFlip3 = PSB_FLIP3_WORDS && kPairs && PZ::kFlip3Op1;
-    constexpr bool kBuFlip3 = PSB_FLIP3_WORDS && kBuPairs && PZ::kFlip3Op1;
+    constexpr bool kFlip3 = kPairs && PZ::kFlip3Op1;
+    constexpr bool kBuFlip3 = kBuPairs && PZ::kFlip3Op1;
     // Bottom-up also finds operator-2 hits per unit (flip4_pull).
-    constexpr bool kBuFlip4 = PSB_FLIP4_WORDS && kBuFlip3 && PZ::kFlip4Op2;
+    constexpr bool kBuFlip4 = kBuFlip3 && PZ::kFlip4Op2;
     constexpr int kThreads = KTHREADS;
     constexpr int kWarps = kThreads / 32;
     constexpr uint32_t kSPU = states_per_unit(MODE);
@@ -828,19 +754,15 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 // rounds (each round re-unranks the states still listed; 13-pancake
                 // depth 12: 58 ms in 2 rounds of 5 against 65 ms in 3 rounds of 4).
                 constexpr int kLeftChildren = PZ::kBranch - (kBuFlip4 ? 3 : kBuFlip3 ? 2 : kBuPairs ? 1 : 0);
-                constexpr int R = (PSB_PROBE_TWO_ROUNDS && PZ::kPairOp0) ? (kLeftChildren > 1 ? (kLeftChildren + 1) / 2 : 1)
-                                                                         : PZ::kProbeRound;
+                constexpr int R = PZ::kPairOp0 ? (kLeftChildren > 1 ? (kLeftChildren + 1) / 2 : 1) : PZ::kProbeRound;
                 const uint32_t cur_pat = a.cur_code == 2 ? 1u : 3u;
                 uint32_t left = total;
                 constexpr int kFirst = kBuFlip4 ? 3 : kBuFlip3 ? 2 : kBuPairs ? 1 : 0;
                 constexpr int kRounds = (PZ::kBranch - kFirst + R - 1) / R;
                 for (int round = 0; round < kRounds && left; ++round) {
-                    // children [lo, hi) of this round: ascending from kFirst, or
-                    // (PSB_PROBE_DESC) descending from the last child
-                    const int lo = PSB_PROBE_DESC ? (PZ::kBranch - (round + 1) * R > kFirst ? PZ::kBranch - (round + 1) * R : kFirst)
-                                                  : kFirst + round * R;
-                    const int hi = PSB_PROBE_DESC ? PZ::kBranch - round * R
-                                                  : (lo + R < PZ::kBranch ? lo + R : PZ::kBranch);
+                    // children [lo, hi) of this round, ascending from kFirst
+                    const int lo = kFirst + round * R;
+                    const int hi = lo + R < PZ::kBranch ? lo + R : PZ::kBranch;
                     uint32_t kept = 0;
                     for (uint32_t e0 = 0; e0 < left; e0 += 32) {
                         const uint32_t e = e0 + uint32_t(lane);
@@ -861,8 +783,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                             pbad |= pr.bad;
                             if (pr.hit) {
                                 ++hits;
-                                if constexpr (kByteMarks) reinterpret_cast<uint8_t*>(smarks)[o] = 1;
-                                else atomicOr(&smarks[o >> 5], 1u << (o & 31u));
+                                atomicOr(&smarks[o >> 5], 1u << (o & 31u));
                             } else {
                                 miss = true;
                             }
@@ -913,7 +834,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
             const uint32_t next_pat = em.next_pat;
             unsigned long long* codes = reinterpret_cast<unsigned long long*>(a.marks) + (base >> 5);
             for (uint32_t i = tid; i < W / 32; i += kThreads) {
-                const uint32_t v = kByteMarks ? bytes_to_bits(smarks + 8 * i) : smarks[i];
+                const uint32_t v = smarks[i];
                 if (!v || (base >> 5) + i >= a.mark_words) continue;
                 const uint64_t w = __ldcg(codes + i);
                 const uint64_t unvisited = ~(w | (w >> 1)) & kEven;
@@ -928,12 +849,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
             unsigned long long* g = reinterpret_cast<unsigned long long*>(a.marks) + (base >> kShift);
             const uint32_t words = MODE == kFrontier ? W / 16 : W / 64;
             for (uint32_t i = tid; i < words; i += kThreads) {
-                unsigned long long v;
-                if constexpr (MODE != kFrontier && kByteMarks)
-                    v = (unsigned long long)bytes_to_bits(smarks + 16 * i) |
-                        ((unsigned long long)bytes_to_bits(smarks + 16 * i + 8) << 32);
-                else
-                    v = smem64[i];
+                const unsigned long long v = smem64[i];
                 if (v && (base >> kShift) + i < a.mark_words) {
                     atomicOr(g + i, v);
                     // three-bit bottom-up: the found states join the visited

@@ -16,14 +16,25 @@
 //
 // The array is shared by every call: each call clears what must start at
 // zero.  Calls whose GPU work overlaps (two host threads, or two streams)
-// race on it; run them one after the other.  The first call on a device looks
-// up the array's device address (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture.
+// race on it; run them one after the other.  Every call looks up the array's
+// device address (cudaGetSymbolAddress) with the caller's device current, so
+// a context rebuilt after cudaDeviceReset gets its own address.
+//
+// The CUDA runtime loads a module lazily: the first call on a device loads
+// this file's module (with the array) and the level kernels' modules, and
+// that load takes device memory from the driver.  A caller that reserves all
+// device memory for its own arena makes one call (any small search) first.
+// Each call synchronizes `stream` at every level (it reads the level's
+// counters back), so it must not be called while that stream is captured.
+//
+// d_arrays must be 256-byte aligned: the finalize sweeps read it 16 bytes at
+// a time and the arrays inside it are padded to 256 bytes.  Any other pointer
+// is rejected with PSB_ERR_ARG before the device is touched.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
-#include <mutex>
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -37,10 +48,6 @@ constexpr size_t kScratchBytes = 256 + 2 * kMaxWindows;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_ptr[kMaxDevices] = {nullptr};
-
 int na_fail(int code, const std::string& msg) { return psb_set_error(code, msg.c_str()); }
 
 #define NA_CUDA(call)                                                                    \
@@ -50,18 +57,13 @@ int na_fail(int code, const std::string& msg) { return psb_set_error(code, msg.c
             return na_fail(PSB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-// Device address of the scratch array on the current device (looked up once).
+// Device address of the scratch array on the current device.  Looked up on
+// every call: it is cheap, and a cached address would go stale when the
+// context is rebuilt.
 int scratch_address(unsigned char** out) {
-    int dev = 0;
-    NA_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return na_fail(PSB_ERR_ARG, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_ptr[dev]) {
-        void* ptr = nullptr;
-        NA_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        g_scratch_ptr[dev] = ptr;
-    }
-    *out = static_cast<unsigned char*>(g_scratch_ptr[dev]);
+    void* ptr = nullptr;
+    NA_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    *out = static_cast<unsigned char*>(ptr);
     return PSB_OK;
 }
 
@@ -83,6 +85,8 @@ extern "C" int psb_bfs_noalloc(const psb_puzzle* p, int algo, uint64_t initial, 
                                uint64_t d_array_words, uint32_t max_depth, void* stream_ptr, uint64_t* counts,
                                uint32_t cap, uint32_t* n_depths) {
     if (!p || !d_arrays || !counts || !n_depths || cap == 0) return na_fail(PSB_ERR_ARG, "bad argument");
+    if (reinterpret_cast<uintptr_t>(d_arrays) % 256 != 0)
+        return na_fail(PSB_ERR_ARG, "d_arrays must be 256-byte aligned");
     const uint64_t N = p->n_states;
     if (initial >= N) return na_fail(PSB_ERR_ARG, "initial index >= IndexesCount()");
     int mode = -1, n_arr = 0;

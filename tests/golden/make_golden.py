@@ -337,7 +337,8 @@ def ref_expand_batches(lib):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("PSB_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("PSB_REFERENCE"), required=not os.environ.get("PSB_REFERENCE"),
+                    help="the reference project's source tree (or set PSB_REFERENCE)")
     ap.add_argument("--skip-ref-runs", action="store_true")
     args = ap.parse_args()
     ref = args.reference

@@ -126,6 +126,21 @@ def test_footprint():
     assert psb.PancakeSimple(9).final_words("three_bit") == 3 * ((math.factorial(9) + 63) // 64)
 
 
+def test_noalloc_rejects_unaligned_arrays_on_the_host():
+    """psb_bfs_noalloc checks d_arrays' 256-byte alignment before it touches
+    the device, so this address is never dereferenced (no GPU needed)."""
+    p = psb.PancakeSimple(8)
+    cap = 64
+    counts = (ctypes.c_uint64 * cap)()
+    nd = ctypes.c_uint32()
+    for addr in (0x100008, 0x100080):
+        rc = psb.lib().psb_bfs_noalloc(p.handle, psb.THREE_BIT, 0, ctypes.cast(addr, psb.u64p), 1 << 20, 0,
+                                       None, counts, cap, ctypes.byref(nd))
+        with pytest.raises(psb.PsbError) as e:
+            psb._check(rc)
+        assert e.value.code == -1 and "aligned" in str(e.value)
+
+
 def test_no_device_error_without_gpu():
     if psb.device_count() > 0:
         pytest.skip("a GPU is visible")

@@ -79,3 +79,16 @@ def test_rejects_what_does_not_fit():
     rc = psb.lib().psb_bfs_noalloc(huge.handle, psb.TWO_BIT, 0, ctypes.cast(small.data_ptr(), psb.u64p),
                                    2 ** 62, 0, None, counts, cap, ctypes.byref(nd))
     assert rc == -4
+
+
+def test_rejects_unaligned_arrays():
+    """A sub-tensor one word in is 8-byte aligned only: rejected on the host
+    before the device is touched, and the next aligned call still works."""
+    torch = pytest.importorskip("torch")
+    p = psb.PancakeSimple(9)
+    d = torch.empty(p.footprint("three_bit") // 8 + 64, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    with pytest.raises(psb.PsbError) as e:
+        noalloc(p, "three_bit", d[1:])
+    assert e.value.code == -1
+    assert noalloc(p, "three_bit", d) == psb.bfs(p, "three_bit", 0)["counts"]
