@@ -3,12 +3,16 @@
 //
 // It mirrors, name for name, what lightln2/PuzzleSearch callers use on the
 // complete-BFS path:
-//   Puzzle                      Common/Puzzle.h:16-48
+//   Puzzle (abstract)           Common/Puzzle.h:16-48
 //   ExpandHint                  Common/Puzzle.h:11-14
-//   ExpandBuffer                Common/Puzzle.h:50-120
+//   ExpandBuffer                Common/Puzzle.h:50-120, Common/Puzzle.cpp:3-13
+//   Buffer<T> (the fixed-capacity buffer CrossSegmentPostProcess takes)
+//                               Common/Buffer.h:10-60
 //   SlidingTilePuzzleSimple     Puzzles/SlidingTilePuzzleSimple.h:8-40
+//   SlidingTilePuzzleGpu        Puzzles/SlidingTilePuzzleGpu.h:7-30
 //   PancakeSimple               Puzzles/PancakeSimple.h:8-37
 //   FourPegHanoiSimple          Puzzles/FourPegHanoiSimple.h:8-40
+//   FourPegHanoiGPU             Puzzles/FourPegHanoiGPU.h:8-22
 //   InMemoryClassicBFS, InMemoryTwoBitBFS, InMemoryThreeBitBFS,
 //   InMemoryFrontierSearch      Common/InMemoryBFS.h:5-11
 // so the reference's tests and drivers compile against it by swapping
@@ -16,12 +20,25 @@
 // PSB200_GLOBAL_NAMES before including to also declare them in the global
 // namespace, as the reference does.
 //
-// Differences, all on the error path: failures throw psb200::Error (a
+// The *Gpu classes use the same index spaces as the *Simple ones (n! tile
+// permutations, 4^n peg assignments), as in the reference, and so does every
+// search here: all of them run on the GPU.
+//
+// Puzzle is abstract, as in the reference, so callers may derive their own
+// puzzles: ExpandBuffer batches work for any Puzzle (it calls the virtual
+// Expand), but the InMemory*BFS searches run only on this library's puzzle
+// classes, whose expanders are device kernels.  Given any other Puzzle they
+// throw psb200::Error with code PSB_ERR_UNSUPPORTED.
+//
+// Other differences, all on the error path: failures throw psb200::Error (a
 // std::runtime_error carrying the C status code) where the reference calls
 // ensure() -> exit(-1) or throws std::runtime_error from GPU.cu.
 #pragma once
 
+#include <atomic>
+#include <chrono>
 #include <cstdint>
+#include <iostream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -52,32 +69,100 @@ struct ExpandHint {
     bool CrossSegment = false;
 };
 
+// Buffer<T> (Common/Buffer.h:10-60): a buffer of fixed capacity whose size
+// changes without initialising its elements.
+template <typename T>
+class Buffer {
+public:
+    explicit Buffer(size_t capacity) : size_(0), data_(capacity) {}
+    size_t Capacity() const { return data_.size(); }
+    void SetCapacity(size_t capacity) { data_.resize(capacity); }
+    size_t Size() const { return size_; }
+    void SetSize(size_t size) {
+        if (size > Capacity()) throw Error(PSB_ERR_CAPACITY, "psb200: Buffer size above capacity");
+        size_ = size;
+    }
+    T& operator[](size_t index) { return data_[index]; }
+    const T& operator[](size_t index) const { return data_[index]; }
+    void Add(T value) { data_[size_++] = value; }
+    void Clear() { size_ = 0; }
+    bool IsFull() const { return size_ == Capacity(); }
+    bool IsEmpty() const { return size_ == 0; }
+    T* Buf() { return data_.data(); }
+    const T* Buf() const { return data_.data(); }
+
+private:
+    size_t size_;
+    std::vector<T> data_;
+};
+
+// Puzzle (Common/Puzzle.h:16-48): the abstract state space.
 class Puzzle {
 public:
     static constexpr size_t MAX_INDEXES_BUFFER = 2 * 1024 * 1024;
     static constexpr uint64_t INVALID_INDEX = uint64_t(-1);
 
-    Puzzle(const Puzzle&) = delete;
-    Puzzle& operator=(const Puzzle&) = delete;
-    virtual ~Puzzle() { psb_puzzle_destroy(h_); }
+    virtual ~Puzzle() = default;
 
-    std::string Name() const {
+    virtual std::string Name() const = 0;
+    virtual int OperatorsCount() const = 0;
+    virtual int BranchingFactor() const = 0;
+    virtual uint64_t IndexesCount() const = 0;
+    virtual bool HasOddLengthCycles() const = 0;
+
+    virtual std::string ToString(uint64_t index) = 0;
+
+    virtual uint64_t Parse(std::string state) = 0;
+
+    virtual void Expand(std::vector<uint64_t>& indexes, std::vector<int>& usedOperatorBits,
+                        std::vector<uint64_t>& expandedIndexes, std::vector<int>& expandedOperators,
+                        ExpandHint hint) = 0;
+
+    // Only the reference's segmented disk drivers call this; a no-op by default.
+    virtual void CrossSegmentPostProcess(int op, int segment, int segmentBits, Buffer<uint32_t>& expandedIndexes) {
+        (void)op, (void)segment, (void)segmentBits, (void)expandedIndexes;
+    }
+
+    // This library's handle when the puzzle is one of its device classes;
+    // NULL for puzzles defined elsewhere (the searches reject those).
+    virtual const psb_puzzle* handle() const { return nullptr; }
+
+protected:
+    // Common/Puzzle.cpp:15-26: room for a full batch's children, then empty.
+    virtual void SetupOutputBuffers(std::vector<uint64_t>& expandedIndexes, std::vector<int>& expandedOperators) {
+        const size_t capacity = MAX_INDEXES_BUFFER * size_t(BranchingFactor());
+        if (expandedIndexes.capacity() < capacity) expandedIndexes.reserve(capacity);
+        if (expandedOperators.capacity() < capacity) expandedOperators.reserve(capacity);
+        expandedIndexes.clear();
+        expandedOperators.clear();
+    }
+};
+
+// The library's puzzles: every method goes through the C ABI, Expand runs the
+// device expander, and the searches run on the GPU.
+class DevicePuzzle : public Puzzle {
+public:
+    DevicePuzzle(const DevicePuzzle&) = delete;
+    DevicePuzzle& operator=(const DevicePuzzle&) = delete;
+    ~DevicePuzzle() override { psb_puzzle_destroy(h_); }
+
+    std::string Name() const override {
         char buf[256];
         check(psb_puzzle_name(h_, buf, sizeof buf));
         return buf;
     }
-    int OperatorsCount() const { return ops_; }
-    int BranchingFactor() const { return branching_; }
-    uint64_t IndexesCount() const { return n_; }
-    bool HasOddLengthCycles() const { return odd_ != 0; }
+    int OperatorsCount() const override { return ops_; }
+    int BranchingFactor() const override { return branching_; }
+    uint64_t IndexesCount() const override { return n_; }
+    bool HasOddLengthCycles() const override { return odd_ != 0; }
 
-    std::string ToString(uint64_t index) {
+    std::string ToString(uint64_t index) override {
         char buf[512];
         check(psb_to_string(h_, index, buf, sizeof buf));
         return buf;
     }
 
-    uint64_t Parse(std::string state) {
+    uint64_t Parse(std::string state) override {
         uint64_t idx = 0;
         check(psb_parse(h_, state.c_str(), &idx));
         return idx;
@@ -88,7 +173,8 @@ public:
     // first.  The hint only matters to the reference's segmented disk
     // drivers, which this library does not provide.
     void Expand(std::vector<uint64_t>& indexes, std::vector<int>& usedOperatorBits,
-                std::vector<uint64_t>& expandedIndexes, std::vector<int>& expandedOperators, ExpandHint hint = {}) {
+                std::vector<uint64_t>& expandedIndexes, std::vector<int>& expandedOperators,
+                ExpandHint hint = {}) override {
         (void)hint;
         const size_t n = indexes.size();
         if (!usedOperatorBits.empty() && usedOperatorBits.size() != n)
@@ -105,10 +191,10 @@ public:
         expandedOperators.assign(ops.begin(), ops.begin() + n_out);
     }
 
-    const psb_puzzle* handle() const { return h_; }
+    const psb_puzzle* handle() const override { return h_; }
 
 protected:
-    Puzzle(int kind, int a, int b) {
+    DevicePuzzle(int kind, int a, int b) {
         check(psb_puzzle_create(kind, a, b, &h_));
         check(psb_puzzle_info(h_, &n_, &ops_, &branching_, &odd_));
     }
@@ -119,24 +205,57 @@ private:
     int ops_ = 0, branching_ = 0, odd_ = 0;
 };
 
-class SlidingTilePuzzleSimple : public Puzzle {
+class SlidingTilePuzzleSimple : public DevicePuzzle {
 public:
-    SlidingTilePuzzleSimple(int width, int height) : Puzzle(PSB_SLIDING, width, height) {}
+    SlidingTilePuzzleSimple(int width, int height) : DevicePuzzle(PSB_SLIDING, width, height) {}
 };
 
-class PancakeSimple : public Puzzle {
+// The reference's GPU sliding-tile class: the same n! index space as the
+// Simple class.
+class SlidingTilePuzzleGpu : public DevicePuzzle {
 public:
-    explicit PancakeSimple(int size) : Puzzle(PSB_PANCAKE, size, 0) {}
+    SlidingTilePuzzleGpu(int width, int height)
+        : DevicePuzzle(PSB_SLIDING, width, height), width_(width), height_(height) {}
+    std::string Name() const override {
+        return "Sliding-Tile GPU: " + std::to_string(width_) + " x " + std::to_string(height_);
+    }
+
+private:
+    int width_, height_;
 };
 
-class FourPegHanoiSimple : public Puzzle {
+class PancakeSimple : public DevicePuzzle {
+public:
+    explicit PancakeSimple(int size) : DevicePuzzle(PSB_PANCAKE, size, 0) {}
+};
+
+class FourPegHanoiSimple : public DevicePuzzle {
 public:
     explicit FourPegHanoiSimple(int size, bool useSymmetry = false)
-        : Puzzle(PSB_HANOI4, size, useSymmetry ? 1 : 0), size_(size), sym_(useSymmetry) {}
+        : DevicePuzzle(PSB_HANOI4, size, useSymmetry ? 1 : 0), size_(size), sym_(useSymmetry) {}
     int Size() const { return size_; }
     bool UseSymmetry() const { return sym_; }
 
 private:
+    int size_;
+    bool sym_;
+};
+
+// The reference's GPU Hanoi class: the Simple class's 4^n index space, at
+// most 24 disks (Puzzles/FourPegHanoiGPU.h:10-14).
+class FourPegHanoiGPU : public DevicePuzzle {
+public:
+    FourPegHanoiGPU(int size, bool useSymmetry)
+        : DevicePuzzle(PSB_HANOI4, checked_size(size), useSymmetry ? 1 : 0), size_(size), sym_(useSymmetry) {}
+    std::string Name() const override {
+        return "Four-Peg Hanoi Towers (GPU), size=" + std::to_string(size_) + "; symmetry=" + std::to_string(int(sym_));
+    }
+
+private:
+    static int checked_size(int size) {
+        if (size > 24) throw Error(PSB_ERR_ARG, "psb200: FourPegHanoiGPU holds at most 24 disks");
+        return size;
+    }
     int size_;
     bool sym_;
 };
@@ -166,10 +285,28 @@ public:
         SetExpandHint(0, false);
     }
 
+    // Expand batches, parents and time over all buffers (Common/Puzzle.cpp:7-13).
+    static void PrintStats() {
+        std::cerr << "Expand: " << stats().times.load() << " times, " << stats().nodes.load() << " nodes in "
+                  << stats().nanos.load() / 1000000 << " ms" << std::endl;
+    }
+
 private:
+    struct Stats {
+        std::atomic<uint64_t> nodes{0}, nanos{0}, times{0};
+    };
+    static Stats& stats() {
+        static Stats s;
+        return s;
+    }
     template <typename F>
     void Expand(F func) {
+        const auto t0 = std::chrono::steady_clock::now();
         puzzle_.Expand(indexes_, ops_, children_, child_ops_, hint_);
+        stats().times++;
+        stats().nodes += indexes_.size();
+        stats().nanos += uint64_t(
+            std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
         for (size_t i = 0; i < children_.size(); i++)
             if (children_[i] != Puzzle::INVALID_INDEX) func(children_[i], child_ops_[i]);
         indexes_.clear();
@@ -186,6 +323,9 @@ private:
 // number of states at each depth, element 0 = 1 (the initial state).
 inline std::vector<uint64_t> RunInMemory(Puzzle& puzzle, int algo, const std::string& initialState,
                                          const psb_bfs_opts* opts = nullptr, psb_bfs_stats* stats = nullptr) {
+    if (!puzzle.handle())
+        throw Error(PSB_ERR_UNSUPPORTED, "psb200: the in-memory searches run on the GPU for this library's puzzle "
+                                         "classes only; '" + puzzle.Name() + "' has no device expander");
     const uint64_t init = puzzle.Parse(initialState);
     std::vector<uint64_t> counts(1 << 16);
     uint32_t n = 0;
@@ -210,8 +350,10 @@ inline std::vector<uint64_t> InMemoryFrontierSearch(Puzzle& puzzle, std::string 
 }  // namespace psb200
 
 #ifdef PSB200_GLOBAL_NAMES
+using psb200::Buffer;
 using psb200::ExpandBuffer;
 using psb200::ExpandHint;
+using psb200::FourPegHanoiGPU;
 using psb200::FourPegHanoiSimple;
 using psb200::InMemoryClassicBFS;
 using psb200::InMemoryFrontierSearch;
@@ -219,5 +361,6 @@ using psb200::InMemoryThreeBitBFS;
 using psb200::InMemoryTwoBitBFS;
 using psb200::PancakeSimple;
 using psb200::Puzzle;
+using psb200::SlidingTilePuzzleGpu;
 using psb200::SlidingTilePuzzleSimple;
 #endif

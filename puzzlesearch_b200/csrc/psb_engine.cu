@@ -520,6 +520,10 @@ int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial, uint
     const uint64_t code_words = two_bit_words(p->n_states);
     const uint64_t flag_words = flag_words_for(p->n_states);
     const uint64_t words = instance_words(p->n_states);
+    if (words > e->pool_words)  // can never fit, however much space is freed
+        return psb_set_error(PSB_ERR_NOMEM, ("search needs " + std::to_string(words * 8) +
+                                             " bytes; the engine pool holds " + std::to_string(e->pool_words * 8))
+                                                .c_str());
     uint64_t off = 0;
     if (int rc = alloc_space(e, words, &off)) return rc;
     const uint32_t s = e->free_slots.back();

@@ -194,6 +194,62 @@ __global__ void __launch_bounds__(kThreads) retire_two_bit(ulonglong2* __restric
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
 }
 
+// Two-bit level end when the level's long-range marks went to the far
+// bitmap (LevelArgs::far): a state whose far bit is set becomes NEXT if its
+// code is UNVISITED (the `array.Get(child) == UNVISITED` test of
+// InMemoryTwoBitBFS.cpp:44-49, applied once per state after the level instead
+// of once per child), the bitmap is cleared for the next level, and the
+// states that become NEXT are counted into `count` (the next frontier's
+// size).  Far word j (32 states) pairs with code word j.  Each thread takes
+// four far words and their four code words; `next_lo` is the low bit of the
+// NEXT code (NEXT = 3: both bits, NEXT = 2: the high bit only).
+__device__ __forceinline__ uint32_t fold_word(unsigned long long& w, uint32_t f, uint32_t next_lo) {
+    if (!f) return 0;
+    const uint64_t unvisited = ~(w | (w >> 1)) & kEven;
+    const uint64_t m = spread_even(f) & unvisited;
+    w |= m | (next_lo ? (m << 1) : 0);
+    return uint32_t(__popcll(m));
+}
+__device__ __forceinline__ uint32_t fold_quad(ulonglong2* __restrict__ codes, uint4* __restrict__ far, uint64_t i,
+                                              uint32_t next_lo) {
+    const uint4 f = far[i];
+    if (!(f.x | f.y | f.z | f.w)) return 0;
+    ulonglong2 c0 = codes[2 * i], c1 = codes[2 * i + 1];
+    uint32_t c = fold_word(c0.x, f.x, next_lo) + fold_word(c0.y, f.y, next_lo) + fold_word(c1.x, f.z, next_lo) +
+                 fold_word(c1.y, f.w, next_lo);
+    codes[2 * i] = c0;
+    codes[2 * i + 1] = c1;
+    far[i] = make_uint4(0, 0, 0, 0);
+    return c;
+}
+__global__ void __launch_bounds__(kThreads) fold_two_bit(ulonglong2* __restrict__ codes, uint4* __restrict__ far,
+                                                        uint64_t n4, uint32_t next_lo,
+                                                        unsigned long long* count) {
+    uint32_t c = 0;
+    for (uint64_t i = blockIdx.x * uint64_t(kThreads) + threadIdx.x; i < n4; i += uint64_t(gridDim.x) * kThreads)
+        c += fold_quad(codes, far, i, next_lo);
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+// The same over the windows flagged this level only (a sparse level flags
+// every window it marks, far marks included); `quads` far quads per window.
+__global__ void __launch_bounds__(kThreads) fold_two_bit_flagged(ulonglong2* __restrict__ codes,
+                                                                uint4* __restrict__ far, uint64_t n4,
+                                                                const uint8_t* __restrict__ flags,
+                                                                uint64_t n_windows, uint32_t quads,
+                                                                uint32_t next_lo, unsigned long long* count) {
+    uint32_t c = 0;
+    for (uint64_t w = blockIdx.x; w < n_windows; w += gridDim.x) {
+        if (!flags[w]) continue;
+        for (uint32_t j = threadIdx.x; j < quads; j += kThreads) {
+            const uint64_t i = w * quads + j;
+            if (i < n4) c += fold_quad(codes, far, i, next_lo);
+        }
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
 }  // namespace psb
 
 namespace {
@@ -684,6 +740,8 @@ struct psb_bfs_session {
     uint64_t words[4] = {0, 0, 0, 0};  // padded sizes
     int n_arr = 0;
     uint64_t* visited = nullptr;  // three-bit searches that may run bottom-up: states at depth <= current
+    uint32_t* far = nullptr;      // two-bit: long-range mark bitmap (1 bit per state), folded after each level
+    uint64_t far_words = 0;       // its size in 64-bit words (padded)
     bool bottom_up = false;       // this search's algorithm and puzzle support bottom-up levels
     unsigned long long* d_stats = nullptr;
     unsigned long long* h_stats = nullptr;
@@ -703,6 +761,7 @@ struct psb_bfs_session {
     ~psb_bfs_session() {
         for (auto* a : arr) if (a) cudaFreeAsync(a, stream);
         if (visited) cudaFreeAsync(visited, stream);
+        if (far) cudaFreeAsync(far, stream);
         if (d_stats) cudaFreeAsync(d_stats, stream);
         for (auto* f : wflags) if (f) cudaFreeAsync(f, stream);
         if (spill) spill_return(spill);
@@ -951,6 +1010,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     if (S->device >= 0) PSB_CUDA(cudaSetDevice(S->device));
     for (int i = 0; i < S->n_arr; i++) PSB_CUDA(cudaMemsetAsync(S->arr[i], 0, S->words[i] * 8, s));
     if (S->visited) PSB_CUDA(cudaMemsetAsync(S->visited, 0, S->words[0] * 8, s));
+    if (S->far) PSB_CUDA(cudaMemsetAsync(S->far, 0, S->far_words * 8, s));
     PSB_CUDA(cudaEventRecord(S->ev[0], s));
     const int direction = opts ? opts->direction : PSB_DIR_AUTO;
     const double bu_ratio = (opts && opts->bottom_up_ratio > 0) ? double(opts->bottom_up_ratio) : kBottomUpRatio;
@@ -1082,13 +1142,17 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             switch (S->algo) {
             case PSB_THREE_BIT: a.front = cur; a.marks = nw; a.front_words = W1; a.mark_words = W1; break;
             case PSB_CLASSIC: a.front = open; a.marks = nopen; a.front_words = W1; a.mark_words = W1; break;
-            case PSB_TWO_BIT: a.front = codes; a.marks = codes; a.front_words = W2; a.mark_words = W2; a.cur_code = cur_code; break;
+            case PSB_TWO_BIT:
+                a.front = codes; a.marks = codes; a.front_words = W2; a.mark_words = W2; a.cur_code = cur_code;
+                a.far = S->far;
+                break;
             case PSB_FRONTIER:
                 a.front = fcur; a.marks = fnext; a.excl_cur = cex; a.excl_next = nex;
                 a.front_words = W4; a.mark_words = W4;
                 break;
             }
             PSB_CUDA(P.k.level[S->mode](a, grid, smem, s));
+            a.far = nullptr;
             launches++;
         }
         PSB_CUDA(cudaEventRecord(S->ev[2], s));
@@ -1127,6 +1191,18 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         } else if (S->algo == PSB_TWO_BIT && bu) {
             psb::retire_two_bit<<<148 * 8, psb::kThreads, 0, s>>>(reinterpret_cast<ulonglong2*>(codes), (W2 + 1) / 2,
                                                                  cur_code, S->d_stats + 4);
+            PSB_CUDA(cudaGetLastError());
+        } else if (S->algo == PSB_TWO_BIT && S->far) {
+            const uint64_t n4 = (W2 + 3) / 4;
+            const uint32_t next_lo = cur_code == 2 ? 1u : 0u;  // NEXT = 5 - CUR
+            if (produce)
+                psb::fold_two_bit_flagged<<<148 * 8, psb::kThreads, 0, s>>>(
+                    reinterpret_cast<ulonglong2*>(codes), reinterpret_cast<uint4*>(S->far), n4, S->wflags[flags_next],
+                    S->n_windows, uint32_t((uint64_t(1) << S->window_bits) / 128), next_lo, S->d_stats + 5);
+            else
+                psb::fold_two_bit<<<148 * 8, psb::kThreads, 0, s>>>(reinterpret_cast<ulonglong2*>(codes),
+                                                                   reinterpret_cast<uint4*>(S->far), n4, next_lo,
+                                                                   S->d_stats + 5);
             PSB_CUDA(cudaGetLastError());
         }
         PSB_CUDA(cudaEventRecord(S->ev[3], s));
@@ -1263,6 +1339,7 @@ int psb_bfs_footprint(const psb_puzzle* p, int algo, uint64_t* bytes) {
     if (int rc = layout(p, algo, w, &n)) return rc;
     *bytes = (w[0] + w[1] + w[2] + w[3]) * 8 + 64;
     if (algo == PSB_THREE_BIT && supports_bottom_up(p, algo)) *bytes += w[0] * 8;  // visited array
+    if (algo == PSB_TWO_BIT) *bytes += padded(words_for(p->n_states)) * 8;           // far bitmap
     return PSB_OK;
 }
 
@@ -1301,6 +1378,19 @@ int psb_bfs_session_create(const psb_puzzle* p, int algo, const psb_bfs_opts* op
             S->bytes += S->words[0] * 8;
         } else {
             cudaGetLastError();  // an allocation failure is not sticky; clear it
+        }
+    }
+    if (algo == PSB_TWO_BIT) {
+        // Optional as well: without room for the far bitmap every long-range
+        // mark reads the target's code first.
+        void* v = nullptr;
+        const uint64_t fw = padded(words_for(p->n_states));
+        if (cudaMallocFromPoolAsync(&v, fw * 8, S->pool, S->stream) == cudaSuccess) {
+            S->far = static_cast<uint32_t*>(v);
+            S->far_words = fw;
+            S->bytes += fw * 8;
+        } else {
+            cudaGetLastError();
         }
     }
     S->n_windows = (p->n_states + (uint64_t(1) << S->window_bits) - 1) >> S->window_bits;

@@ -165,6 +165,7 @@ struct LevelArgs {
     const uint8_t* wflag_cur;   // optional: 1 byte per window, non-zero if the window may hold frontier states
     uint8_t* wflag_next;        // optional: set for every window that receives a mark this level
     const uint64_t* probe;      // bottom-up levels: the frontier array the unvisited states probe
+    uint32_t* far;              // two-bit top-down, optional: 1 bit per state for long-range marks (see Emitter)
 };
 
 constexpr uint64_t kEven = 0x5555555555555555ull;
@@ -360,6 +361,7 @@ struct Emitter {
     uint32_t next_pat;    // two-bit: bits of the NEXT code (hi at bit 0, lo at bit 1)
     uint8_t* wflag_next;  // optional active-window flags of the next level
     int window_bits;
+    uint32_t* farbits;    // two-bit: long-range mark bitmap (NULL: read the target's code, then mark it)
     uint32_t children = 0, local = 0, bad = 0;
     uint32_t marked = 0;      // two-bit: long-range UNVISITED -> NEXT marks issued (two lanes may mark one state)
     uint32_t parent_off = 0;  // offset of the parent being expanded in the window (rel)
@@ -392,6 +394,15 @@ struct Emitter {
             flag_window(c);
             atomicOr(reinterpret_cast<unsigned int*>(gmarks) + (c >> 3), 1u << (4 * (uint32_t(c) & 7u) + op));
         } else if constexpr (MODE == kTwoBit) {
+            if (farbits) {
+                // Fire-and-forget: set the child's bit in the long-range
+                // bitmap; fold_two_bit turns the UNVISITED ones into NEXT
+                // after the level.  No dependent read of the target's code.
+                flag_window(c);
+                if constexpr (kFar) red_or_far(farbits + (c >> 5), 1u << (uint32_t(c) & 31u));
+                else atomicOr(farbits + (c >> 5), 1u << (uint32_t(c) & 31u));
+                return;
+            }
             unsigned long long* w = reinterpret_cast<unsigned long long*>(gmarks) + (c >> 5);
             const uint32_t sh = 2u * (uint32_t(c) & 31u);
             const uint64_t v = kFar ? ld_cg_far(w) : __ldcg(reinterpret_cast<const unsigned long long*>(w));
@@ -535,7 +546,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     __syncthreads();
 
     Emitter<MODE> em{base, span, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u), a.wflag_next,
-                     a.window_bits};
+                     a.window_bits, MODE == kTwoBit ? a.far : nullptr};
     uint32_t found = 0;
     // ORs a mask of unit x's states into the window's shared marks.
     auto mark_unit = [&](uint32_t x, uint64_t m) {
@@ -901,7 +912,7 @@ __global__ void __launch_bounds__(Shape<MODE, BU>::threads, Shape<MODE, BU>::min
 template <class PZ>
 __global__ void seed_kernel(LevelArgs a, uint64_t initial) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Emitter<kFrontier> em{~uint64_t(0), 0, nullptr, a.marks, a.n_states, 0, a.wflag_next, a.window_bits};
+    Emitter<kFrontier> em{~uint64_t(0), 0, nullptr, a.marks, a.n_states, 0, a.wflag_next, a.window_bits, nullptr};
     PZ::template expand<true>(initial, 0u, a.pz, em);
     if (a.odd) a.excl_next[initial >> 6] |= 1ull << (initial & 63);
     a.stats[1] += em.children;

@@ -3,13 +3,18 @@
 //
 // Clients submit solve requests (puzzle, start state) from any thread without
 // blocking.  One server thread owns a psb_engine and loops:
-//   1. admit queued requests, first come first served, while an instance
-//      slot and pool space for the request's two-bit array are free
-//      (admission by HBM footprint: 2 bits x states, padded);
+//   1. admit queued requests while an instance slot and pool space for the
+//      request's two-bit array are free (admission by HBM footprint: 2 bits x
+//      states, padded).  The smallest requests go first; a request that does
+//      not fit now waits without holding back the others, until it has been
+//      passed over kMaxBypass times: then nothing else is admitted until it
+//      fits, which the running searches guarantee as they finish.  A request
+//      larger than the whole pool completes at once with PSB_ERR_NOMEM;
 //   2. advance every resident search by one BFS level (psb_engine_step), so
 //      requests that arrive while others are running overlap on the GPU;
 //   3. collect finished searches: per-depth counts, eccentricity (the last
 //      depth) and latency from submission to completion.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -32,7 +37,12 @@ struct Request {
     int kind, a, b;
     uint64_t initial;
     Clock::time_point submitted;
+    uint64_t footprint;   // engine pool bytes (0 if the puzzle is invalid: admission reports why)
+    uint32_t bypassed;    // times a later request was admitted while this one did not fit
 };
+
+// A request passed over this many times stops later admissions until it fits.
+constexpr uint32_t kMaxBypass = 64;
 
 struct Done {
     uint64_t ticket;
@@ -61,6 +71,46 @@ struct psb_server {
 
 namespace {
 
+// Admits queued requests, smallest footprint first (ties: oldest first), while
+// the engine has a slot and pool space.  Called with s->mu held.
+void admit_queued(psb_server* s) {
+    std::vector<size_t> order(s->queue.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t x, size_t y) { return s->queue[x].footprint < s->queue[y].footprint; });
+    // The oldest request that has been passed over too often goes first, alone.
+    for (size_t i = 0; i < s->queue.size(); i++) {
+        if (s->queue[i].bypassed >= kMaxBypass) {
+            order.assign(1, i);
+            break;
+        }
+    }
+    std::vector<bool> gone(s->queue.size(), false);
+    std::vector<size_t> waiting;  // did not fit this time
+    for (size_t i : order) {
+        Request& r = s->queue[i];
+        uint32_t slot = 0;
+        const int rc = psb_engine_add(s->engine, r.kind, r.a, r.b, r.initial, r.ticket, &slot);
+        if (rc == PSB_ERR_CAPACITY) {  // no slot or pool space now: wait for running searches to finish
+            waiting.push_back(i);
+            continue;
+        }
+        gone[i] = true;
+        if (rc != PSB_OK) {  // unsupported puzzle, bad start, larger than the pool: report at once
+            s->done.push_back(Done{r.ticket, rc, {}, 0.0});
+            continue;
+        }
+        s->running.emplace(r.ticket, r);
+        s->admitted++;
+        for (size_t w : waiting)  // admitted ahead of requests that were submitted earlier
+            if (s->queue[w].ticket < r.ticket) s->queue[w].bypassed++;
+    }
+    std::deque<Request> rest;
+    for (size_t i = 0; i < s->queue.size(); i++)
+        if (!gone[i]) rest.push_back(s->queue[i]);
+    s->queue.swap(rest);
+}
+
 void serve(psb_server* s) {
     std::vector<uint64_t> tags(1024), counts;
     std::vector<uint32_t> nd(1024);
@@ -72,20 +122,12 @@ void serve(psb_server* s) {
             if (s->running.empty())
                 s->cv.wait(lock, [&] { return s->stop.load() || !s->queue.empty(); });
             if (s->stop.load()) return;
-            // FIFO admission while the engine has room.
-            while (!s->queue.empty()) {
-                const Request& r = s->queue.front();
-                uint32_t slot = 0;
-                const int rc = psb_engine_add(s->engine, r.kind, r.a, r.b, r.initial, r.ticket, &slot);
-                if (rc == PSB_ERR_CAPACITY) break;  // wait for a slot or pool space to free up
-                if (rc != PSB_OK) {                 // unsupported puzzle or bad start: report, drop
-                    s->done.push_back(Done{r.ticket, rc, {}, 0.0});
-                    s->queue.pop_front();
-                    continue;
-                }
-                s->running.emplace(r.ticket, r);
-                s->admitted++;
-                s->queue.pop_front();
+            admit_queued(s);
+            if (s->running.empty() && !s->queue.empty()) {
+                // Nothing runs and nothing was admitted: only possible while the
+                // engine is still releasing space.  Wait briefly instead of spinning.
+                s->cv.wait_for(lock, std::chrono::milliseconds(1));
+                continue;
             }
         }
         if (!s->running.empty()) {
@@ -140,7 +182,9 @@ int psb_server_start(const psb_server_opts* opts, psb_server** out) {
 
 int psb_server_submit(psb_server* s, int kind, int a, int b, uint64_t initial, uint64_t* ticket) {
     if (!s || !ticket) return psb_set_error(PSB_ERR_ARG, "bad argument");
-    Request r{s->next_ticket.fetch_add(1), kind, a, b, initial, Clock::now()};
+    uint64_t footprint = 0;
+    if (psb_engine_footprint(kind, a, b, &footprint) != PSB_OK) footprint = 0;
+    Request r{s->next_ticket.fetch_add(1), kind, a, b, initial, Clock::now(), footprint, 0};
     {
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->stop.load()) return psb_set_error(s->fatal ? s->fatal : PSB_ERR_ARG, "server stopped");

@@ -1,10 +1,16 @@
 // psb200_driver.cpp -- exercises include/psb200.hpp the way the reference's
 // tests use its classes (PuzzlesTests/PuzzleSearchTests.cpp, PancakeTest.cpp,
 // FourPegHanoiTest.cpp).  Reads commands on stdin, one per line:
-//   bfs <sliding|pancake|hanoi4> <a> <b> <classic|two_bit|three_bit|frontier> <state...>
-//   expand <sliding|pancake|hanoi4> <a> <b> <state...>
-// and prints one result line per command (space-separated counts, or
-// "child-state|op" items separated by ';').  tests/test_gpu_cpp_adapter.py
+//   bfs <kind> <a> <b> <classic|two_bit|three_bit|frontier> <state...>
+//   expand <kind> <a> <b> <state...>
+//   custom <n>
+// with kind one of sliding, sliding_gpu, pancake, hanoi4, hanoi4_gpu (the
+// *_gpu kinds construct the reference's GPU class names,
+// SlidingTilePuzzleGpu and FourPegHanoiGPU), and prints one result line per
+// command (space-separated counts, or "child-state|op" items separated by
+// ';').  `custom` drives a Puzzle subclass defined here, as a caller would:
+// it prints the number of children ExpandBuffer delivers over all n states,
+// then what InMemoryTwoBitBFS does with it.  tests/test_gpu_cpp_adapter.py
 // feeds it the reference's golden vectors.
 #define PSB200_GLOBAL_NAMES
 #include "../../include/psb200.hpp"
@@ -16,9 +22,35 @@
 
 static std::unique_ptr<Puzzle> make(const std::string& kind, int a, int b) {
     if (kind == "sliding") return std::make_unique<SlidingTilePuzzleSimple>(a, b);
+    if (kind == "sliding_gpu") return std::make_unique<SlidingTilePuzzleGpu>(a, b);
     if (kind == "pancake") return std::make_unique<PancakeSimple>(a);
+    if (kind == "hanoi4_gpu") return std::make_unique<FourPegHanoiGPU>(a, b != 0);
     return std::make_unique<FourPegHanoiSimple>(a, b != 0);
 }
+
+// A caller's own puzzle: n states on a ring, two moves each (i-1 and i+1).
+class RingPuzzle : public Puzzle {
+public:
+    explicit RingPuzzle(uint64_t n) : n_(n) {}
+    std::string Name() const override { return "ring of " + std::to_string(n_); }
+    int OperatorsCount() const override { return 2; }
+    int BranchingFactor() const override { return 2; }
+    uint64_t IndexesCount() const override { return n_; }
+    bool HasOddLengthCycles() const override { return n_ % 2 == 1; }
+    std::string ToString(uint64_t index) override { return std::to_string(index); }
+    uint64_t Parse(std::string state) override { return std::stoull(state); }
+    void Expand(std::vector<uint64_t>& indexes, std::vector<int>& usedOperatorBits,
+                std::vector<uint64_t>& expandedIndexes, std::vector<int>& expandedOperators, ExpandHint) override {
+        SetupOutputBuffers(expandedIndexes, expandedOperators);
+        for (size_t i = 0; i < indexes.size(); i++) {
+            if (!(usedOperatorBits[i] & 1)) { expandedIndexes.push_back((indexes[i] + n_ - 1) % n_); expandedOperators.push_back(1); }
+            if (!(usedOperatorBits[i] & 2)) { expandedIndexes.push_back((indexes[i] + 1) % n_); expandedOperators.push_back(0); }
+        }
+    }
+
+private:
+    uint64_t n_;
+};
 
 int main() {
     std::string line;
@@ -26,7 +58,27 @@ int main() {
         std::istringstream in(line);
         std::string cmd, kind;
         int a = 0, b = 0;
-        in >> cmd >> kind >> a >> b;
+        in >> cmd;
+        if (cmd == "custom") {
+            uint64_t n = 0;
+            in >> n;
+            RingPuzzle ring(n);
+            uint64_t children = 0;
+            ExpandBuffer nodes(ring);
+            auto count = [&](uint64_t, int) { children++; };
+            for (uint64_t i = 0; i < n; i++) nodes.Add(i, 0, count);
+            nodes.Finish(count);
+            std::cout << children;
+            try {
+                InMemoryTwoBitBFS(ring, "0");
+                std::cout << " searched\n";
+            } catch (const psb200::Error& e) {
+                std::cout << " ERROR " << e.code() << " " << e.what() << "\n";
+            }
+            std::cout.flush();
+            continue;
+        }
+        in >> kind >> a >> b;
         try {
             auto puzzle = make(kind, a, b);
             if (cmd == "bfs") {

@@ -160,6 +160,25 @@ def test_stats_are_consistent():
     assert st["levels"] == len(r["counts"])
 
 
+@pytest.mark.parametrize("spec,algo", [(["hanoi4", 8, 0], "two_bit"), (["hanoi4", 9, 0], "three_bit"),
+                                       (["hanoi4", 10, 0], "two_bit"), (["sliding", 3, 3], "two_bit"),
+                                       (["sliding", 3, 3], "three_bit"), (["pancake", 9, 0], "two_bit")])
+def test_children_stat_equals_oracle_expand(spec, algo):
+    """A top-down search expands every reached state once, so its children
+    statistic equals the oracle's Expand count over all reached states
+    (4-peg Hanoi: 6*4^n - 6*2^n, since no move joins two empty pegs)."""
+    p = {"pancake": lambda: psb.PancakeSimple(spec[1]), "sliding": lambda: psb.SlidingTilePuzzleSimple(*spec[1:]),
+         "hanoi4": lambda: psb.FourPegHanoiSimple(spec[1], bool(spec[2]))}[spec[0]]()
+    r = psb.bfs(p, algo, 0, levels=True, direction="top_down")
+    dist, _ = O.depths(spec, 0)
+    reached = [i for i in range(len(dist)) if dist[i] != 255]
+    want = sum(len(O.expand(spec, reached[k:k + 4096])[0]) for k in range(0, len(reached), 4096))
+    assert r["stats"]["children"] == want
+    assert sum(r["level_children"]) == want
+    if spec[0] == "hanoi4":
+        assert want == 6 * 4 ** spec[1] - 6 * 2 ** spec[1]
+
+
 def test_trivial_puzzles():
     assert psb.bfs(psb.PancakeSimple(2), "three_bit", 0)["counts"] == [1, 1]
     assert psb.bfs(psb.FourPegHanoiSimple(1), "two_bit", 0)["counts"] == [1, 3]

@@ -65,3 +65,41 @@ def test_expand_known_answers_through_adapter(golden):
 def test_error_path_through_adapter():
     got = run(["bfs pancake 6 0 frontier"])
     assert got[0].startswith("ERROR -5")
+
+
+@pytest.mark.gpu
+def test_reference_gpu_class_bodies_through_adapter(golden):
+    """The reference's GPU test bodies (PuzzlesTests/PuzzleSearchTests.cpp:85-131)
+    construct SlidingTilePuzzleGpu(w, h) and run every in-memory search on it;
+    FourPegHanoiGPU(n, symmetry) takes the Simple class's index space as well.
+    Through the adapter they give the reference's golden vectors."""
+    cases = []
+    for v in golden["search"]:
+        kind, a, b = v["puzzle"]
+        if not v["full"] or kind == "pancake" or (kind == "sliding" and a * b > 8):
+            continue
+        gpu_kind = {"sliding": "sliding_gpu", "hanoi4": "hanoi4_gpu"}[kind]
+        for algo in ("classic", "two_bit", "three_bit", "frontier"):
+            cases.append((f"bfs {gpu_kind} {a} {b} {algo} {v['start'] or ''}".rstrip(), v["counts"]))
+    assert len(cases) >= 12
+    got = run([c for c, _ in cases])
+    for (cmd, exp), line in zip(cases, got):
+        assert [int(x) for x in line.split()] == exp, cmd
+
+
+def test_caller_defined_puzzle():
+    """Puzzle is abstract as in the reference: a caller's own subclass runs
+    through ExpandBuffer (every state's two children delivered), and the
+    in-memory searches, which need a device expander, reject it with
+    PSB_ERR_UNSUPPORTED instead of running it on the host."""
+    line = run(["custom 5000"])[0]
+    children, rest = line.split(" ", 1)
+    assert int(children) == 10000
+    assert rest.startswith("ERROR -5")
+
+
+@pytest.mark.gpu
+def test_gpu_class_limits_and_names():
+    got = run(["bfs hanoi4_gpu 25 0 two_bit", "expand sliding_gpu 3 2 1 0 2 3 4 5"])
+    assert got[0].startswith("ERROR -1")
+    assert got[1] == run(["expand sliding 3 2 1 0 2 3 4 5"])[0]

@@ -87,3 +87,50 @@ def test_admission_waits_for_pool_space():
         time.sleep(0.005)
     srv.stop()
     assert [done[t][1] for t in tickets] == [psb.bfs(p, "two_bit", s)["counts"] for s in (0, 1, 2, 3)]
+
+
+def test_request_larger_than_the_pool_fails_at_once():
+    """A request whose footprint exceeds the whole pool completes at once with
+    PSB_ERR_NOMEM; the requests submitted before and after it all complete
+    with their correct counts, and the server stays responsive."""
+    small = psb.PancakeSimple(9)
+    big = psb.PancakeSimple(12)  # 120 MB of codes: never fits a 16 MB pool
+    foot = psb.Engine.footprint(small)
+    srv = psb.Server(max_instances=8, pool_bytes=16 << 20)
+    assert psb.Engine.footprint(big) > 16 << 20 > 2 * foot
+    before = [srv.submit(small, s) for s in (0, 5)]
+    bad = srv.submit(big, 0)
+    after = [srv.submit(small, s) for s in (7, 11, 13)]
+    done = {}
+    deadline = time.time() + 60
+    while len(done) < 6 and time.time() < deadline:
+        done.update(srv.poll())
+        time.sleep(0.005)
+    info = srv.info()
+    srv.stop()
+    assert len(done) == 6, info
+    assert done[bad][0] == -3
+    for t, s in zip(before + after, (0, 5, 7, 11, 13)):
+        assert done[t][0] == 0 and done[t][1] == psb.bfs(small, "two_bit", s)["counts"]
+
+
+def test_small_requests_pass_a_waiting_large_one():
+    """While a large request waits for pool space, smaller ones that fit are
+    admitted around it; the large one still completes once space frees up."""
+    small, large = psb.PancakeSimple(8), psb.PancakeSimple(10)
+    fl, fs = psb.Engine.footprint(large), psb.Engine.footprint(small)
+    srv = psb.Server(max_instances=16, pool_bytes=fl + 2 * fs + 4096)
+    first = srv.submit(large, 0)      # takes most of the pool
+    waiting = srv.submit(large, 1)    # must wait for the first to finish
+    smalls = [srv.submit(small, s) for s in range(6)]
+    done = {}
+    deadline = time.time() + 120
+    while len(done) < 8 and time.time() < deadline:
+        done.update(srv.poll())
+        time.sleep(0.002)
+    srv.stop()
+    assert len(done) == 8
+    assert done[first][1] == psb.bfs(large, "two_bit", 0)["counts"]
+    assert done[waiting][1] == psb.bfs(large, "two_bit", 1)["counts"]
+    for s, t in enumerate(smalls):
+        assert done[t][0] == 0 and done[t][1] == psb.bfs(small, "two_bit", s)["counts"]
