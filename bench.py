@@ -1,23 +1,28 @@
 #!/usr/bin/env python3
-"""Benchmark: full in-memory BFS of the 13-pancake puzzle (three-bit arrays) on B200.
+"""Benchmark: full in-memory BFS of the 14-pancake puzzle (two-bit codes,
+frontier spill) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-One step is one complete BFS from the identity (13! = 6,227,020,800 states,
-16 depths, three bit arrays of 778 MB each, resident in HBM).  The metric
-is BFS states per second: states reached divided by device time.
+One step is one complete BFS from the identity (14! = 87,178,291,200 states,
+17 depths, a 21.8 GB two-bit array resident in HBM), with every depth's
+frontier encoded on the GPU into the reference's compressed segment stream
+and handed over from pinned host memory (the large-instance configuration:
+14-pancake and 18-disk 4-peg Hanoi two-bit with frontier compression).  The
+metric is BFS states per second: states reached divided by device time.
 `value` times psb_bfs_session_run with the arrays already allocated.  `e2e`
-times the public C-ABI call psb_bfs, which allocates, runs and copies the
-per-depth counts back to the host.
+times the public C-ABI call psb_bfs, which allocates from the pool, runs,
+copies every spilled segment and the per-depth counts to the host.
 
 Multi-GPU: the path does not shard across GPUs inside one search (the
 reference has no multi-GPU path), so --gpus N runs N independent replicas,
 one process per GPU under torchrun.  value = total states / max-over-ranks time.
 
---impl reference times the reference's own CPU path: InMemoryThreeBitBFS
-built from its sources into oracle/_ref.  It runs on a bounded sample (the
-full 11-pancake search) so the run ends in minutes.  The single-threaded
-13-pancake search takes tens of minutes.
+--impl reference times the reference's own CPU path: InMemoryTwoBitBFS built
+from its sources into oracle/_ref.  The reference's in-memory search is
+single-threaded, so every step runs one search per host core at once, on a
+bounded sample (the full 10-pancake search) so the run ends in minutes; the
+single-threaded 14-pancake search takes many hours.
 """
 import argparse
 import ctypes
@@ -35,11 +40,11 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 WORKLOADS = {
-    # name: (kind, a, b, algo, description)
-    "pancake13-3bit": ("pancake", 13, 0, "three_bit", "13-pancake in-memory three-bit BFS, full solve from the identity"),
-    "sliding3x4-2bit": ("sliding", 3, 4, "two_bit", "3x4 sliding-tile in-memory two-bit BFS, full solve from the solved state"),
+    # name: (kind, a, b, algo, description); the two large instances spill every depth by default
     "pancake14-2bit": ("pancake", 14, 0, "two_bit", "14-pancake in-memory two-bit BFS, full solve from the identity"),
     "hanoi18-2bit": ("hanoi4", 18, 0, "two_bit", "18-disk 4-peg Hanoi in-memory two-bit BFS, full solve from all disks on peg 0"),
+    "pancake13-3bit": ("pancake", 13, 0, "three_bit", "13-pancake in-memory three-bit BFS, full solve from the identity"),
+    "sliding3x4-2bit": ("sliding", 3, 4, "two_bit", "3x4 sliding-tile in-memory two-bit BFS, full solve from the solved state"),
     # smaller cases of the same kernels, sized for ncu captures (arrays above L2, a few GB at most)
     "hanoi15-2bit": ("hanoi4", 15, 0, "two_bit", "15-disk 4-peg Hanoi in-memory two-bit BFS (profiling case)"),
     "pancake12-3bit": ("pancake", 12, 0, "three_bit", "12-pancake in-memory three-bit BFS (profiling case)"),
@@ -48,7 +53,9 @@ WORKLOADS = {
     "pancake12-classic": ("pancake", 12, 0, "classic", "12-pancake in-memory classic BFS, full solve from the identity"),
     "sliding4x3-frontier": ("sliding", 4, 3, "frontier", "4x3 sliding-tile in-memory frontier search, full solve"),
 }
-REF_SAMPLE = ("pancake", 11, 0, "three_bit")  # CPU baseline sample (reference InMemoryThreeBitBFS)
+SPILL_BY_DEFAULT = {"pancake14-2bit", "hanoi18-2bit"}
+REF_SAMPLE = ("pancake", 11, 0, "two_bit")      # cpu_baseline: one reference InMemoryTwoBitBFS, one core
+REF_ARM_SAMPLE = ("pancake", 10, 0, "two_bit")  # --impl reference: one search per host core per step
 
 
 def load_peaks():
@@ -115,16 +122,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def level_traffic(workload):
-    """DRAM bytes per level-kernel launch from the committed ncu launch list
-    (mean over one search's launches), or None for workloads without one."""
-    path = os.path.join(REPO, "profiles", f"level_kernel_{workload.replace('-', '_')}_launches.md")
-    if not os.path.exists(path):
-        return None
-    m = re.search(r"traffic bytes per level launch: (\d+)", open(path).read())
-    return int(m.group(1)) if m else None
-
-
 def dist_setup(n_gpus, backend="nccl"):
     """One process per GPU (torchrun): returns (rank, world, local_rank, torch.distributed or None)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -157,15 +154,19 @@ def job_rate(world, steps, units_per_step, seconds):
     return world * steps * units_per_step / seconds
 
 
-def cpu_reference_sample(sample=REF_SAMPLE):
-    """Runs the reference's InMemory BFS (oracle/_ref/psbref) on the sample; returns (states, seconds, kind)."""
+def _ref_cmd(sample):
     kind, a, b, algo = sample
     kinds = {"sliding": 1, "pancake": 2, "hanoi4": 3}
     algos = {"two_bit": 1, "three_bit": 2, "frontier": 3, "classic": 4}
-    exe = os.path.join(REPO, "oracle", "_ref", "psbref")
-    if os.path.exists(exe):
-        out = subprocess.run([exe, str(kinds[kind]), str(a), str(b), str(algos[algo])], capture_output=True,
-                             text=True, check=True).stdout
+    return [os.path.join(REPO, "oracle", "_ref", "psbref"), str(kinds[kind]), str(a), str(b), str(algos[algo])]
+
+
+def cpu_reference_sample(sample=REF_SAMPLE):
+    """Runs the reference's InMemory BFS (oracle/_ref/psbref) on the sample; returns (states, seconds, kind)."""
+    kind, a, b, algo = sample
+    cmd = _ref_cmd(sample)
+    if os.path.exists(cmd[0]):
+        out = subprocess.run(cmd, capture_output=True, text=True, check=True).stdout
         d = json.loads(out.strip().splitlines()[-1])
         return d["states"], d["seconds"], "reference"
     sys.path.insert(0, os.path.join(REPO, "oracle"))
@@ -175,27 +176,60 @@ def cpu_reference_sample(sample=REF_SAMPLE):
     return sum(counts), time.perf_counter() - t0, "port"
 
 
+def reference_step(procs, sample=REF_ARM_SAMPLE):
+    """One step of the reference arm: `procs` copies of the reference's
+    single-threaded search at once, one per host core.  Returns (states, wall seconds)."""
+    cmd = _ref_cmd(sample)
+    t0 = time.perf_counter()
+    running = [subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+               for _ in range(procs)]
+    states = 0
+    for p in running:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"reference search failed: {' '.join(cmd)}")
+        states += json.loads(out.strip().splitlines()[-1])["states"]
+    return states, time.perf_counter() - t0
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    kind, a, b, algo = REF_SAMPLE
+    kind, a, b, algo = REF_ARM_SAMPLE
+    wl = WORKLOADS[args.workload]
+    if not os.path.exists(_ref_cmd(REF_ARM_SAMPLE)[0]):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/psbref was not built (the reference's "
+                          "sources were absent when the repository was built)"}), flush=True)
+        return 0
+    procs = host_cores()
     for _ in range(args.warmup):
-        cpu_reference_sample()
-    secs, states, ck = 0.0, 0, "reference"
+        reference_step(procs)
+    secs, states = 0.0, 0
     for _ in range(args.steps):
-        s, t, ck = cpu_reference_sample()
+        s, t = reference_step(procs)
         states += s
         secs += t
     value = states / secs
-    wl = WORKLOADS[args.workload]
+    sample = (f"reference InMemoryTwoBitBFS on {a}-pancake (full search, {math.factorial(a):,} states), "
+              f"{procs} single-threaded searches at once, one per host core, per step")
     line = {
         "impl": "reference", "metric": f"BFS states/sec ({wl[4]})", "value": value, "unit": "states/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample": f"{a}-pancake full {algo} BFS ({math.factorial(a)} states)"},
-        "cpu_baseline": {"value": value, "unit": "states/s", "cores": 1, "kind": ck,
-                         "sample": f"reference InMemoryThreeBitBFS on {a}-pancake (full search, {math.factorial(a)} states), single-threaded as in the reference"},
+        "config": {"workload": args.workload, "sample": sample, "same_config": False,
+                   "why_not_same_config": "the reference's single-threaded in-memory search of the full workload "
+                                          "takes hours; the sample runs the same algorithm on a smaller instance of "
+                                          "the same puzzle, whose arrays fit the host caches (a faster rate per "
+                                          "state than the full instance would reach)"},
+        "cpu_baseline": {"value": value, "unit": "states/s", "cores": procs, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "states/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -396,7 +430,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pancake13-3bit", choices=sorted(WORKLOADS) + ["batch4096", "serve"])
+    ap.add_argument("--workload", default="pancake14-2bit", choices=sorted(WORKLOADS) + ["batch4096", "serve"])
     ap.add_argument("--window-bits", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--direction", default="auto", choices=["auto", "top_down", "bottom_up"],
@@ -405,7 +439,10 @@ def main():
                     help="auto: a level runs bottom-up when unvisited < ratio x frontier (0 = library default)")
     ap.add_argument("--spill", action="store_true",
                     help="encode every depth's frontier on the GPU (segment streams) and hand it over in pinned"
-                         " host memory during the timed searches")
+                         " host memory during the timed searches (default for pancake14-2bit and hanoi18-2bit)")
+    ap.add_argument("--no-spill", action="store_true", help="no frontier spill, whatever the workload")
+    ap.add_argument("--e2e-calls", type=int, default=5,
+                    help="timed calls of the public entry point for `e2e` (at most --steps)")
     ap.add_argument("--segment-bits", type=int, default=0, help="with --spill: 2^bits states per segment (0 = 32)")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the level window (single searches) or the engine's blocks per SM (batch4096) by"
@@ -420,6 +457,7 @@ def main():
     ap.add_argument("--max-requests", type=int, default=400, help="--workload serve: requests per rate at most")
     ap.add_argument("--pool-gb", type=int, default=32, help="--workload serve: engine pool (HBM admission limit)")
     args = ap.parse_args()
+    args.spill = (args.spill or args.workload in SPILL_BY_DEFAULT) and not args.no_spill
     if args.profile_once:
         return profile_once(args)
     if args.workload == "batch4096":
@@ -500,9 +538,10 @@ def main():
     value = job_rate(world, args.steps, states_per_step, elapsed_ms / 1000.0)
 
     # e2e: the public C-ABI entry point, host in/out, allocation included.
-    # Untimed warm-up calls first, as for the device loop: the first call
-    # grows the library's memory pool.
-    for _ in range(args.warmup):
+    # An untimed warm-up call first: the first call grows the library's
+    # memory pool.  Fewer calls than device steps keep the run short.
+    e2e_calls = max(1, min(args.steps, args.e2e_calls))
+    for _ in range(1):
         psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
                 spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits)
     torch.cuda.synchronize()
@@ -510,7 +549,7 @@ def main():
     t0 = time.perf_counter()
     levels = 0
     calls = []
-    for _ in range(args.steps):
+    for _ in range(e2e_calls):
         tc = time.perf_counter()
         r = psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
                     spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits)
@@ -519,7 +558,7 @@ def main():
         levels = r["stats"]["levels"]
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
-    e2e_value = job_rate(world, args.steps, states_per_step, e2e_s)
+    e2e_value = job_rate(world, e2e_calls, states_per_step, e2e_s)
 
     psb.lib().psb_bfs_session_destroy(h)
     if rank != 0:
@@ -541,7 +580,6 @@ def main():
     expand_ms = sum(s.expand_ms for s in stats) / len(stats)
     achieved = alg_bytes / (expand_ms / 1000.0) / 1e9
     peak, peak_kind = load_peaks()
-    traffic = level_traffic(args.workload) if args.direction == "auto" else None
     # level kernels + one finalize per level (three-bit, classic) or one
     # CUR -> OLD pass per bottom-up level (two-bit)
     launches_per_step = st.levels + (st.levels if algo in ("three_bit", "classic") else st.bottom_up_levels)
@@ -558,15 +596,16 @@ def main():
                    "index_space": N, "device_bytes": st.device_bytes, "window_bits": st.window_bits,
                    "l2": "inputs larger than L2 (bit arrays of %d MB resident in HBM)" % (st.device_bytes >> 20),
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
-        "e2e": {"value": e2e_value, "unit": "states/s", "h2d_bytes_per_step": 8,
+        "e2e": {"value": e2e_value, "unit": "states/s", "calls": e2e_calls, "h2d_bytes_per_step": 8,
                 "d2h_bytes_per_step": 64 * levels + 8 * len(ref_counts),
                 "call_s": [round(c, 4) for c in calls]},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
+                     "frac": achieved / peak, "traffic": None,
                      "note": f"level kernel (top-down and bottom-up launches), {peak_kind} peak; algorithmic bytes"
-                             " per level = N/8 sweep + 8 B per child generated or probe issued; traffic = ncu DRAM"
-                             " read+write bytes per level launch (profiles/level_kernel_pancake13_3bit_launches.md)"},
+                             f" per level = {'N/8' if algo != 'two_bit' else '2 x 2N/8'} sweep + 8 B per child"
+                             " generated or probe issued; traffic is not measured in this run (ncu is not run"
+                             " inside the bench)"},
         "kernel_ms_per_step": {"level": expand_ms, "finalize": sum(s.finalize_ms for s in stats) / len(stats)},
         "children_per_step": st.children, "local_child_fraction": st.local_children / max(st.children, 1),
         "direction": {"mode": args.direction, "bottom_up_levels": st.bottom_up_levels, "levels": st.levels},
@@ -586,8 +625,11 @@ def main():
         line["e2e"]["d2h_bytes_per_step"] += st.spill_bytes
     if not args.no_cpu_baseline and world == 1:
         s, secs, ck = cpu_reference_sample()
+        kind_s, a_s, _, algo_s = REF_SAMPLE
         line["cpu_baseline"] = {"value": s / secs, "unit": "states/s", "cores": 1, "kind": ck,
-                                "sample": "reference InMemoryThreeBitBFS on 11-pancake (full search, 39,916,800 states), single-threaded as in the reference"}
+                                "sample": f"reference InMemory{'TwoBit' if algo_s == 'two_bit' else 'ThreeBit'}BFS"
+                                          f" on {a_s}-pancake (full search, {math.factorial(a_s):,} states),"
+                                          " single-threaded as in the reference"}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
