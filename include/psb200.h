@@ -279,6 +279,15 @@ int psb_frontier_index(const uint8_t* stream, uint64_t stream_bytes, psb_codec_b
 int psb_frontier_decode(const uint8_t* d_stream, const psb_codec_block* blocks, uint32_t n_blocks,
                         uint64_t* d_bits, uint64_t first_bit, uint64_t n_bits, void* stream);
 
+/* OpBitsCompression<bits>::Encode / Decode (Common/OpBitsCompression.cpp:
+ * 10-76) on the GPU: `count` op-bit bytes (a multiple of 8, each below
+ * 2^bits) <-> count * bits / 8 packed bytes; bits = 2, 4 or 8.  bits = 4 is
+ * also StreamVInt's operator "bounds" packing (Common/StreamVInt.cpp:139-147).
+ * Device pointers: the op-bit bytes 8-byte aligned, the packed bytes aligned
+ * to `bits` bytes.  Asynchronous on `stream`. */
+int psb_opbits_encode(int bits, const uint8_t* d_op_bits, uint64_t count, uint8_t* d_out, void* stream);
+int psb_opbits_decode(int bits, const uint8_t* d_in, uint64_t count, uint8_t* d_op_bits, void* stream);
+
 /* --- Batched and served solves -----------------------------------------------
  * No single counterpart in the reference (one InMemoryTwoBitBFS per call).
  * An engine keeps many independent two-bit searches on the GPU at once, each

@@ -9,6 +9,8 @@
 #   * std::chrono::high_resolution_clock -> steady_clock (MSVC aliases them)
 #   * `*(__m128i*)(p) = v;` -> _mm_storeu_si128 (MSVC emits an unaligned store
 #     for it; GCC assumes 16-byte alignment)
+#   * `static` dropped from explicit template specializations (MSVC accepts it,
+#     GCC does not)
 #   * a generated <intrin.h> mapping the MSVC intrinsics to GCC builtins, and
 #     the AVX-512VL byte load/store intrinsics to their SSE2 equivalents so the
 #     library runs on any x86-64-v3 host.
@@ -34,7 +36,8 @@ rm -rf "$SRC"
 mkdir -p "$SRC/Common" "$SRC/Puzzles"
 COMMON="Util.h Util.cpp Puzzle.h Puzzle.cpp Buffer.h Array.h BitArray.h InMemoryBFS.h
         InMemoryClassicBFS.cpp InMemoryTwoBitBFS.cpp InMemoryThreeBitBFS.cpp InMemoryFrontierSearch.cpp
-        StreamVInt.h StreamVInt.cpp FrontierCompression.h FrontierCompression.cpp"
+        StreamVInt.h StreamVInt.cpp FrontierCompression.h FrontierCompression.cpp
+        OpBitsCompression.h OpBitsCompression.cpp"
 PUZZLES="PermutationMap.h PermutationMap.cpp SlidingTilePuzzleSimple.h SlidingTilePuzzleSimple.cpp
          PancakeSimple.h PancakeSimple.cpp FourPegHanoiSimple.h FourPegHanoiSimple.cpp"
 for f in $COMMON; do cp "$REF/Common/$f" "$SRC/Common/$f"; done
@@ -44,6 +47,7 @@ find "$SRC" -type f \( -name '*.h' -o -name '*.cpp' \) -print0 | xargs -0 sed -E
     -e 's/([0-9A-Fa-f])ui32/\1U/g' \
     -e 's/([0-9])i64/\1LL/g' \
     -e 's/high_resolution_clock/steady_clock/g' \
+    -e 's/^__forceinline static int (_(En|De)codeTuple<[0-9]>)/__forceinline int \1/' \
     -e 's/\*\(__m128i\*\)\(([^)]*)\) = ([a-z_]+);/_mm_storeu_si128((__m128i*)(\1), \2);/g'
 
 cat > "$SRC/intrin.h" <<'EOF'

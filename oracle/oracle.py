@@ -62,6 +62,9 @@ def lib():
             getattr(L, f).argtypes = [ctypes.c_int, u32p, u8p]
         L.orc_fc_decode.argtypes = [ctypes.POINTER(ctypes.c_int), u8p, u32p]
         L.orc_fc_is_bitmap.argtypes = [u8p]
+        for f in ("orc_opbits_encode", "orc_opbits_decode"):
+            getattr(L, f).restype = ctypes.c_int64
+            getattr(L, f).argtypes = [ctypes.c_int, ctypes.c_uint64, u8p, u8p]
         _lib = L
     return _lib
 
@@ -322,3 +325,34 @@ def segment_stream(offsets):
         k = lib().orc_fc_encode(n, idx.ctypes.data_as(u32p), buf)
         out.append(bytes(buf[:k]))
     return b"".join(out)
+
+
+def opbits_encode(bits, ops):
+    """OpBitsCompression<bits>::Encode (Common/OpBitsCompression.cpp:57-65): bytes."""
+    n = len(ops)
+    src = (ctypes.c_uint8 * max(n, 1))(*ops)
+    out = (ctypes.c_uint8 * max(n, 1))()
+    k = lib().orc_opbits_encode(bits, n, src, out)
+    if k < 0:
+        raise ValueError("count must be a multiple of 8 and bits 2, 4 or 8")
+    return bytes(out[:k])
+
+
+def opbits_decode(bits, data, count):
+    src = (ctypes.c_uint8 * max(len(data), 1))(*data)
+    out = (ctypes.c_uint8 * max(count, 1))()
+    if lib().orc_opbits_decode(bits, count, src, out) < 0:
+        raise ValueError("count must be a multiple of 8 and bits 2, 4 or 8")
+    return list(out[:count])
+
+
+def ref_opbits_encode(bits, ops):
+    """The reference's own OpBitsCompression<bits>::Encode (oracle/_ref)."""
+    L = ref()
+    L.ref_opbits_encode.restype = ctypes.c_int64
+    L.ref_opbits_encode.argtypes = [ctypes.c_int, ctypes.c_uint64, u8p, u8p]
+    n = len(ops)
+    src = (ctypes.c_uint8 * max(n, 1))(*ops)
+    out = (ctypes.c_uint8 * max(n, 1))()
+    k = L.ref_opbits_encode(bits, n, src, out)
+    return bytes(out[:k])

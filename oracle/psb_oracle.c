@@ -613,6 +613,43 @@ int orc_svi_decode_ops(int* size, const uint8_t* in, uint32_t* idx, uint8_t* bou
     return count;
 }
 
+/* OpBitsCompression<BITS> (Common/OpBitsCompression.cpp:10-76): every group
+ * of 8 op-bit bytes (little-endian u64 `all`) becomes BITS bytes:
+ *   BITS 2: u16 (all | all >> 14 | all >> 28 | all >> 42)
+ *   BITS 4: u32 (all | all >> 28)            (the StreamVInt bounds packing)
+ *   BITS 8: the 8 bytes unchanged.
+ * count must be a multiple of 8; returns the bytes written / read. */
+int64_t orc_opbits_encode(int bits, uint64_t count, const uint8_t* ops, uint8_t* out) {
+    if ((count & 7) || (bits != 2 && bits != 4 && bits != 8)) return -1;
+    uint64_t pos = 0;
+    for (uint64_t i = 0; i < count; i += 8) {
+        uint64_t all = 0;
+        for (int k = 0; k < 8; k++) all |= (uint64_t)ops[i + k] << (8 * k);
+        uint64_t packed = bits == 2 ? (all | (all >> 14) | (all >> 28) | (all >> 42)) : bits == 4 ? (all | (all >> 28)) : all;
+        for (int k = 0; k < bits; k++) out[pos + k] = (uint8_t)(packed >> (8 * k));
+        pos += (uint64_t)bits;
+    }
+    return (int64_t)pos;
+}
+
+int64_t orc_opbits_decode(int bits, uint64_t count, const uint8_t* in, uint8_t* ops) {
+    if ((count & 7) || (bits != 2 && bits != 4 && bits != 8)) return -1;
+    uint64_t pos = 0;
+    for (uint64_t i = 0; i < count; i += 8) {
+        uint64_t st = 0, all;
+        for (int k = 0; k < bits; k++) st |= (uint64_t)in[pos + k] << (8 * k);
+        if (bits == 2)
+            all = (st & 0x0303ull) | ((st & 0x0C0Cull) << 14) | ((st & 0x3030ull) << 28) | ((st & 0xC0C0ull) << 42);
+        else if (bits == 4)
+            all = (st & 0x0F0F0F0Full) | ((st & 0xF0F0F0F0ull) << 28);
+        else
+            all = st;
+        for (int k = 0; k < 8; k++) ops[i + k] = (uint8_t)(all >> (8 * k));
+        pos += (uint64_t)bits;
+    }
+    return (int64_t)pos;
+}
+
 /* ------------------------------------------------------------------------- */
 /* FrontierCompression: Common/FrontierCompression.cpp                         */
 /* ------------------------------------------------------------------------- */

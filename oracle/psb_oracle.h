@@ -74,6 +74,8 @@ int orc_svi_decode(int* size, const uint8_t* in, uint32_t* indexes); /* returns 
 int orc_svi_encode_bounds(int count, const uint32_t* idx_deltas_unused, const uint8_t* bounds, uint8_t* out);
 /* Index stream followed by the operator bits ("bounds", 4 bits per index). */
 int orc_svi_encode_ops(int count, uint32_t* indexes, uint8_t* bounds, uint8_t* out);
+int64_t orc_opbits_encode(int bits, uint64_t count, const uint8_t* ops, uint8_t* out);
+int64_t orc_opbits_decode(int bits, uint64_t count, const uint8_t* in, uint8_t* ops);
 int orc_svi_decode_ops(int* size, const uint8_t* in, uint32_t* indexes, uint8_t* bounds);
 
 /* FrontierCompression (Common/FrontierCompression.cpp) -- byte-exact. */

@@ -6,6 +6,7 @@
 // by bench.py --impl reference for the CPU baseline.
 #include "Common/InMemoryBFS.h"
 #include "Common/FrontierCompression.h"
+#include "Common/OpBitsCompression.h"
 #include "Common/StreamVInt.h"
 #include "Puzzles/FourPegHanoiSimple.h"
 #include "Puzzles/PancakeSimple.h"
@@ -163,6 +164,15 @@ int ref_fc_encode_with_check(int count, uint32_t* indexes, uint8_t* out, int out
 
 int ref_fc_decode(int* size, uint8_t* in, uint32_t* indexes, int cap) {
     return FrontierCompression::Decode(*size, in, indexes, cap);
+}
+
+int64_t ref_opbits_encode(int bits, uint64_t count, const uint8_t* ops, uint8_t* out) {
+    switch (bits) {
+    case 2: return int64_t(OpBitsCompression<2>::Encode(count, ops, out));
+    case 4: return int64_t(OpBitsCompression<4>::Encode(count, ops, out));
+    case 8: return int64_t(OpBitsCompression<8>::Encode(count, ops, out));
+    }
+    return -1;
 }
 
 }  // extern "C"

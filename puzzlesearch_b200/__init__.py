@@ -129,6 +129,10 @@ def lib():
                                          ctypes.c_uint32, u32p]
         L.psb_frontier_decode.argtypes = [ctypes.c_void_p, ctypes.POINTER(CodecBlock), ctypes.c_uint32, u64p,
                                           ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+        L.psb_opbits_encode.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                        ctypes.c_void_p]
+        L.psb_opbits_decode.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                        ctypes.c_void_p]
         L.psb_engine_create.argtypes = [ctypes.POINTER(EngineOpts), ctypes.POINTER(P)]
         L.psb_engine_destroy.argtypes = [P]
         L.psb_engine_footprint.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, u64p]

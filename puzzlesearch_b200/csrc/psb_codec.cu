@@ -710,6 +710,38 @@ int frontier_bits_nibbles(const uint64_t* nibbles, const uint64_t* excl, uint64_
     return PSB_OK;
 }
 
+// OpBitsCompression<BITS> (Common/OpBitsCompression.cpp:10-76): each group of
+// 8 op-bit bytes (a little-endian u64 `all`) packs into BITS bytes,
+//   BITS 2: u16 (all | all >> 14 | all >> 28 | all >> 42)
+//   BITS 4: u32 (all | all >> 28)   (also StreamVInt's bounds, StreamVInt.cpp:139-147)
+//   BITS 8: unchanged.
+// One thread per group: one 8-byte load, one BITS-byte store.
+template <int BITS>
+__global__ void k_opbits_encode(const uint64_t* __restrict__ in, uint64_t groups, uint8_t* __restrict__ out) {
+    for (uint64_t g = blockIdx.x * uint64_t(kT) + threadIdx.x; g < groups; g += uint64_t(gridDim.x) * kT) {
+        const uint64_t all = in[g];
+        if constexpr (BITS == 2) reinterpret_cast<uint16_t*>(out)[g] = uint16_t(all | (all >> 14) | (all >> 28) | (all >> 42));
+        else if constexpr (BITS == 4) reinterpret_cast<uint32_t*>(out)[g] = uint32_t(all | (all >> 28));
+        else reinterpret_cast<uint64_t*>(out)[g] = all;
+    }
+}
+template <int BITS>
+__global__ void k_opbits_decode(const uint8_t* __restrict__ in, uint64_t groups, uint64_t* __restrict__ out) {
+    for (uint64_t g = blockIdx.x * uint64_t(kT) + threadIdx.x; g < groups; g += uint64_t(gridDim.x) * kT) {
+        uint64_t all;
+        if constexpr (BITS == 2) {
+            const uint64_t st = reinterpret_cast<const uint16_t*>(in)[g];
+            all = (st & 0x0303ull) | ((st & 0x0C0Cull) << 14) | ((st & 0x3030ull) << 28) | ((st & 0xC0C0ull) << 42);
+        } else if constexpr (BITS == 4) {
+            const uint64_t st = reinterpret_cast<const uint32_t*>(in)[g];
+            all = (st & 0x0F0F0F0Full) | ((st & 0xF0F0F0F0ull) << 28);
+        } else {
+            all = reinterpret_cast<const uint64_t*>(in)[g];
+        }
+        out[g] = all;
+    }
+}
+
 SegmentEncoder* encoder_create() { return new (std::nothrow) SegmentEncoder(); }
 void encoder_destroy(SegmentEncoder* e) { delete e; }
 
@@ -838,5 +870,47 @@ extern "C" int psb_frontier_decode(const uint8_t* d_in, const psb_codec_block* b
     cudaFree(d_err);
     CD_CUDA(e);
     if (err) return psb_set_error(PSB_ERR_ARG, "a decoded offset lies outside the segment");
+    return PSB_OK;
+}
+
+namespace {
+int opbits_check(int bits, const void* in, uint64_t count, const void* out) {
+    if (bits != 2 && bits != 4 && bits != 8) return psb_set_error(PSB_ERR_ARG, "bits must be 2, 4 or 8");
+    if (count & 7) return psb_set_error(PSB_ERR_ARG, "count must be a multiple of 8");
+    if (count && (!in || !out)) return psb_set_error(PSB_ERR_ARG, "bad argument");
+    return PSB_OK;
+}
+unsigned opbits_grid(uint64_t groups) {
+    return unsigned(std::min<uint64_t>((groups + kT - 1) / kT, 148ull * 16));
+}
+}  // namespace
+
+extern "C" int psb_opbits_encode(int bits, const uint8_t* d_op_bits, uint64_t count, uint8_t* d_out, void* stream) {
+    if (int rc = opbits_check(bits, d_op_bits, count, d_out)) return rc;
+    if (reinterpret_cast<uintptr_t>(d_op_bits) % 8 || reinterpret_cast<uintptr_t>(d_out) % bits)
+        return psb_set_error(PSB_ERR_ARG, "op bits must be 8-byte aligned and the output aligned to `bits` bytes");
+    const uint64_t groups = count / 8;
+    if (!groups) return PSB_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint64_t* in = reinterpret_cast<const uint64_t*>(d_op_bits);
+    if (bits == 2) psb::k_opbits_encode<2><<<opbits_grid(groups), kT, 0, s>>>(in, groups, d_out);
+    else if (bits == 4) psb::k_opbits_encode<4><<<opbits_grid(groups), kT, 0, s>>>(in, groups, d_out);
+    else psb::k_opbits_encode<8><<<opbits_grid(groups), kT, 0, s>>>(in, groups, d_out);
+    CD_CUDA(cudaGetLastError());
+    return PSB_OK;
+}
+
+extern "C" int psb_opbits_decode(int bits, const uint8_t* d_in, uint64_t count, uint8_t* d_op_bits, void* stream) {
+    if (int rc = opbits_check(bits, d_in, count, d_op_bits)) return rc;
+    if (reinterpret_cast<uintptr_t>(d_op_bits) % 8 || reinterpret_cast<uintptr_t>(d_in) % bits)
+        return psb_set_error(PSB_ERR_ARG, "op bits must be 8-byte aligned and the input aligned to `bits` bytes");
+    const uint64_t groups = count / 8;
+    if (!groups) return PSB_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint64_t* out = reinterpret_cast<uint64_t*>(d_op_bits);
+    if (bits == 2) psb::k_opbits_decode<2><<<opbits_grid(groups), kT, 0, s>>>(d_in, groups, out);
+    else if (bits == 4) psb::k_opbits_decode<4><<<opbits_grid(groups), kT, 0, s>>>(d_in, groups, out);
+    else psb::k_opbits_decode<8><<<opbits_grid(groups), kT, 0, s>>>(d_in, groups, out);
+    CD_CUDA(cudaGetLastError());
     return PSB_OK;
 }

@@ -203,6 +203,18 @@ def compression_kats(ref):
             "same_begin_end": {"values": [100, 10000, 2500, 2, 100], "result": -1, "source": f"{path}:{lineno(text, text.index('SameBeginningEnd'))}"}}
 
 
+def opbits_kats(ref):
+    """CommonTests/CompressionOpBitsTests.cpp: OpBitsCompression<BITS> round
+    trips with their encoded sizes."""
+    path = "CommonTests/CompressionOpBitsTests.cpp"
+    text = open(os.path.join(ref, path)).read()
+    out = []
+    for m in re.finditer(r"TestOpBits<(\d)>\(\{([^}]*)\}, (\d+)\);", text):
+        out.append({"bits": int(m.group(1)), "values": [int(x) for x in m.group(2).split(",")],
+                    "bytes": int(m.group(3)), "source": f"{path}:{lineno(text, m.start())}"})
+    return out
+
+
 def bitarray_kat(ref):
     path = "CommonTests/TestBoolArray.cpp"
     text = open(os.path.join(ref, path)).read()
@@ -352,12 +364,18 @@ def main():
         "streamvint": streamvint_kats(ref),
         "compression": compression_kats(ref),
         "bitarray": bitarray_kat(ref),
+        "opbits": opbits_kats(ref),
     }
+    path = os.path.join(HERE, "reference_vectors.json")
+    if args.skip_ref_runs and os.path.exists(path):  # keep the runs already recorded
+        old = json.load(open(path))
+        for key in ("ref_runs", "ref_expand"):
+            if key in old:
+                data[key] = old[key]
     if not args.skip_ref_runs:
         lib = load_ref()
         data["ref_runs"] = ref_runs(lib)
         data["ref_expand"] = ref_expand_batches(lib)
-    path = os.path.join(HERE, "reference_vectors.json")
     with open(path, "w") as f:
         json.dump(data, f, indent=1)
     print(f"wrote {path}: " + ", ".join(f"{k}={len(v) if isinstance(v, list) else 'obj'}" for k, v in data.items()))

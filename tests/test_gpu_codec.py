@@ -147,3 +147,35 @@ def test_encode_mixed_density_segments(case):
     torch.cuda.synchronize()
     psb.frontier_decode(d_out.data_ptr(), blocks, nb, d_back.data_ptr(), 0, n_bits)
     assert torch.equal(d_back.cpu(), d_bits.cpu())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bits", [2, 4, 8])
+def test_opbits_codec_matches_oracle(bits, golden):
+    """psb_opbits_encode / decode (OpBitsCompression<bits>) on the GPU: the
+    packed bytes equal the oracle's, which equal the reference's
+    (tests/test_oracle.py), and decoding gives the op bits back; the
+    reference's own test inputs and a large random array."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(bits)
+    arrays = [np.array(v["values"], dtype=np.uint8) for v in golden["opbits"] if v["bits"] == bits]
+    arrays.append(rng.integers(0, 1 << bits, size=1 << 20, dtype=np.uint8))
+    for ops in arrays:
+        d_ops = torch.from_numpy(ops).cuda()
+        d_packed = torch.empty(len(ops) * bits // 8, dtype=torch.uint8, device="cuda")
+        d_back = torch.empty(len(ops), dtype=torch.uint8, device="cuda")
+        psb._check(psb.lib().psb_opbits_encode(bits, d_ops.data_ptr(), len(ops), d_packed.data_ptr(), None))
+        psb._check(psb.lib().psb_opbits_decode(bits, d_packed.data_ptr(), len(ops), d_back.data_ptr(), None))
+        torch.cuda.synchronize()
+        assert bytes(d_packed.cpu().numpy().tobytes()) == O.opbits_encode(bits, ops.tolist())
+        assert np.array_equal(d_back.cpu().numpy(), ops)
+
+
+def test_opbits_argument_errors():
+    """Checked on the host before anything reaches the device."""
+    with pytest.raises(psb.PsbError):
+        psb._check(psb.lib().psb_opbits_encode(3, 0x1000, 8, 0x2000, None))
+    with pytest.raises(psb.PsbError):
+        psb._check(psb.lib().psb_opbits_encode(4, 0x1000, 12, 0x2000, None))
+    with pytest.raises(psb.PsbError):
+        psb._check(psb.lib().psb_opbits_decode(4, 0x1002, 8, 0x2000, None))

@@ -1,8 +1,11 @@
 """Pins the CPU oracle (oracle/psb_oracle.c) to the reference's golden vectors
 and, when oracle/_ref has been built from the reference's sources, to the
 reference itself.  CPU only."""
+import json
 import math
+import os
 import random
+import subprocess
 
 import pytest
 
@@ -181,6 +184,42 @@ def test_oracle_vs_reference_random_expand():
         assert O.expand(spec, parents, opbits) == O.ref_expand(spec, parents, opbits), spec
 
 
+@pytest.mark.skipif(not os.path.exists(os.path.join(O.HERE, "_ref", "psbref_mt")),
+                    reason="oracle/_ref not built (reference sources absent)")
+def test_mt_fixture_driver_matches_reference():
+    """psbref_mt (the reference's puzzle classes under a multi-threaded
+    three-bit level loop, which made the 14-pancake and 18-disk fixtures)
+    gives the unmodified reference's per-depth counts."""
+    ref_dir = os.path.join(O.HERE, "_ref")
+    for spec in (["pancake", 10, 0], ["hanoi4", 11, 0], ["hanoi4", 9, 1], ["sliding", 3, 3], ["sliding", 4, 2]):
+        kind = {"sliding": 1, "pancake": 2, "hanoi4": 3}[spec[0]]
+        args = [str(kind), str(spec[1]), str(spec[2])]
+        mt = subprocess.run([os.path.join(ref_dir, "psbref_mt")] + args + ["3"], check=True, capture_output=True,
+                            text=True).stdout
+        one = subprocess.run([os.path.join(ref_dir, "psbref")] + args + ["2"], check=True, capture_output=True,
+                             text=True).stdout
+        assert json.loads(mt)["counts"] == json.loads(one)["counts"], spec
+
+
+def test_large_fixtures(golden):
+    """The full-size fixtures: every state reached once, and each vector
+    starts with the reference's own golden prefix where one exists."""
+    path = os.path.join(os.path.dirname(__file__), "golden", "large_counts.json")
+    if not os.path.exists(path):
+        pytest.skip("the large fixtures are still being made (tests/golden/make_large_fixtures.py)")
+    with open(path) as f:
+        large = json.load(f)["searches"]
+    assert sorted(large) == ["hanoi18", "pancake13", "pancake14"]
+    assert sum(large["pancake13"]["counts"]) == math.factorial(13)
+    assert sum(large["pancake14"]["counts"]) == math.factorial(14)
+    assert sum(large["hanoi18"]["counts"]) == 4 ** 18
+    h18 = [v for v in golden["legacy_hanoi"] if v["puzzle"] == ["hanoi4", 18, 0]][0]
+    assert large["hanoi18"]["counts"][:len(h18["counts"])] == h18["counts"]
+    p13 = [v for v in golden["search"] if v["puzzle"] == ["pancake", 13, 0]][0]
+    assert large["pancake13"]["counts"][:len(p13["counts"])] == p13["counts"]
+    assert large["pancake14"]["counts"][:2] == [1, 13]  # depth 1: the 13 flips of the identity
+
+
 # --- codecs (CommonTests/StreamVIntTests.cpp, CompressionTests.cpp) -----------
 
 def test_streamvint_tuples(golden):
@@ -238,3 +277,22 @@ def test_codec_bytes_match_reference():
         vals = sorted(rng.sample(range(span), n)) if span >= n else list(range(n))
         for wc in (False, True):
             assert O.fc_encode(vals, wc) == O.ref_fc_encode(vals, wc), (n, span, wc)
+
+
+def test_opbits_known_answers(golden):
+    """OpBitsCompression<2/4/8> (CommonTests/CompressionOpBitsTests.cpp):
+    encoded sizes and round trips."""
+    assert len(golden["opbits"]) == 9
+    for v in golden["opbits"]:
+        enc = O.opbits_encode(v["bits"], v["values"])
+        assert len(enc) == v["bytes"], v["source"]
+        assert O.opbits_decode(v["bits"], enc, len(v["values"])) == v["values"], v["source"]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_opbits_bytes_match_reference():
+    rng = random.Random(11)
+    for bits in (2, 4, 8):
+        for n in (8, 64, 4096):
+            ops = [rng.randrange(1 << bits) for _ in range(n)]
+            assert O.opbits_encode(bits, ops) == O.ref_opbits_encode(bits, ops), (bits, n)
