@@ -48,6 +48,7 @@ WORKLOADS = {
     # smaller cases of the same kernels, sized for ncu captures (arrays above L2, a few GB at most)
     "hanoi15-2bit": ("hanoi4", 15, 0, "two_bit", "15-disk 4-peg Hanoi in-memory two-bit BFS (profiling case)"),
     "pancake12-3bit": ("pancake", 12, 0, "three_bit", "12-pancake in-memory three-bit BFS (profiling case)"),
+    "pancake13-2bit": ("pancake", 13, 0, "two_bit", "13-pancake in-memory two-bit BFS (profiling case)"),
     # the other two in-memory algorithms
     "hanoi16-frontier": ("hanoi4", 16, 0, "frontier", "16-disk 4-peg Hanoi in-memory frontier search, full solve"),
     "pancake12-classic": ("pancake", 12, 0, "classic", "12-pancake in-memory classic BFS, full solve from the identity"),
@@ -275,22 +276,22 @@ def batch_bench(args):
         items.append((i, t, solvable_start(rng, *t, puzzles[t])))
     total_states = sum(puzzles[t].IndexesCount() // (2 if t[0] == "sliding" else 1) for _, t, _ in items)
     direction = "top_down" if args.direction == "top_down" else "auto"
-    blocks_per_sm, tuning = 0, None
-    if args.autotune:  # persistent grid picked on a separate calibration batch (another seed)
+    blocks_per_sm, wb_offset, tuning = 0, 0, None
+    if args.autotune:  # launch shape picked on a separate calibration batch (another seed)
         from puzzlesearch_b200 import autotune
         crng = random.Random(77)
         calib = []
         for _ in range(min(1024, args.instances)):
             t = BATCH_TYPES[crng.randrange(len(BATCH_TYPES))]
             calib.append((puzzles[t], solvable_start(crng, *t, puzzles[t])))
-        blocks_per_sm, timings = autotune.tune_engine(calib, candidates=(1, 2, 3, 4), pool_bytes=24 << 30,
-                                                      direction=direction)
-        tuning = {"blocks_per_sm": blocks_per_sm, "calibration_instances": len(calib),
-                  "seconds": {str(k): round(v, 4) for k, v in timings.items()}}
+        (blocks_per_sm, wb_offset), timings = autotune.tune_engine(calib, pool_bytes=24 << 30, direction=direction)
+        tuning = {"blocks_per_sm": blocks_per_sm, "window_bits_offset": wb_offset,
+                  "calibration_instances": len(calib),
+                  "seconds": {f"{k[0]} blocks/SM, window offset {k[1]}": round(v, 4) for k, v in timings.items()}}
 
     def run_batched():
         eng = psb.Engine(max_instances=args.instances, max_depths=128, pool_bytes=24 << 30,
-                         blocks_per_sm=blocks_per_sm, direction=direction)
+                         blocks_per_sm=blocks_per_sm, direction=direction, window_bits_offset=wb_offset)
         t0 = time.perf_counter()
         for i, t, st in items:
             assert eng.add(puzzles[t], st, i)
@@ -321,7 +322,8 @@ def batch_bench(args):
             "higher_is_better": True, "dtype": "u64", "data": "seeded random solvable starts",
             "config": {"workload": "batch4096", "instances": len(items), "states": total_states,
                        "engine_levels": levels, "direction": direction,
-                       "blocks_per_sm": blocks_per_sm or 2, "autotune": tuning},
+                       "blocks_per_sm": blocks_per_sm or 2, "window_bits_offset": wb_offset,
+                       "autotune": tuning},
             "batched": {"seconds": b_dt, "solves_per_s": len(items) / b_dt, "states_per_s": total_states / b_dt},
             "plain_one_per_launch": {"seconds": p_dt, "solves_per_s": len(items) / p_dt,
                                      "states_per_s": total_states / p_dt},
@@ -358,22 +360,20 @@ def serve_bench(args):
             ty = SERVE_TYPES[rng.randrange(len(SERVE_TYPES))]
             arrivals.append(t)
             reqs.append((ty, solvable_start(rng, *ty, puzzles[ty])))
-        # plain: one search at a time in arrival order
-        service = []
-        plain_counts = []
-        for ty, st in reqs:
-            t0 = time.perf_counter()
+        # plain: the same arrival times, one search at a time in arrival
+        # order (FIFO); a request waits until it has arrived and the GPU is free
+        plain_counts, plain_lat = [], []
+        t_start = time.perf_counter()
+        for a, (ty, st) in zip(arrivals, reqs):
+            while time.perf_counter() - t_start < a:
+                time.sleep(0.0002)
             c, _ = sessions[ty].run(st)
-            service.append(time.perf_counter() - t0)
+            plain_lat.append(time.perf_counter() - t_start - a)
             plain_counts.append(c)
-        free_at, plain_lat = 0.0, []
-        for a, sv in zip(arrivals, service):
-            begin = max(a, free_at)
-            free_at = begin + sv
-            plain_lat.append(free_at - a)
-        plain_span = free_at - arrivals[0]
+        plain_span = time.perf_counter() - t_start - arrivals[0]
         # served: submit at the arrival times, continuous batching on the GPU
-        srv = psb.Server(max_instances=1024, max_depths=256, pool_bytes=args.pool_gb << 30)
+        srv = psb.Server(max_instances=1024, max_depths=256, pool_bytes=args.pool_gb << 30,
+                         levels_per_step=args.levels_per_step)
         t_start = time.perf_counter()
         tickets = {}
         done = {}
@@ -401,7 +401,8 @@ def serve_bench(args):
     line = {"metric": "served solves/s and p50/p99 latency (Poisson request streams, continuous batching)",
             "value": max(r["served"]["solves_per_s"] for r in rows), "unit": "solves/s", "n_gpus": 1,
             "higher_is_better": True, "dtype": "u64", "data": "seeded Poisson streams, random solvable starts",
-            "config": {"workload": "serve", "types": len(SERVE_TYPES), "pool_gb": args.pool_gb},
+            "config": {"workload": "serve", "types": len(SERVE_TYPES), "pool_gb": args.pool_gb,
+                       "levels_per_step": args.levels_per_step},
             "rates": rows, "results_equal_plain": True}
     print(json.dumps(line), flush=True)
     return 0
@@ -456,6 +457,8 @@ def main():
     ap.add_argument("--window", type=float, default=3.0, help="--workload serve: seconds of arrivals per rate")
     ap.add_argument("--max-requests", type=int, default=400, help="--workload serve: requests per rate at most")
     ap.add_argument("--pool-gb", type=int, default=32, help="--workload serve: engine pool (HBM admission limit)")
+    ap.add_argument("--levels-per-step", type=int, default=4,
+                    help="--workload serve: engine levels per step while no request waits")
     args = ap.parse_args()
     args.spill = (args.spill or args.workload in SPILL_BY_DEFAULT) and not args.no_spill
     if args.profile_once:

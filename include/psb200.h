@@ -310,6 +310,8 @@ typedef struct {
     int32_t use_graph;      /* 1 = replay each step as a CUDA graph */
     int32_t direction;      /* PSB_DIR_AUTO (0): each instance's dense late levels run bottom-up;
                                PSB_DIR_TOP_DOWN: every level top-down */
+    int32_t window_bits_offset; /* each instance's window is 2^(log2 states - 6 + offset) states, clamped to
+                                   2^10 .. 2^16 (0 = the rule; -6..6) */
 } psb_engine_opts;
 int psb_engine_create(const psb_engine_opts* opts, psb_engine** out);
 int psb_engine_destroy(psb_engine* e);
@@ -336,7 +338,8 @@ int psb_engine_info(psb_engine* e, uint32_t* active, uint64_t* largest_free_byte
 typedef struct psb_server psb_server;
 typedef struct {
     uint32_t struct_size;     /* sizeof(psb_server_opts) */
-    uint32_t levels_per_step; /* BFS levels per engine step (0 = 1) */
+    uint32_t levels_per_step; /* BFS levels per engine step while no request waits for admission (0 = 1); one
+                                 level per step while requests wait */
     psb_engine_opts engine;
 } psb_server_opts;
 int psb_server_start(const psb_server_opts* opts, psb_server** out);

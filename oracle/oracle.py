@@ -327,6 +327,51 @@ def segment_stream(offsets):
     return b"".join(out)
 
 
+def frontier_stream(offsets, nibbles):
+    """The reference's frontier-search segment stream for ascending u32
+    offsets and their operator bits: blocks of 262,144 StreamVInt::Encode'd
+    with bounds and concatenated (CompressedFrontierWriter,
+    Common/CompressedFrontier.cpp:56-70)."""
+    import numpy as np
+    L = lib()
+    L.orc_svi_encode_ops.argtypes = [ctypes.c_int, u32p, u8p, u8p]
+    out = []
+    B = 256 * 1024
+    for s in range(0, len(offsets), B):
+        blk = np.ascontiguousarray(offsets[s:s + B], dtype=np.uint32)
+        n = len(blk)
+        adj = (n + 7) // 8 * 8
+        idx = np.zeros(adj + 8, dtype=np.uint32)
+        idx[:n] = blk
+        nib = np.zeros(adj + 8, dtype=np.uint8)
+        nib[:n] = nibbles[s:s + n]
+        buf = (ctypes.c_uint8 * (4 + 17 * (adj // 4) + adj // 2 + 64))()
+        k = L.orc_svi_encode_ops(n, idx.ctypes.data_as(u32p), nib.ctypes.data_as(u8p), buf)
+        out.append(bytes(buf[:k]))
+    return b"".join(out)
+
+
+def frontier_nibbles(spec, dist):
+    """Operator bits a frontier search holds for each state when its depth is
+    the frontier: the OR of (1 << op) over the moves from its neighbours one
+    depth closer (InMemoryFrontierSearch.cpp:57-112).  dist: orc_depths.
+    One Expand per reached state: for small puzzles only."""
+    import numpy as np
+    nib = np.zeros(len(dist), dtype=np.uint8)
+    P1 = (ctypes.c_uint64 * 1)()
+    O1 = (ctypes.c_uint32 * 1)()
+    C = (ctypes.c_uint64 * 16)()
+    CO = (ctypes.c_uint32 * 16)()
+    for p in np.nonzero(dist != 255)[0]:
+        P1[0] = int(p)
+        n = lib().orc_expand(_p(spec), P1, O1, 1, C, CO, 16)
+        for j in range(n):
+            c = C[j]
+            if dist[c] == dist[p] + 1:
+                nib[c] |= 1 << CO[j]
+    return nib
+
+
 def opbits_encode(bits, ops):
     """OpBitsCompression<bits>::Encode (Common/OpBitsCompression.cpp:57-65): bytes."""
     n = len(ops)

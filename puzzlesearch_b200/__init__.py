@@ -72,7 +72,8 @@ class BfsStats(ctypes.Structure):
 class EngineOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("max_instances", ctypes.c_uint32),
                 ("max_depths", ctypes.c_uint32), ("device", ctypes.c_int32), ("pool_bytes", ctypes.c_uint64),
-                ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32), ("direction", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32), ("direction", ctypes.c_int32),
+                ("window_bits_offset", ctypes.c_int32)]
 
 
 class ServerOpts(ctypes.Structure):
@@ -432,8 +433,9 @@ class Engine:
     (batched solves, and continuous batching for serving)."""
 
     def __init__(self, max_instances=4096, max_depths=128, pool_bytes=8 << 30, blocks_per_sm=0, use_graph=True,
-                 device=-1, direction="auto"):
+                 device=-1, direction="auto", window_bits_offset=0):
         o = EngineOpts()
+        o.window_bits_offset = window_bits_offset
         o.direction = DIRECTIONS[direction] if isinstance(direction, str) else int(direction)
         o.struct_size = ctypes.sizeof(EngineOpts)
         o.max_instances = max_instances
@@ -498,12 +500,15 @@ class Engine:
 class Server:
     """psb_server: a solve server with continuous batching on one GPU."""
 
-    def __init__(self, max_instances=1024, max_depths=256, pool_bytes=16 << 30, levels_per_step=1, device=-1):
+    def __init__(self, max_instances=1024, max_depths=256, pool_bytes=16 << 30, levels_per_step=1, device=-1,
+                 blocks_per_sm=0, window_bits_offset=0):
         o = ServerOpts()
         o.struct_size = ctypes.sizeof(ServerOpts)
         o.levels_per_step = levels_per_step
         e = o.engine
         e.struct_size = ctypes.sizeof(EngineOpts)
+        e.blocks_per_sm = blocks_per_sm
+        e.window_bits_offset = window_bits_offset
         e.max_instances = max_instances
         e.max_depths = max_depths
         e.device = device

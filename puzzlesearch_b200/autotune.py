@@ -1,7 +1,8 @@
-"""Autotuner for the two launch shapes that are picked by measurement rather
-than by rule: the batch engine's persistent grid (blocks per SM) and the
-window of a single search's level kernel (states per thread-block window,
-the unit of work the kernel sweeps and marks in shared memory).
+"""Autotuner for the launch shapes that are picked by measurement rather than
+by rule: the batch engine's persistent grid (blocks per SM) and its
+instances' window size, and the window of a single search's level kernel
+(states per thread-block window, the unit of work the kernel sweeps and
+marks in shared memory).
 
 Each candidate runs the same workload on this device.  The tuner checks that
 every candidate gives the same results, and returns the fastest one with all
@@ -54,9 +55,10 @@ class Cache:
             os.replace(tmp, self.path)
 
 
-def _run_engine(items, blocks_per_sm, levels_per_step, pool_bytes, direction):
+def _run_engine(items, shape, levels_per_step, pool_bytes, direction):
+    blocks_per_sm, window_bits_offset = shape if isinstance(shape, tuple) else (shape, 0)
     eng = Engine(max_instances=len(items), pool_bytes=pool_bytes, blocks_per_sm=blocks_per_sm,
-                 direction=direction)
+                 direction=direction, window_bits_offset=window_bits_offset)
     try:
         t0 = time.perf_counter()
         for tag, (puzzle, start) in enumerate(items):
@@ -71,14 +73,22 @@ def _run_engine(items, blocks_per_sm, levels_per_step, pool_bytes, direction):
         eng.close()
 
 
-def tune_engine(items, candidates=(1, 2, 3, 4), levels_per_step=8, pool_bytes=8 << 30, direction="auto",
+ENGINE_SHAPES = tuple((b, w) for b in (1, 2, 3, 4) for w in (-2, -1, 0, 1))
+
+
+def tune_engine(items, candidates=ENGINE_SHAPES, levels_per_step=8, pool_bytes=8 << 30, direction="auto",
                 cache=None, key=None):
-    """Blocks per SM for the batch engine's persistent level kernel, timed on
-    a calibration batch `items` = [(puzzle, start index)] (admission, all
-    steps and the result read-back).  Returns (best, {candidate: seconds})."""
+    """The batch engine's launch shape, timed on a calibration batch `items`
+    = [(puzzle, start index)] (admission, all steps and the result
+    read-back): persistent blocks per SM x the instances' window size (as an
+    offset from the engine's rule of 2^(log2 states - 6) states; windows are
+    also the engine's work items and flag units).  A candidate is a
+    (blocks_per_sm, window_bits_offset) pair, or a plain blocks-per-SM count.
+    Returns (best, {candidate: seconds})."""
     dev = device_name()
     if cache and key and cache.get(dev, key) is not None:
-        return cache.get(dev, key), {}
+        hit = cache.get(dev, key)
+        return (tuple(hit) if isinstance(hit, list) else hit), {}
     _run_engine(items[: max(1, len(items) // 8)], candidates[0], levels_per_step, pool_bytes, direction)  # warm-up
     best, timings = tune(candidates, lambda c: _run_engine(items, c, levels_per_step, pool_bytes, direction))
     if cache and key:

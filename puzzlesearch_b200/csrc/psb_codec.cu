@@ -280,7 +280,9 @@ __global__ void __launch_bounds__(kT) k_select_blocks(const uint64_t* bits, uint
 // FrontierCompression::Encode (FrontierCompression.cpp:92-102): a block is a
 // bitmap block when it holds more than 128 offsets and its bitmap is smaller
 // than 10 bits per offset.
-__global__ void k_block_decide(uint64_t count, BlockInfo* blocks, uint32_t nb) {
+// With operator bits (force_svi) every block is a StreamVInt block, as
+// CompressedFrontierWriter writes them (Common/CompressedFrontier.cpp:63-70).
+__global__ void k_block_decide(uint64_t count, BlockInfo* blocks, uint32_t nb, int force_svi) {
     const uint32_t b = blockIdx.x * kT + threadIdx.x;
     if (b >= nb) return;
     BlockInfo& bi = blocks[b];
@@ -288,7 +290,7 @@ __global__ void k_block_decide(uint64_t count, BlockInfo* blocks, uint32_t nb) {
     const uint32_t n = uint32_t(count - r0 < kBlock ? count - r0 : kBlock);
     bi.count = n;
     const uint64_t bm_bytes = (uint64_t(bi.last) - bi.first + 63) / 64 * 8 + 8;
-    bi.is_bitmap = (n > 128 && bm_bytes * 8 < uint64_t(n) * 10 - 8) ? 1 : 0;
+    bi.is_bitmap = (!force_svi && n > 128 && bm_bytes * 8 < uint64_t(n) * 10 - 8) ? 1 : 0;
     bi.bytes = bi.is_bitmap ? bm_bytes : 0;
     bi.out_off = 0;
 }
@@ -324,14 +326,46 @@ __global__ void k_tuple_len(const uint32_t* idx, const BlockInfo* blocks, const 
     tlen[t] = len;
 }
 
+// Bytes of each StreamVInt block: header, tuples and, with operator bits,
+// the bounds (one nibble per padded value, StreamVInt.cpp:253-275).
 __global__ void k_block_bytes(BlockInfo* blocks, const SviRef* refs, uint32_t n_refs,
-                              const unsigned long long* tscan, uint64_t tuples, unsigned long long total) {
+                              const unsigned long long* tscan, uint64_t tuples, unsigned long long total,
+                              int with_ops) {
     const uint32_t j = blockIdx.x * kT + threadIdx.x;
     if (j >= n_refs) return;
     BlockInfo& bi = blocks[refs[j].block];
     const uint64_t t0 = refs[j].tuple0, t1 = j + 1 < n_refs ? refs[j + 1].tuple0 : tuples;
     const unsigned long long end = t1 < tuples ? tscan[t1] : total;
-    bi.bytes = 4 + (end - tscan[t0]);
+    bi.bytes = 4 + (end - tscan[t0]) + (with_ops ? (uint64_t(bi.count) + 7) / 8 * 4 : 0);
+}
+
+// Bounds of the StreamVInt blocks (StreamVInt::EncodeBounds,
+// StreamVInt.cpp:139-147,193-198): the operator nibble of each value, 8 per
+// group packed as bytes b_q | b_(q+4) << 4, after the block's tuples.  The
+// nibble of offset v is state nib_first + v of the 4-bit array `nib` (NULL:
+// every nibble is 0); values past the count have nibble 0.  One thread per
+// group of 8 values (two tuples).
+__global__ void k_write_bounds(const uint32_t* idx, const BlockInfo* blocks, const SviRef* refs, uint32_t n_refs,
+                               uint64_t groups, const uint64_t* nib, uint64_t nib_first, uint8_t* out) {
+    const uint64_t g = blockIdx.x * uint64_t(kT) + threadIdx.x;
+    if (g >= groups) return;
+    const SviRef ref = refs[svi_of(refs, n_refs, 2 * g)];
+    const uint32_t k = uint32_t(2 * g - ref.tuple0) * 4;  // first value of the group in its block
+    const BlockInfo bi = blocks[ref.block];
+    const uint64_t r0 = uint64_t(ref.block) * kBlock;
+    const uint64_t adj = (uint64_t(bi.count) + 7) / 8 * 8;
+    uint8_t* p = out + bi.out_off + bi.bytes - adj / 2 + k / 2;
+    uint32_t b[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        b[j] = 0;
+        if (nib && k + j < bi.count) {
+            const uint64_t state = nib_first + idx[r0 + k + j];
+            b[j] = uint32_t(nib[state >> 4] >> (4 * (state & 15))) & 15u;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) p[q] = uint8_t(b[q] | (b[q + 4] << 4));
 }
 
 __global__ void k_write_svi(const uint32_t* idx, const BlockInfo* blocks, const SviRef* refs, uint32_t n_refs,
@@ -477,6 +511,17 @@ struct SegmentEncoder {
     uint32_t nb = 0, n_refs = 0;
     bool any_bitmap = false;
     uint64_t launches = 0;  // kernels launched since the last encoder_take_launches
+    // Operator bits (set_ops): every block StreamVInt with bounds, the nibble
+    // of offset v being state ops_first + v of ops_nib (NULL: all zero).
+    bool with_ops = false;
+    const uint64_t* ops_nib = nullptr;
+    uint64_t ops_first = 0;
+
+    void set_ops(bool on, const uint64_t* nib, uint64_t first) {
+        with_ops = on;
+        ops_nib = nib;
+        ops_first = first;
+    }
 
     ~SegmentEncoder() {
         cudaFree(x.bsum); cudaFree(x.tot); cudaFree(x.tlen); cudaFree(x.gsum);
@@ -524,7 +569,7 @@ struct SegmentEncoder {
         nb = uint32_t((count + kBlock - 1) / kBlock);
         if (int rc = grow(&x.blocks, &x.cap_blocks, size_t(nb) * sizeof(BlockInfo))) return rc;
         k_select_blocks<<<2 * nb, kT, 0, s>>>(bits, n_words, n_bits, x.bsum, nbs, count, x.blocks, nb);
-        k_block_decide<<<(nb + kT - 1) / kT, kT, 0, s>>>(count, x.blocks, nb);
+        k_block_decide<<<(nb + kT - 1) / kT, kT, 0, s>>>(count, x.blocks, nb, with_ops ? 1 : 0);
         launches += 2;
         CD_CUDA(cudaGetLastError());
         hb.resize(nb);
@@ -560,7 +605,8 @@ struct SegmentEncoder {
             unsigned long long svi_total = 0;
             CD_CUDA(cudaMemcpyAsync(&svi_total, x.tot, 8, cudaMemcpyDeviceToHost, s));
             CD_CUDA(cudaStreamSynchronize(s));
-            k_block_bytes<<<(n_refs + kT - 1) / kT, kT, 0, s>>>(x.blocks, x.refs, n_refs, x.tlen, tuples, svi_total);
+            k_block_bytes<<<(n_refs + kT - 1) / kT, kT, 0, s>>>(x.blocks, x.refs, n_refs, x.tlen, tuples, svi_total,
+                                                              with_ops ? 1 : 0);
             launches += 6;
             CD_CUDA(cudaGetLastError());
             CD_CUDA(cudaMemcpyAsync(hb.data(), x.blocks, size_t(nb) * sizeof(BlockInfo), cudaMemcpyDeviceToHost, s));
@@ -583,6 +629,12 @@ struct SegmentEncoder {
             k_write_svi<<<unsigned((tuples + kT - 1) / kT), kT, 0, s>>>(x.idx, x.blocks, x.refs, n_refs, tuples, x.tlen,
                                                                        d_out);
             launches++;
+            if (with_ops) {
+                const uint64_t groups = tuples / 2;
+                k_write_bounds<<<unsigned((groups + kT - 1) / kT), kT, 0, s>>>(x.idx, x.blocks, x.refs, n_refs, groups,
+                                                                              ops_nib, ops_first, d_out);
+                launches++;
+            }
         }
         if (any_bitmap) {
             k_write_bitmap<<<dim3(unsigned((max_words + kT - 1) / kT), nb), kT, 0, s>>>(
@@ -758,6 +810,10 @@ int encoder_plan(SegmentEncoder* e, const uint64_t* d_bits, uint64_t n_bits, cud
 }
 
 int encoder_write(SegmentEncoder* e, uint8_t* d_out, cudaStream_t s) { return e->write(d_out, s); }
+
+void encoder_set_ops(SegmentEncoder* e, bool on, const uint64_t* nibbles, uint64_t first_state) {
+    e->set_ops(on, nibbles, first_state);
+}
 
 uint64_t encoder_take_launches(SegmentEncoder* e) {
     const uint64_t n = e->launches;

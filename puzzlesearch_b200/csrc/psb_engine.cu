@@ -313,10 +313,13 @@ struct psb_engine {
     cudaGraphExec_t exec = nullptr;
     bool use_graph = true;
     bool bottom_up = true;  // instances may run bottom-up levels
+    int wb_offset = 0;      // window bits relative to engine_window_bits' rule
     unsigned grid = 0;
     size_t smem = 0;
     uint64_t levels_run = 0;
     uint32_t* h_done_count = nullptr;  // pinned
+    unsigned long long* h_err = nullptr;  // pinned: the error word, read with the done count after each step
+    bool done_fresh = false;           // *h_done_count was read after the last step and nothing ran since
     unsigned long long* d_staging = nullptr;  // collect rows (device)
     std::vector<unsigned long long> h_staging;
 
@@ -330,6 +333,7 @@ struct psb_engine {
         cudaFree(d.item_start);
         cudaFree(d.err);
         if (h_done_count) cudaFreeHost(h_done_count);
+        if (h_err) cudaFreeHost(h_err);
         cudaFree(d_staging);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -363,21 +367,22 @@ int engine_type(int kind, int a, int b, uint32_t* type) {
                          "engine puzzles: sliding tile with 6, 8, 9, 10 or 12 cells, pancake 7..12, Hanoi up to 16 disks");
 }
 
-int engine_window_bits(uint64_t n) {
+// An instance's window: 2^(log2 n - 6 + offset) states, within 2^10 .. 2^16
+// (offset: psb_engine_opts.window_bits_offset, picked by the autotuner).
+int engine_window_bits(uint64_t n, int offset = 0) {
     int lg = 0;
     while (lg < 63 && (uint64_t(1) << (lg + 1)) <= n) lg++;
-    return std::max(10, std::min(int(psb::kEWindowBitsMax), lg - 6));
+    return std::max(10, std::min(int(psb::kEWindowBitsMax), lg - 6 + offset));
 }
 
 uint64_t two_bit_words(uint64_t n) { return ((2 * n + 63) / 64 + 31) / 32 * 32; }
 
-uint32_t instance_windows(uint64_t n) {
-    const int wb = engine_window_bits(n);
-    return uint32_t((n + (uint64_t(1) << wb) - 1) >> wb);
-}
+uint32_t instance_windows(uint64_t n, int wb) { return uint32_t((n + (uint64_t(1) << wb) - 1) >> wb); }
 
-// Two 256-byte-aligned arrays of one flag byte per window.
-uint64_t flag_words_for(uint64_t n) { return 2 * ((uint64_t(instance_windows(n)) + 255) / 256 * 32); }
+// Two 256-byte-aligned arrays of one flag byte per window, sized for the
+// smallest window (2^10 states), so an instance's footprint does not depend
+// on the engine's window offset.
+uint64_t flag_words_for(uint64_t n) { return 2 * ((uint64_t(instance_windows(n, 10)) + 255) / 256 * 32); }
 
 // Pool words of one instance: its two-bit array plus its window flags.
 uint64_t instance_words(uint64_t n) { return two_bit_words(n) + flag_words_for(n); }
@@ -440,6 +445,9 @@ int psb_engine_create(const psb_engine_opts* opts, psb_engine** out) {
     e->pool_words = opts->pool_bytes / 8;
     e->use_graph = opts->use_graph != 0;
     e->bottom_up = opts->direction != PSB_DIR_TOP_DOWN;
+    if (opts->window_bits_offset < -6 || opts->window_bits_offset > 6)
+        return psb_set_error(PSB_ERR_ARG, "window_bits_offset outside -6..6");
+    e->wb_offset = opts->window_bits_offset;
     EN_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     EN_CUDA(cudaMalloc(&e->pool, e->pool_words * 8));
     e->free_space[0] = e->pool_words;
@@ -465,6 +473,7 @@ int psb_engine_create(const psb_engine_opts* opts, psb_engine** out) {
     EN_CUDA(cudaMemsetAsync(e->d.stats, 0, 8 * 8ull * e->n_slots, e->stream));
     EN_CUDA(cudaMemsetAsync(ib, 0, ints * 4 + 16, e->stream));
     EN_CUDA(cudaMallocHost(&e->h_done_count, 4));
+    EN_CUDA(cudaMallocHost(&e->h_err, 8));
     EN_CUDA(cudaMalloc(&e->d_staging, 8ull * e->n_slots * (e->max_depths + 2)));
     e->h_staging.resize(size_t(e->n_slots) * (e->max_depths + 2));
     e->host_slots.assign(e->n_slots, psb::EngineSlot{});
@@ -515,8 +524,8 @@ int psb_engine_add(psb_engine* e, int kind, int a, int b, uint64_t initial, uint
     std::unique_ptr<psb_puzzle, int (*)(psb_puzzle*)> guard(p, psb_puzzle_destroy);
     if (initial >= p->n_states) return psb_set_error(PSB_ERR_ARG, "initial index >= IndexesCount()");
     if (e->free_slots.empty()) return psb_set_error(PSB_ERR_CAPACITY, "no free instance slot");
-    const int wb = engine_window_bits(p->n_states);
-    const uint32_t windows = instance_windows(p->n_states);
+    const int wb = engine_window_bits(p->n_states, e->wb_offset);
+    const uint32_t windows = instance_windows(p->n_states, wb);
     const uint64_t code_words = two_bit_words(p->n_states);
     const uint64_t flag_words = flag_words_for(p->n_states);
     const uint64_t words = instance_words(p->n_states);
@@ -578,9 +587,13 @@ int psb_engine_step(psb_engine* e, uint32_t levels) {
         else if (int rc = record_step(e)) return rc;
         e->levels_run++;
     }
+    // One host round trip per step: the error word and the completion count
+    // together (psb_engine_poll reuses the count).
+    EN_CUDA(cudaMemcpyAsync(e->h_err, e->d.err, 8, cudaMemcpyDeviceToHost, e->stream));
+    EN_CUDA(cudaMemcpyAsync(e->h_done_count, e->d.done_count, 4, cudaMemcpyDeviceToHost, e->stream));
     EN_CUDA(cudaStreamSynchronize(e->stream));
-    unsigned long long err = 0;
-    EN_CUDA(cudaMemcpy(&err, e->d.err, 8, cudaMemcpyDeviceToHost));
+    e->done_fresh = true;
+    const unsigned long long err = *e->h_err;
     if (err & 1) return psb_set_error(PSB_ERR_DEVICE, "a level produced a child index >= IndexesCount()");
     if (err & 2) return psb_set_error(PSB_ERR_CAPACITY, "an instance has more depths than max_depths");
     return PSB_OK;
@@ -590,11 +603,14 @@ int psb_engine_poll(psb_engine* e, uint64_t* tags, uint32_t* n_depths, uint64_t*
     if (!e || !n || (cap && (!tags || !n_depths || !counts))) return psb_set_error(PSB_ERR_ARG, "bad argument");
     *n = 0;
     cudaStream_t st = e->stream;
-    EN_CUDA(cudaMemcpyAsync(e->h_done_count, e->d.done_count, 4, cudaMemcpyDeviceToHost, st));
-    EN_CUDA(cudaStreamSynchronize(st));
+    if (!e->done_fresh) {
+        EN_CUDA(cudaMemcpyAsync(e->h_done_count, e->d.done_count, 4, cudaMemcpyDeviceToHost, st));
+        EN_CUDA(cudaStreamSynchronize(st));
+    }
     const uint32_t done = *e->h_done_count;
     const uint32_t k = std::min(cap, done - e->done_seen);
     if (k == 0) return PSB_OK;
+    e->done_fresh = false;  // the release below changes the ring
     const size_t row = size_t(e->max_depths) + 2;
     psb::engine_collect<<<k, 128, 0, st>>>(e->d, e->done_seen, k, e->d_staging);
     EN_CUDA(cudaGetLastError());

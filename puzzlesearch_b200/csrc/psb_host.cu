@@ -844,6 +844,9 @@ struct SpillSource {
     const uint64_t* nibbles = nullptr;
     const uint64_t* excl = nullptr;
     uint64_t single = PSB_INVALID_INDEX;
+    // Frontier search: the stream carries each state's operator bits, as
+    // the reference's frontier-search segment files do (CompressedFrontierWriter).
+    bool ops = false;
     // Active-window flags of this depth (one byte per 2^window_bits states,
     // a superset of the windows holding its states), or NULL: segments with
     // no flagged window are empty and skipped without touching the array.
@@ -966,7 +969,12 @@ int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const
         }
         const uint64_t* bits = src.bitmap ? src.bitmap + first / 64 : R->bits;  // after the scratch exists
         uint64_t bytes = 0, count = 0;
-        if (int rc = psb::encoder_plan(R->enc, bits, n, s, sums_ready, &bytes, &count)) return rc;
+        psb::encoder_set_ops(R->enc, src.ops, src.nibbles, first);  // the initial state's nibble is 0
+        const int prc = psb::encoder_plan(R->enc, bits, n, s, sums_ready, &bytes, &count);
+        if (prc) {
+            psb::encoder_set_ops(R->enc, false, nullptr, 0);
+            return prc;
+        }
         if (count == 0) continue;
         if (R->arena_cap < off + bytes) {  // grow, keeping this depth's segments written so far
             const uint64_t want = (off + bytes) + (off + bytes) / 4;
@@ -978,7 +986,9 @@ int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const
             R->arena = bigger;
             R->arena_cap = want;
         }
-        if (int rc = psb::encoder_write(R->enc, R->arena + off, s)) return rc;
+        const int wrc = psb::encoder_write(R->enc, R->arena + off, s);
+        psb::encoder_set_ops(R->enc, false, nullptr, 0);
+        if (wrc) return wrc;
         R->segs.push_back(SpillSeg{depth, uint32_t(g), off, bytes, count});
         off += bytes;
     }
@@ -1094,6 +1104,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             case PSB_FRONTIER:
                 if (first) src.single = initial;
                 else { src.nibbles = fcur; src.excl = P.odd ? cex : nullptr; }
+                src.ops = true;
                 break;
             }
             if (flags_valid >= 0) {

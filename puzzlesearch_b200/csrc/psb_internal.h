@@ -53,6 +53,11 @@ void encoder_destroy(SegmentEncoder* e);
 int encoder_plan(SegmentEncoder* e, const uint64_t* d_bits, uint64_t n_bits, cudaStream_t s, bool sums_ready,
                  uint64_t* bytes, uint64_t* count);
 int encoder_write(SegmentEncoder* e, uint8_t* d_out, cudaStream_t s);
+// Frontier-search segments carry each state's operator bits: with `on`, the
+// following plans write CompressedFrontierWriter's stream (StreamVInt blocks
+// with bounds, Common/CompressedFrontier.cpp:63-70) whose nibble for offset v
+// is state first_state + v of `nibbles` (a 4-bit array; NULL = all zero).
+void encoder_set_ops(SegmentEncoder* e, bool on, const uint64_t* nibbles, uint64_t first_state);
 // The encoder's chunk-sum buffer sized for an n_bits segment.
 int encoder_chunk_sums(SegmentEncoder* e, uint64_t n_bits, unsigned long long** sums);
 // Kernels the encoder launched since the last call.

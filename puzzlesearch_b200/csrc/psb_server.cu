@@ -131,7 +131,15 @@ void serve(psb_server* s) {
             }
         }
         if (!s->running.empty()) {
-            int rc = psb_engine_step(s->engine, s->levels_per_step);
+            // Several levels per step while nothing waits for admission (fewer
+            // host round trips); one level while requests wait, so they are
+            // admitted as soon as a finished search frees its space.
+            uint32_t levels = s->levels_per_step;
+            {
+                std::lock_guard<std::mutex> lock(s->mu);
+                if (!s->queue.empty()) levels = 1;
+            }
+            int rc = psb_engine_step(s->engine, levels);
             uint32_t n = 0;
             if (rc == PSB_OK) rc = psb_engine_poll(s->engine, tags.data(), nd.data(), counts.data(), 1024, &n);
             const auto now = Clock::now();

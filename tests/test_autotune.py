@@ -24,3 +24,11 @@ def test_cache_round_trip(tmp_path):
     assert again.get("NVIDIA B200 (sm_100, 148 SMs)", "batch") == 3
     assert again.get("NVIDIA B200 (sm_100, 148 SMs)", "pancake13-3bit") == 16
     assert again.get("other GPU", "batch") is None
+
+
+def test_engine_shapes_cover_grid_and_window():
+    """The engine tuner's default candidates span both dimensions it tunes."""
+    shapes = autotune.ENGINE_SHAPES
+    assert {b for b, _ in shapes} == {1, 2, 3, 4}
+    assert {w for _, w in shapes} == {-2, -1, 0, 1}
+    assert len(shapes) == len(set(shapes)) == 16

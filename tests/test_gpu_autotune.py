@@ -42,3 +42,30 @@ def test_window_bits():
     assert best in (10, 12, 14) and set(timings) == {10, 12, 14}
     assert all(ms > 0 for ms in timings.values())
     assert psb.device_name().startswith("NVIDIA")
+
+
+def test_engine_window_offsets(tmp_path):
+    """Both engine dimensions: every (blocks per SM, window offset) pair gives
+    the single-instance counts (the tuner checks that all candidates agree),
+    and a cached tuple pick comes back as a tuple."""
+    rng = random.Random(5)
+    items = []
+    for _ in range(48):
+        p = [psb.PancakeSimple(9), psb.SlidingTilePuzzleSimple(2, 5), psb.FourPegHanoiSimple(9)][rng.randrange(3)]
+        items.append((p, rng.randrange(p.IndexesCount()) if not p.Name().startswith("Sliding") else 0))
+    cands = [(2, -2), (2, 0), (4, 1), (1, -1)]
+    cache = autotune.Cache(str(tmp_path / "tune.json"))
+    best, timings = autotune.tune_engine(items, candidates=cands, pool_bytes=1 << 30, cache=cache, key="mix2")
+    assert best in cands and set(timings) == set(cands)
+    assert autotune.tune_engine(items, candidates=cands, cache=autotune.Cache(str(tmp_path / "tune.json")),
+                                key="mix2") == (best, {})
+    eng = psb.Engine(max_instances=8, pool_bytes=1 << 30, blocks_per_sm=best[0], window_bits_offset=best[1])
+    for tag, (p, s) in enumerate(items[:8]):
+        assert eng.add(p, s, tag)
+    done = {}
+    while len(done) < 8:
+        eng.step(8)
+        done.update(eng.poll())
+    eng.close()
+    for tag, (p, s) in enumerate(items[:8]):
+        assert done[tag] == psb.bfs(p, "two_bit", s)["counts"]

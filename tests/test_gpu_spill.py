@@ -1,7 +1,8 @@
 """Frontier spill (psb_bfs_opts.spill): every depth's states, encoded on the
 GPU segment by segment into the reference's compressed segment stream
-(Common/CompressedFrontier.cpp:103-140) and handed over from pinned host
-memory.  Each stream must equal, byte for byte, the oracle's segment stream
+(Common/CompressedFrontier.cpp:103-140; for frontier search the stream with
+each state's operator bits, CompressedFrontierWriter, :56-70) and handed over
+from pinned host memory.  Each stream must equal, byte for byte, the oracle's segment stream
 of that depth's states in that segment (the oracle's distances come from
 orc_depths, pinned to the reference's per-depth counts in test_oracle.py)."""
 import math
@@ -32,19 +33,24 @@ def run_spill(spec, algo, start=0, segment_bits=0, **kw):
     return res, got
 
 
-def expected_streams(dist, depth, segment_bits):
-    """{segment: stream} of the states at `depth`, by the oracle."""
+def expected_streams(dist, depth, segment_bits, nibbles=None):
+    """{segment: stream} of the states at `depth`, by the oracle: the segment
+    stream, or for frontier search (nibbles = each state's operator bits) the
+    stream with operator bits."""
     states = np.nonzero(dist == depth)[0].astype(np.uint64)
     seg = states >> np.uint64(segment_bits)
     out = {}
     for g in np.unique(seg):
-        offs = (states[seg == g] - (g << np.uint64(segment_bits))).astype(np.uint32)
-        out[int(g)] = O.segment_stream(offs)
+        sel = states[seg == g]
+        offs = (sel - (g << np.uint64(segment_bits))).astype(np.uint32)
+        out[int(g)] = (O.segment_stream(offs) if nibbles is None
+                       else O.frontier_stream(offs, nibbles[sel.astype(np.int64)]))
     return out
 
 
 def check(spec, algo, start, segment_bits, res, got):
     dist, n_depths = O.depths(spec, start)
+    nib = O.frontier_nibbles(spec, dist) if algo == "frontier" else None
     assert len(res["counts"]) == n_depths
     sb = segment_bits or 32
     # depths ascending, segments ascending within a depth, every depth present
@@ -53,7 +59,7 @@ def check(spec, algo, start, segment_bits, res, got):
     assert sorted({d for d, _, _, _ in got}) == list(range(n_depths))
     for d in range(n_depths):
         mine = {g: (data, states) for dd, g, data, states in got if dd == d}
-        want = expected_streams(dist, d, sb)
+        want = expected_streams(dist, d, sb, nib)
         assert set(mine) == set(want), (spec, algo, d)
         assert sum(st for _, st in mine.values()) == res["counts"][d]
         for g, stream in want.items():
@@ -110,8 +116,9 @@ def test_spill_with_max_depth(algo):
     assert len(res["counts"]) == 8
     assert sorted({d for d, _, _, _ in got}) == list(range(8))
     dist, _ = O.depths(spec, 0)
+    nib = O.frontier_nibbles(spec, dist) if algo == "frontier" else None
     for d in range(8):
-        want = expected_streams(dist, d, 12)
+        want = expected_streams(dist, d, 12, nib)
         mine = {g: data for dd, g, data, _ in got if dd == d}
         assert mine == want
 
