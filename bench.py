@@ -418,7 +418,7 @@ def profile_once(args):
     sink = psb.SPILL_FN(lambda *_: 0) if args.spill else None
     r = psb.bfs(puzzle, algo, 0, max_depth=args.max_depth, window_bits=args.window_bits, levels=True,
                 direction=args.direction, bottom_up_ratio=args.bottom_up_ratio, spill=sink,
-                segment_bits=args.segment_bits)
+                segment_bits=args.segment_bits, far_marks=args.far_marks)
     out = {"workload": args.workload, "counts": r["counts"], "level_ms": [round(x, 3) for x in r["level_ms"]],
            "level_children": r["level_children"], "stats": r["stats"]}
     print(json.dumps(out), flush=True)
@@ -442,6 +442,8 @@ def main():
                     help="encode every depth's frontier on the GPU (segment streams) and hand it over in pinned"
                          " host memory during the timed searches (default for pancake14-2bit and hanoi18-2bit)")
     ap.add_argument("--no-spill", action="store_true", help="no frontier spill, whatever the workload")
+    ap.add_argument("--far-marks", default="auto", choices=["auto", "none", "near", "all"],
+                    help="two-bit long-range marks (PSB_FAR_*); --autotune picks it for two-bit workloads")
     ap.add_argument("--e2e-calls", type=int, default=5,
                     help="timed calls of the public entry point for `e2e` (at most --steps)")
     ap.add_argument("--segment-bits", type=int, default=0, help="with --spill: 2^bits states per segment (0 = 32)")
@@ -487,9 +489,13 @@ def main():
         from puzzlesearch_b200 import autotune
         args.window_bits, timings = autotune.tune_window_bits(puzzle, algo, 0, direction=args.direction)
         tuning = {"window_bits": args.window_bits, "search_ms": {str(k): round(v, 2) for k, v in timings.items()}}
+        if algo == "two_bit":
+            args.far_marks, ft = autotune.tune_far_marks(puzzle, 0, window_bits=args.window_bits)
+            tuning.update({"far_marks": args.far_marks, "far_marks_ms": {k: round(v, 2) for k, v in ft.items()}})
     stream = torch.cuda.Stream()
     # Session on torch's stream so the CUDA events below bracket exactly the searches.
-    opts = psb._opts(0, args.window_bits, local, stream.cuda_stream, direction=args.direction)
+    opts = psb._opts(0, args.window_bits, local, stream.cuda_stream, direction=args.direction,
+                     far_marks=args.far_marks)
     h = ctypes.c_void_p()
     psb._check(psb.lib().psb_bfs_session_create(puzzle.handle, psb._algo(algo), ctypes.byref(opts), ctypes.byref(h)))
     cap = 1 << 16
@@ -511,7 +517,8 @@ def main():
         st = psb.BfsStats()
         st.struct_size = ctypes.sizeof(psb.BfsStats)
         o = psb._opts(0, 0, local, stream.cuda_stream, direction=args.direction,
-                      bottom_up_ratio=args.bottom_up_ratio, spill=spill_fn, segment_bits=args.segment_bits)
+                      bottom_up_ratio=args.bottom_up_ratio, spill=spill_fn, segment_bits=args.segment_bits,
+                      far_marks=args.far_marks)
         psb._check(psb.lib().psb_bfs_session_run(h, 0, ctypes.byref(o), counts, cap, ctypes.byref(nd), ctypes.byref(st)))
         return list(counts[:nd.value]), st
 
@@ -546,7 +553,8 @@ def main():
     e2e_calls = max(1, min(args.steps, args.e2e_calls))
     for _ in range(1):
         psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
-                spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits)
+                spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits,
+                far_marks=args.far_marks)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -555,7 +563,8 @@ def main():
     for _ in range(e2e_calls):
         tc = time.perf_counter()
         r = psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
-                    spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits)
+                    spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits,
+                far_marks=args.far_marks)
         calls.append(time.perf_counter() - tc)
         assert r["counts"] == ref_counts
         levels = r["stats"]["levels"]

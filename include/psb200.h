@@ -114,6 +114,20 @@ int psb_expand(const psb_puzzle* p, const uint64_t* parents, const uint32_t* opb
 typedef int (*psb_spill_fn)(void* user, uint32_t depth, uint32_t segment, const uint8_t* stream, uint64_t bytes,
                             uint64_t states);
 
+/* Long-range marks of a two-bit level (children outside the thread block's
+ * window).  PSB_FAR_NONE: read the target's code, then OR NEXT into it if it
+ * is UNVISITED (InMemoryTwoBitBFS.cpp:44-49 per child).  PSB_FAR_NEAR: marks
+ * whose target lies in the parent's aligned block of 12! states (pancake
+ * flips up to 12; every long-range mark of the other puzzles) set a bit in a
+ * 1-bit-per-state far bitmap, folded into the codes after the level; the
+ * flips of more than 12 read first.  PSB_FAR_ALL: every long-range mark goes
+ * to the far bitmap.  PSB_FAR_AUTO picks by measurement on B200: ALL for
+ * pancake up to 13, NEAR for 14 and more and for sliding tiles, NONE for
+ * Hanoi (its marks are local; the fold would not pay).  NEAR and ALL hold the
+ * bitmap (N/8 bytes) in device memory; without room for it the search runs
+ * as NONE. */
+enum { PSB_FAR_AUTO = 0, PSB_FAR_NONE = 1, PSB_FAR_NEAR = 2, PSB_FAR_ALL = 3 };
+
 typedef struct {
     uint32_t struct_size;  /* sizeof(psb_bfs_opts) */
     uint32_t max_depth;    /* stop after this depth (0 = until the frontier is empty; PuzzleOptions::maxSteps, Common/DiskBasedBFS.h:10) */
@@ -131,6 +145,12 @@ typedef struct {
     void* spill_user;      /* first argument of spill */
     int32_t segment_bits;  /* states per spilled segment = 2^segment_bits, 6..32 (0 = 32, the default of
                               PuzzleOptions::segmentBits, Common/DiskBasedBFS.h:11) */
+    int32_t far_marks;     /* PSB_TWO_BIT top-down levels: where long-range marks go (PSB_FAR_*) */
+    uint64_t* restored_counts; /* optional, counts_cap entries; 4-peg Hanoi with symmetry and PSB_TWO_BIT only:
+                              the counts HanoiSearch reports (HanoiTowers/HanoiSearch.cpp:247-262), i.e. each
+                              depth's canonical states weighted by their class size (PegsMult,
+                              HanoiTowers/HanoiTowers.h:48-55) = the per-depth counts of the search without
+                              symmetry; entry 0 is 1 */
 } psb_bfs_opts;
 
 /* With opts->spill set, the states at each depth d = 0, 1, ... (every depth
@@ -288,6 +308,38 @@ int psb_frontier_decode(const uint8_t* d_stream, const psb_codec_block* blocks, 
 int psb_opbits_encode(int bits, const uint8_t* d_op_bits, uint64_t count, uint8_t* d_out, void* stream);
 int psb_opbits_decode(int bits, const uint8_t* d_in, uint64_t count, uint8_t* d_op_bits, void* stream);
 
+/* --- Segmented (out-of-core) search -------------------------------------------
+ * The reference's disk-based search, DiskBasedOptThreeBitBFS
+ * (Common/DiskBasedOptThreeBitBFS.cpp:12-252), with host memory in place of
+ * its segment files: the state space is split into segments of
+ * 2^segment_bits states (SegmentedOptions::GetSegIdx, Common/DiskBasedBFS.h:
+ * 22-24) and only one segment's three bit arrays (3 x 2^segment_bits bits)
+ * plus an expansion buffer sit in device memory.  Every segment's last three
+ * frontier layers are kept in host memory as the reference's compressed
+ * segment streams, and the children a segment's states have in other
+ * segments as 4-byte offsets per target segment.  Per-depth counts equal the
+ * in-memory searches'.  A search larger than device memory runs this way;
+ * PCIe carries the layers and the cross-segment children. */
+typedef struct {
+    uint32_t struct_size;   /* sizeof(psb_segmented_opts) */
+    uint32_t max_depth;     /* stop after this depth (0 = until the frontier is empty) */
+    int32_t segment_bits;   /* 10..32 (0 = 32, PuzzleOptions::segmentBits' default) */
+    int32_t device;         /* CUDA device (-1 = current) */
+    uint64_t chunk_states;  /* states expanded per launch (bounds the child buffer; 0 = 2^22) */
+} psb_segmented_opts;
+typedef struct {
+    uint32_t struct_size;     /* sizeof(psb_segmented_stats) */
+    uint32_t pad;
+    uint64_t segments;        /* segments of the state space */
+    uint64_t device_bytes;    /* device memory the search held */
+    uint64_t peak_host_bytes; /* largest host memory held by layers and cross-segment children */
+    uint64_t h2d_bytes, d2h_bytes;
+    uint64_t cross_children;  /* children that landed in another segment than their parent's */
+    double total_ms;          /* wall time of the call */
+} psb_segmented_stats;
+int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial_index, const psb_segmented_opts* opts,
+                      uint64_t* depth_counts, uint32_t counts_cap, uint32_t* n_depths, psb_segmented_stats* stats);
+
 /* --- Batched and served solves -----------------------------------------------
  * No single counterpart in the reference (one InMemoryTwoBitBFS per call).
  * An engine keeps many independent two-bit searches on the GPU at once, each
@@ -329,18 +381,26 @@ int psb_engine_poll(psb_engine* e, uint64_t* tags, uint32_t* n_depths, uint64_t*
 int psb_engine_info(psb_engine* e, uint32_t* active, uint64_t* largest_free_bytes, uint64_t* levels_run);
 
 /* --- Solve server (continuous batching) -------------------------------------
- * No counterpart in the reference.  A server thread owns a psb_engine: it
- * admits submitted requests first come first served while a slot and pool
- * space are free (admission by HBM footprint), advances all resident searches
- * one level per step, and completes each with its per-depth counts, its
- * eccentricity (n_depths - 1) and its latency from submission.  Submit and
- * poll are non-blocking and may be called from any thread. */
+ * No counterpart in the reference.  Two lanes share the GPU:
+ *   * the batch lane: a server thread owns a psb_engine; it admits submitted
+ *     requests smallest first while a slot and pool space are free
+ *     (admission by HBM footprint) and advances all resident searches
+ *     together, level by level (continuous batching);
+ *   * the large lane: requests with more than large_states states run one at
+ *     a time as single two-bit searches (psb_bfs sessions, one per puzzle
+ *     size, reused) on a second thread and stream, overlapping the batch
+ *     lane's steps on the device.  A large search's levels would otherwise
+ *     set the pace of every small search resident with it.
+ * Each request completes with its per-depth counts, its eccentricity
+ * (n_depths - 1) and its latency from submission.  Submit and poll are
+ * non-blocking and may be called from any thread. */
 typedef struct psb_server psb_server;
 typedef struct {
     uint32_t struct_size;     /* sizeof(psb_server_opts) */
     uint32_t levels_per_step; /* BFS levels per engine step while no request waits for admission (0 = 1); one
                                  level per step while requests wait */
     psb_engine_opts engine;
+    uint64_t large_states;    /* requests with more states go to the large lane (0 = 2^26; UINT64_MAX = none) */
 } psb_server_opts;
 int psb_server_start(const psb_server_opts* opts, psb_server** out);
 int psb_server_submit(psb_server* s, int kind, int a, int b, uint64_t initial_index, uint64_t* ticket);

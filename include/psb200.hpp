@@ -15,6 +15,10 @@
 //   FourPegHanoiGPU             Puzzles/FourPegHanoiGPU.h:8-22
 //   InMemoryClassicBFS, InMemoryTwoBitBFS, InMemoryThreeBitBFS,
 //   InMemoryFrontierSearch      Common/InMemoryBFS.h:5-11
+//   StoreOptions, PuzzleOptions, DiskBased*BFS / *FrontierSearch
+//                               Common/Store.h:18-28, Common/DiskBasedBFS.h:9-46
+//   HanoiTowers<size>, SearchOptions, HanoiSearch<size>
+//                               HanoiTowers/HanoiTowers.h:9-70, HanoiSearch.h:9-18
 // so the reference's tests and drivers compile against it by swapping
 // includes.  The names live in namespace psb200; define
 // PSB200_GLOBAL_NAMES before including to also declare them in the global
@@ -41,6 +45,7 @@
 #include <iostream>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "psb200.h"
@@ -318,6 +323,117 @@ private:
     std::vector<int> ops_, child_ops_;
 };
 
+// StoreOptions (Common/Store.h:18-28) and PuzzleOptions (Common/DiskBasedBFS.h:
+// 9-14).  The segmented searches keep their segment data in host memory:
+// directories and filesPerPath are accepted and unused, and so is threads
+// (the GPU runs each segment's work); segmentBits and maxSteps apply.
+struct StoreOptions {
+    std::vector<std::string> directories = {"."};
+    int filesPerPath = 5;
+};
+struct PuzzleOptions {
+    size_t maxSteps = 10000;
+    int segmentBits = 32;
+    int threads = 1;
+    StoreOptions storeOptions;
+};
+
+// The reference's disk-based searches (Common/DiskBasedBFS.h:40-46) all
+// return the per-depth counts of the whole space; here each is the segmented
+// out-of-core search of psb_bfs_segmented (one segment's arrays on the
+// device at a time, DiskBasedOptThreeBitBFS's three-layer scheme).
+inline std::vector<uint64_t> RunSegmented(Puzzle& puzzle, const std::string& initialState, const PuzzleOptions& opts) {
+    if (!puzzle.handle())
+        throw Error(PSB_ERR_UNSUPPORTED, "psb200: the segmented searches run on the GPU for this library's puzzle "
+                                         "classes only; '" + puzzle.Name() + "' has no device expander");
+    const uint64_t init = puzzle.Parse(initialState);
+    psb_segmented_opts o{};
+    o.struct_size = sizeof(psb_segmented_opts);
+    o.segment_bits = opts.segmentBits;
+    o.device = -1;
+    o.max_depth = opts.maxSteps < 10000 ? uint32_t(opts.maxSteps) : 0;
+    std::vector<uint64_t> counts(1 << 16);
+    uint32_t n = 0;
+    check(psb_bfs_segmented(puzzle.handle(), init, &o, counts.data(), uint32_t(counts.size()), &n, nullptr));
+    counts.resize(n);
+    return counts;
+}
+inline std::vector<uint64_t> DiskBasedClassicBFS(Puzzle& puzzle, std::string initialState, PuzzleOptions opts = {}) {
+    return RunSegmented(puzzle, initialState, opts);
+}
+inline std::vector<uint64_t> DiskBasedTwoBitBFS(Puzzle& puzzle, std::string initialState, PuzzleOptions opts = {}) {
+    return RunSegmented(puzzle, initialState, opts);
+}
+inline std::vector<uint64_t> DiskBasedThreeBitBFS(Puzzle& puzzle, std::string initialState, PuzzleOptions opts = {}) {
+    return RunSegmented(puzzle, initialState, opts);
+}
+inline std::vector<uint64_t> DiskBasedFrontierSearch(Puzzle& puzzle, std::string initialState,
+                                                     PuzzleOptions opts = {}) {
+    return RunSegmented(puzzle, initialState, opts);
+}
+inline std::vector<uint64_t> DiskBasedOptFrontierSearch(Puzzle& puzzle, std::string initialState,
+                                                        PuzzleOptions opts = {}) {
+    return RunSegmented(puzzle, initialState, opts);
+}
+inline std::vector<uint64_t> DiskBasedOptThreeBitBFS(Puzzle& puzzle, std::string initialState,
+                                                     PuzzleOptions opts = {}) {
+    return RunSegmented(puzzle, initialState, opts);
+}
+inline std::vector<uint64_t> DiskBasedOptThreeBitBFS2(Puzzle& puzzle, std::string initialState,
+                                                      PuzzleOptions opts = {}) {
+    return RunSegmented(puzzle, initialState, opts);
+}
+
+// HanoiTowers<size> (HanoiTowers/HanoiTowers.h:9-70): the index space of the
+// reference's symmetric 4-peg Hanoi search: 2 bits per disk, the same layout
+// and ToString/Parse format as FourPegHanoiSimple.
+template <int size>
+class HanoiTowers {
+public:
+    static constexpr int Size = size;
+    static uint64_t IndexesCount() { return uint64_t(1) << (size * 2); }
+    static int MaxSegments() { return int((IndexesCount() + 0xFFFFFFFFull) >> 32); }
+    static std::string ToString(uint64_t index) { return FourPegHanoiSimple(size, true).ToString(index); }
+    static uint64_t Parse(std::string state) { return FourPegHanoiSimple(size, true).Parse(state); }
+    static std::pair<int, uint32_t> SplitIndex(uint64_t index) { return {int(index >> 32), uint32_t(index)}; }
+    // Size of the symmetry class of a canonical state (pegs 1..3 ordered by
+    // their bottom disk): 6 with disks on pegs 1 and 2, 3 with disks on peg 1 only.
+    static int PegsMult(uint64_t index) {
+        const uint64_t even = 0x5555555555555555ull, hi = index >> 1, lo = index;
+        const uint64_t pegs1 = ~hi & lo & even, pegs2 = hi & ~lo & even;
+        return 6 - int(pegs2 == 0) * 3 - int(pegs1 == 0);
+    }
+};
+
+// SearchOptions (HanoiTowers/HanoiSearch.h:9-13).  The search runs in device
+// memory: threads and directories (the reference's disk stores) are accepted
+// and unused; maxSteps bounds the depth.
+struct SearchOptions {
+    int maxSteps = 1000000;
+    int threads = 4;
+    std::vector<std::string> directories = {"."};
+};
+
+// HanoiSearch<size> (HanoiTowers/HanoiSearch.cpp:204-290): BFS over the
+// symmetric 4-peg Hanoi space from initialState; entry d is the number of
+// states at depth d of the full (unreduced) space: each canonical state
+// counts PegsMult times, depth 0 counts 1.  A two-bit search on the GPU.
+template <int size>
+std::vector<uint64_t> HanoiSearch(std::string initialState, SearchOptions options = {}) {
+    FourPegHanoiSimple puzzle(size, true);
+    const uint64_t init = puzzle.Parse(initialState);
+    std::vector<uint64_t> counts(1 << 16), restored(1 << 16);
+    psb_bfs_opts o{};
+    o.struct_size = sizeof(psb_bfs_opts);
+    o.device = -1;
+    o.max_depth = options.maxSteps > 0 && options.maxSteps < 1000000 ? uint32_t(options.maxSteps) : 0;
+    o.restored_counts = restored.data();
+    uint32_t n = 0;
+    check(psb_bfs(puzzle.handle(), PSB_TWO_BIT, init, &o, counts.data(), uint32_t(counts.size()), &n, nullptr));
+    restored.resize(n);
+    return restored;
+}
+
 // In-memory searches (Common/InMemoryBFS.h:5-11): the whole search runs on
 // the GPU with the bit arrays resident in device memory; the result is the
 // number of states at each depth, element 0 = 1 (the initial state).
@@ -351,16 +467,28 @@ inline std::vector<uint64_t> InMemoryFrontierSearch(Puzzle& puzzle, std::string 
 
 #ifdef PSB200_GLOBAL_NAMES
 using psb200::Buffer;
+using psb200::DiskBasedClassicBFS;
+using psb200::DiskBasedFrontierSearch;
+using psb200::DiskBasedOptFrontierSearch;
+using psb200::DiskBasedOptThreeBitBFS;
+using psb200::DiskBasedOptThreeBitBFS2;
+using psb200::DiskBasedThreeBitBFS;
+using psb200::DiskBasedTwoBitBFS;
 using psb200::ExpandBuffer;
 using psb200::ExpandHint;
 using psb200::FourPegHanoiGPU;
 using psb200::FourPegHanoiSimple;
+using psb200::HanoiSearch;
+using psb200::HanoiTowers;
 using psb200::InMemoryClassicBFS;
 using psb200::InMemoryFrontierSearch;
 using psb200::InMemoryThreeBitBFS;
 using psb200::InMemoryTwoBitBFS;
 using psb200::PancakeSimple;
 using psb200::Puzzle;
+using psb200::PuzzleOptions;
+using psb200::SearchOptions;
 using psb200::SlidingTilePuzzleGpu;
 using psb200::SlidingTilePuzzleSimple;
+using psb200::StoreOptions;
 #endif

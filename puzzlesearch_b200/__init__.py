@@ -17,7 +17,7 @@ import os
 __all__ = [
     "PsbError", "lib", "SlidingTilePuzzleSimple", "PancakeSimple", "FourPegHanoiSimple",
     "InMemoryTwoBitBFS", "InMemoryThreeBitBFS", "InMemoryFrontierSearch", "InMemoryClassicBFS",
-    "bfs", "BfsSession", "TWO_BIT", "THREE_BIT", "FRONTIER", "CLASSIC", "INVALID_INDEX",
+    "bfs", "bfs_segmented", "BfsSession", "TWO_BIT", "THREE_BIT", "FRONTIER", "CLASSIC", "INVALID_INDEX",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -50,7 +50,8 @@ class BfsOpts(ctypes.Structure):
                 ("stream", ctypes.c_void_p), ("final_words", u64p), ("final_cap", ctypes.c_uint64),
                 ("level_ms", ctypes.POINTER(ctypes.c_float)), ("level_children", u64p),
                 ("direction", ctypes.c_int32), ("bottom_up_ratio", ctypes.c_float),
-                ("spill", SPILL_FN), ("spill_user", ctypes.c_void_p), ("segment_bits", ctypes.c_int32)]
+                ("spill", SPILL_FN), ("spill_user", ctypes.c_void_p), ("segment_bits", ctypes.c_int32),
+                ("far_marks", ctypes.c_int32), ("restored_counts", u64p)]
 
 
 class BfsStats(ctypes.Structure):
@@ -77,7 +78,20 @@ class EngineOpts(ctypes.Structure):
 
 
 class ServerOpts(ctypes.Structure):
-    _fields_ = [("struct_size", ctypes.c_uint32), ("levels_per_step", ctypes.c_uint32), ("engine", EngineOpts)]
+    _fields_ = [("struct_size", ctypes.c_uint32), ("levels_per_step", ctypes.c_uint32), ("engine", EngineOpts),
+                ("large_states", ctypes.c_uint64)]
+
+
+class SegmentedOpts(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("segment_bits", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("chunk_states", ctypes.c_uint64)]
+
+
+class SegmentedStats(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("segments", ctypes.c_uint64),
+                ("device_bytes", ctypes.c_uint64), ("peak_host_bytes", ctypes.c_uint64),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("cross_children", ctypes.c_uint64),
+                ("total_ms", ctypes.c_double)]
 
 
 class CodecBlock(ctypes.Structure):
@@ -134,6 +148,8 @@ def lib():
                                         ctypes.c_void_p]
         L.psb_opbits_decode.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                         ctypes.c_void_p]
+        L.psb_bfs_segmented.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(SegmentedOpts), u64p, ctypes.c_uint32,
+                                        u32p, ctypes.POINTER(SegmentedStats)]
         L.psb_engine_create.argtypes = [ctypes.POINTER(EngineOpts), ctypes.POINTER(P)]
         L.psb_engine_destroy.argtypes = [P]
         L.psb_engine_footprint.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, u64p]
@@ -336,9 +352,13 @@ def _check_call(call):
     _check(call())
 
 
+FAR_MARKS = {"auto": 0, "none": 1, "near": 2, "all": 3}
+
+
 def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_ms=None, level_children=None,
-          direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0):
+          direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0, far_marks="auto"):
     o = BfsOpts()
+    o.far_marks = FAR_MARKS[far_marks] if isinstance(far_marks, str) else int(far_marks)
     if spill is not None:
         o.spill = spill  # a SPILL_FN the caller keeps alive for the call
         o.segment_bits = segment_bits
@@ -360,14 +380,18 @@ def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_
 
 
 def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels=False, device=-1,
-        direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0):
+        direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0, restored=False, far_marks="auto"):
     """Runs psb_bfs.  Returns a dict with counts, stats and optionally the final
     arrays (list of 64-bit words in the reference's layout) and per-level data.
     direction: "auto", "top_down" or "bottom_up" (PSB_DIR_*).
     spill: optional callable(depth, segment, stream_bytes, states) receiving
     every depth's frontier as compressed segment streams (2^segment_bits
     states per segment, 0 = 2^32); a truthy return stops the search.  A
-    SPILL_FN is passed through as is (it sees the pinned buffer itself)."""
+    SPILL_FN is passed through as is (it sees the pinned buffer itself).
+    far_marks: two-bit long-range marks, "auto", "none", "near" or "all" (PSB_FAR_*).
+    restored: 4-peg Hanoi with symmetry, two-bit: also return "restored", the
+    per-depth counts weighted by each canonical state's class size
+    (HanoiSearch's result)."""
     if isinstance(initial, str):
         initial = puzzle.Parse(initial)
     cap = 1 << 16
@@ -379,7 +403,11 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
     lm = (ctypes.c_float * cap)() if levels else None
     lc = (ctypes.c_uint64 * cap)() if levels else None
     fn, runner = _spill_fn(spill)
-    o = _opts(max_depth, window_bits, device, None, fin, lm, lc, direction, bottom_up_ratio, fn, segment_bits)
+    o = _opts(max_depth, window_bits, device, None, fin, lm, lc, direction, bottom_up_ratio, fn, segment_bits,
+              far_marks)
+    rc = (ctypes.c_uint64 * cap)() if restored else None
+    if restored:
+        o.restored_counts = ctypes.cast(rc, u64p)
     st = BfsStats()
     st.struct_size = ctypes.sizeof(BfsStats)
     runner(lambda: lib().psb_bfs(puzzle.handle, _algo(algo), initial, ctypes.byref(o), counts, cap,
@@ -390,7 +418,26 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
     if levels:
         out["level_ms"] = list(lm[:nd.value])
         out["level_children"] = list(lc[:nd.value])
+    if restored:
+        out["restored"] = list(rc[:nd.value])
     return out
+
+
+def bfs_segmented(puzzle, initial=0, segment_bits=0, max_depth=0, chunk_states=0, device=-1):
+    """psb_bfs_segmented: the out-of-core three-layer search (one segment's
+    bit arrays on the device at a time).  Returns {"counts", "stats"}."""
+    if isinstance(initial, str):
+        initial = puzzle.Parse(initial)
+    cap = 1 << 16
+    counts = (ctypes.c_uint64 * cap)()
+    nd = ctypes.c_uint32()
+    o = SegmentedOpts(ctypes.sizeof(SegmentedOpts), max_depth, segment_bits, device, chunk_states)
+    st = SegmentedStats()
+    st.struct_size = ctypes.sizeof(SegmentedStats)
+    _check(lib().psb_bfs_segmented(puzzle.handle, initial, ctypes.byref(o), counts, cap, ctypes.byref(nd),
+                                   ctypes.byref(st)))
+    return {"counts": list(counts[:nd.value]),
+            "stats": {k: getattr(st, k) for k, _ in SegmentedStats._fields_ if k not in ("struct_size", "pad")}}
 
 
 class BfsSession:
@@ -501,9 +548,12 @@ class Server:
     """psb_server: a solve server with continuous batching on one GPU."""
 
     def __init__(self, max_instances=1024, max_depths=256, pool_bytes=16 << 30, levels_per_step=1, device=-1,
-                 blocks_per_sm=0, window_bits_offset=0):
+                 blocks_per_sm=0, window_bits_offset=0, large_states=0):
+        """large_states: requests with more states run in the large lane (0 =
+        the library's default, None = no large lane)."""
         o = ServerOpts()
         o.struct_size = ctypes.sizeof(ServerOpts)
+        o.large_states = (1 << 64) - 1 if large_states is None else large_states
         o.levels_per_step = levels_per_step
         e = o.engine
         e.struct_size = ctypes.sizeof(EngineOpts)

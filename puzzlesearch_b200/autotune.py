@@ -1,8 +1,9 @@
-"""Autotuner for the launch shapes that are picked by measurement rather than
-by rule: the batch engine's persistent grid (blocks per SM) and its
-instances' window size, and the window of a single search's level kernel
-(states per thread-block window, the unit of work the kernel sweeps and
-marks in shared memory).
+"""Autotuner for the launch shapes and strategies that are picked by
+measurement rather than by rule: the batch engine's persistent grid (blocks
+per SM) and its instances' window size; the window of a single search's
+level kernel (states per thread-block window, the unit of work the kernel
+sweeps and marks in shared memory); and where a two-bit search's long-range
+marks go (PSB_FAR_*).
 
 Each candidate runs the same workload on this device.  The tuner checks that
 every candidate gives the same results, and returns the fastest one with all
@@ -15,7 +16,7 @@ import time
 
 from . import Engine, bfs, device_name, lib
 
-__all__ = ["tune", "tune_engine", "tune_window_bits", "Cache"]
+__all__ = ["tune", "tune_engine", "tune_window_bits", "tune_far_marks", "Cache"]
 
 
 def tune(candidates, measure):
@@ -110,6 +111,26 @@ def tune_window_bits(puzzle, algo, initial=0, candidates=None, direction="auto",
 
     def measure(wb):
         r = bfs(puzzle, algo, initial, window_bits=wb, direction=direction)
+        return r["stats"]["total_ms"], r["counts"]
+
+    best, timings = tune(candidates, measure)
+    if cache and key:
+        cache.put(dev, key, best)
+    return best, timings
+
+
+def tune_far_marks(puzzle, initial=0, candidates=("none", "near", "all"), window_bits=0, cache=None, key=None):
+    """Where a two-bit search's long-range marks go (PSB_FAR_*: read the
+    target's code first, or a far bitmap folded after each level, for the
+    near marks only or for all of them), timed as the device time of the
+    whole search.  Returns (best, {mode: ms})."""
+    dev = device_name()
+    if cache and key and cache.get(dev, key) is not None:
+        return cache.get(dev, key), {}
+    bfs(puzzle, "two_bit", initial, window_bits=window_bits, far_marks=candidates[-1])  # warm-up (pool growth)
+
+    def measure(mode):
+        r = bfs(puzzle, "two_bit", initial, window_bits=window_bits, far_marks=mode)
         return r["stats"]["total_ms"], r["counts"]
 
     best, timings = tune(candidates, measure)

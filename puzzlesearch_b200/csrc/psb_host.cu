@@ -224,7 +224,9 @@ __device__ __forceinline__ uint32_t fold_quad(ulonglong2* __restrict__ codes, ui
 }
 __global__ void __launch_bounds__(kThreads) fold_two_bit(ulonglong2* __restrict__ codes, uint4* __restrict__ far,
                                                         uint64_t n4, uint32_t next_lo,
+                                                        const unsigned long long* far_marks,
                                                         unsigned long long* count) {
+    if (*far_marks == 0) return;  // the level made no far mark: the bitmap is clear
     uint32_t c = 0;
     for (uint64_t i = blockIdx.x * uint64_t(kThreads) + threadIdx.x; i < n4; i += uint64_t(gridDim.x) * kThreads)
         c += fold_quad(codes, far, i, next_lo);
@@ -237,7 +239,10 @@ __global__ void __launch_bounds__(kThreads) fold_two_bit_flagged(ulonglong2* __r
                                                                 uint4* __restrict__ far, uint64_t n4,
                                                                 const uint8_t* __restrict__ flags,
                                                                 uint64_t n_windows, uint32_t quads,
-                                                                uint32_t next_lo, unsigned long long* count) {
+                                                                uint32_t next_lo,
+                                                                const unsigned long long* far_marks,
+                                                                unsigned long long* count) {
+    if (*far_marks == 0) return;
     uint32_t c = 0;
     for (uint64_t w = blockIdx.x; w < n_windows; w += gridDim.x) {
         if (!flags[w]) continue;
@@ -803,6 +808,19 @@ int layout(const psb_puzzle* p, int algo, uint64_t* words, int* n_arr) {
 // Default switch ratio of PSB_DIR_AUTO (unvisited < ratio x frontier).
 constexpr double kBottomUpRatio = 1.0;
 
+// PSB_FAR_AUTO's pick (measured on B200, two-bit, full searches):
+//   13-pancake: ALL 241 ms, NEAR 254 ms, NONE 265 ms;
+//   14-pancake: NEAR 4.18 s, NONE 4.45 s, ALL 4.73 s (its flips of 13 and 14
+//   land anywhere in a 10.9 GB bitmap; read-first keeps them read-only);
+//   18-disk Hanoi: NONE 1.58 s, ALL 1.84 s (0.3% of its marks are long-range).
+int far_mode(const psb_puzzle* p, int algo, int requested) {
+    if (algo != PSB_TWO_BIT) return PSB_FAR_NONE;
+    if (requested >= PSB_FAR_NONE && requested <= PSB_FAR_ALL) return requested;
+    if (p->kind == PSB_HANOI4) return PSB_FAR_NONE;
+    if (p->kind == PSB_PANCAKE && p->n_states <= 6227020800ull) return PSB_FAR_ALL;
+    return PSB_FAR_NEAR;
+}
+
 bool supports_bottom_up(const psb_puzzle* p, int algo) {
     if (algo != PSB_THREE_BIT && algo != PSB_TWO_BIT && algo != PSB_CLASSIC) return false;
     return !(p->kind == PSB_HANOI4 && p->pz.sym);
@@ -1007,6 +1025,10 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     if (initial >= N) return fail(PSB_ERR_ARG, "initial index %llu >= IndexesCount()", (unsigned long long)initial);
     if (!counts || !n_depths || cap == 0) return fail(PSB_ERR_ARG, "counts buffer missing");
     const uint32_t max_depth = opts ? opts->max_depth : 0;
+    uint64_t* restored = opts ? opts->restored_counts : nullptr;
+    const int far_marks = S->far ? far_mode(&P, S->algo, opts ? opts->far_marks : PSB_FAR_AUTO) : PSB_FAR_NONE;
+    if (restored && !(P.kind == PSB_HANOI4 && P.pz.sym && S->algo == PSB_TWO_BIT))
+        return fail(PSB_ERR_UNSUPPORTED, "restored_counts: 4-peg Hanoi with symmetry, two-bit searches only");
     const bool spill = opts && opts->spill;
     if (spill && opts->segment_bits && (opts->segment_bits < 6 || opts->segment_bits > 32))
         return fail(PSB_ERR_ARG, "segment_bits %d outside 6..32", opts->segment_bits);
@@ -1020,7 +1042,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     if (S->device >= 0) PSB_CUDA(cudaSetDevice(S->device));
     for (int i = 0; i < S->n_arr; i++) PSB_CUDA(cudaMemsetAsync(S->arr[i], 0, S->words[i] * 8, s));
     if (S->visited) PSB_CUDA(cudaMemsetAsync(S->visited, 0, S->words[0] * 8, s));
-    if (S->far) PSB_CUDA(cudaMemsetAsync(S->far, 0, S->far_words * 8, s));
+    if (S->far && far_marks != PSB_FAR_NONE) PSB_CUDA(cudaMemsetAsync(S->far, 0, S->far_words * 8, s));
     PSB_CUDA(cudaEventRecord(S->ev[0], s));
     const int direction = opts ? opts->direction : PSB_DIR_AUTO;
     const double bu_ratio = (opts && opts->bottom_up_ratio > 0) ? double(opts->bottom_up_ratio) : kBottomUpRatio;
@@ -1043,6 +1065,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     a.odd = P.odd;
     a.pz = P.pz;
     a.stats = S->d_stats;
+    a.sym_mult = restored ? 1 : 0;
 
     uint64_t *old_ = S->arr[0], *cur = S->arr[1], *nw = S->arr[2];       // three-bit
     uint64_t *closed = S->arr[0], *open = S->arr[1], *nopen = S->arr[2]; // classic
@@ -1155,7 +1178,8 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             case PSB_CLASSIC: a.front = open; a.marks = nopen; a.front_words = W1; a.mark_words = W1; break;
             case PSB_TWO_BIT:
                 a.front = codes; a.marks = codes; a.front_words = W2; a.mark_words = W2; a.cur_code = cur_code;
-                a.far = S->far;
+                a.far = far_marks != PSB_FAR_NONE ? S->far : nullptr;
+                a.far_all = far_marks == PSB_FAR_ALL ? 1 : 0;
                 break;
             case PSB_FRONTIER:
                 a.front = fcur; a.marks = fnext; a.excl_cur = cex; a.excl_next = nex;
@@ -1203,17 +1227,18 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             psb::retire_two_bit<<<148 * 8, psb::kThreads, 0, s>>>(reinterpret_cast<ulonglong2*>(codes), (W2 + 1) / 2,
                                                                  cur_code, S->d_stats + 4);
             PSB_CUDA(cudaGetLastError());
-        } else if (S->algo == PSB_TWO_BIT && S->far) {
+        } else if (S->algo == PSB_TWO_BIT && S->far && far_marks != PSB_FAR_NONE) {
             const uint64_t n4 = (W2 + 3) / 4;
             const uint32_t next_lo = cur_code == 2 ? 1u : 0u;  // NEXT = 5 - CUR
             if (produce)
                 psb::fold_two_bit_flagged<<<148 * 8, psb::kThreads, 0, s>>>(
                     reinterpret_cast<ulonglong2*>(codes), reinterpret_cast<uint4*>(S->far), n4, S->wflags[flags_next],
-                    S->n_windows, uint32_t((uint64_t(1) << S->window_bits) / 128), next_lo, S->d_stats + 5);
+                    S->n_windows, uint32_t((uint64_t(1) << S->window_bits) / 128), next_lo, S->d_stats + 6,
+                    S->d_stats + 5);
             else
                 psb::fold_two_bit<<<148 * 8, psb::kThreads, 0, s>>>(reinterpret_cast<ulonglong2*>(codes),
                                                                    reinterpret_cast<uint4*>(S->far), n4, next_lo,
-                                                                   S->d_stats + 5);
+                                                                   S->d_stats + 6, S->d_stats + 5);
             PSB_CUDA(cudaGetLastError());
         }
         PSB_CUDA(cudaEventRecord(S->ev[3], s));
@@ -1252,6 +1277,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
         case PSB_TWO_BIT:
             count = bu ? S->h_stats[4] : S->h_stats[0];  // states with code CUR = states at this depth
             if (count == 0) goto done;
+            if (restored && res.size() < cap) restored[res.size()] = res.empty() ? 1 : S->h_stats[7];
             res.push_back(count);
             cur_code = 5 - cur_code;
             break;
@@ -1350,7 +1376,7 @@ int psb_bfs_footprint(const psb_puzzle* p, int algo, uint64_t* bytes) {
     if (int rc = layout(p, algo, w, &n)) return rc;
     *bytes = (w[0] + w[1] + w[2] + w[3]) * 8 + 64;
     if (algo == PSB_THREE_BIT && supports_bottom_up(p, algo)) *bytes += w[0] * 8;  // visited array
-    if (algo == PSB_TWO_BIT) *bytes += padded(words_for(p->n_states)) * 8;           // far bitmap
+    if (far_mode(p, algo, PSB_FAR_AUTO) != PSB_FAR_NONE) *bytes += padded(words_for(p->n_states)) * 8;  // far bitmap
     return PSB_OK;
 }
 
@@ -1391,7 +1417,7 @@ int psb_bfs_session_create(const psb_puzzle* p, int algo, const psb_bfs_opts* op
             cudaGetLastError();  // an allocation failure is not sticky; clear it
         }
     }
-    if (algo == PSB_TWO_BIT) {
+    if (far_mode(p, algo, opts ? opts->far_marks : PSB_FAR_AUTO) != PSB_FAR_NONE) {
         // Optional as well: without room for the far bitmap every long-range
         // mark reads the target's code first.
         void* v = nullptr;

@@ -83,6 +83,7 @@ struct PancakeK {
     static constexpr bool kFlip3Op1 = N >= 3;  // operator 1 permutes each aligned block of 6 (see flip3_push)
     static constexpr bool kFlip4Op2 = N >= 4;  // operator 2 permutes each aligned block of 24 (see flip4_pull)
     static constexpr bool kChunkPrefix = true;
+    static constexpr bool kSymMult = false;
     static constexpr uint32_t kBlock = Pancake<N>::kBlock;
     using Prefix = typename Pancake<N>::Prefix;
     __device__ __forceinline__ static void make_prefix(uint32_t q, Prefix& P) { Pancake<N>::make_prefix(q, P); }
@@ -117,6 +118,7 @@ struct SlidingK {
     static constexpr bool kFlip3Op1 = false;
     static constexpr bool kFlip4Op2 = false;
     static constexpr bool kChunkPrefix = false;
+    static constexpr bool kSymMult = false;
     static constexpr uint32_t kBlock = 1;
     struct Prefix { uint32_t unused; };
     template <bool kOpBits, class E>
@@ -136,6 +138,18 @@ struct HanoiK {
     static constexpr bool kFlip3Op1 = false;
     static constexpr bool kFlip4Op2 = false;
     static constexpr bool kChunkPrefix = false;
+    // With symmetry the index space holds one state per class of peg 1-3
+    // permutations (pegs 1..3 ordered by their bottom disk).  The class size
+    // is HanoiTowers::PegsMult (HanoiTowers/HanoiTowers.h:48-55): 6 when
+    // pegs 1 and 2 hold disks, 3 when only peg 1 does (peg 1 empty leaves
+    // only the all-on-peg-0 state, whose depth 0 the search counts as 1).
+    static constexpr bool kSymMult = true;
+    __device__ __forceinline__ static uint32_t sym_mult(uint64_t i) {
+        const uint64_t hi = i >> 1, lo = i;
+        const uint64_t peg1 = ~hi & lo & kEvenBits, peg2 = hi & ~lo & kEvenBits;
+        return 6u - 3u * uint32_t(peg2 == 0) - uint32_t(peg1 == 0);
+    }
+    static constexpr uint64_t kEvenBits = 0x5555555555555555ull;
     static constexpr uint32_t kBlock = 1;
     struct Prefix { uint32_t unused; };
     template <bool kOpBits, class E>
@@ -161,11 +175,14 @@ struct LevelArgs {
     int odd;                   // frontier search: exclusion bitsets in use
     PuzzleArgs pz;
     unsigned long long* stats;  // [0] frontier (bottom-up: unvisited) states, [1] children (probes),
-                                // [2] local children (bottom-up: found), [3] error flag, [5] two-bit next-frontier size
+                                // [2] local children (bottom-up: found), [3] error flag, [5] two-bit next-frontier size,
+                                // [6] two-bit far-bitmap marks, [7] class sizes of the frontier (sym_mult)
     const uint8_t* wflag_cur;   // optional: 1 byte per window, non-zero if the window may hold frontier states
     uint8_t* wflag_next;        // optional: set for every window that receives a mark this level
     const uint64_t* probe;      // bottom-up levels: the frontier array the unvisited states probe
     uint32_t* far;              // two-bit top-down, optional: 1 bit per state for long-range marks (see Emitter)
+    int far_all;                // far != NULL: the far-reaching marks (Emitter::far) use it too
+    int sym_mult;               // Hanoi with symmetry: add each frontier state's class size to stats[7]
 };
 
 constexpr uint64_t kEven = 0x5555555555555555ull;
@@ -362,8 +379,10 @@ struct Emitter {
     uint8_t* wflag_next;  // optional active-window flags of the next level
     int window_bits;
     uint32_t* farbits;    // two-bit: long-range mark bitmap (NULL: read the target's code, then mark it)
+    int far_all;          // the far-reaching marks (far()) go to farbits too; else they read first
     uint32_t children = 0, local = 0, bad = 0;
     uint32_t marked = 0;      // two-bit: long-range UNVISITED -> NEXT marks issued (two lanes may mark one state)
+    uint32_t farmarks = 0;    // two-bit: marks set in the far bitmap
     uint32_t parent_off = 0;  // offset of the parent being expanded in the window (rel)
 
     // Records that window c >> window_bits receives a mark.  Most long-range
@@ -394,11 +413,12 @@ struct Emitter {
             flag_window(c);
             atomicOr(reinterpret_cast<unsigned int*>(gmarks) + (c >> 3), 1u << (4 * (uint32_t(c) & 7u) + op));
         } else if constexpr (MODE == kTwoBit) {
-            if (farbits) {
+            if (farbits && (!kFar || far_all)) {
                 // Fire-and-forget: set the child's bit in the long-range
                 // bitmap; fold_two_bit turns the UNVISITED ones into NEXT
                 // after the level.  No dependent read of the target's code.
                 flag_window(c);
+                ++farmarks;
                 if constexpr (kFar) red_or_far(farbits + (c >> 5), 1u << (uint32_t(c) & 31u));
                 else atomicOr(farbits + (c >> 5), 1u << (uint32_t(c) & 31u));
                 return;
@@ -478,7 +498,7 @@ struct Probe {
 struct WindowShared {
     uint32_t any;         // some warp found a frontier state in the window
     uint32_t next_chunk;  // chunks are handed out dynamically so warps finish together
-    unsigned long long cnt[6];  // the window's counters (stats[0..5]), added to stats once per block
+    unsigned long long cnt[8];  // the window's counters (stats[0..7]), added to stats once per block
 };
 
 // One window of one level (see the top of this file).  KTHREADS threads of
@@ -541,12 +561,12 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     if (tid == 0) {
         sh.any = 0;
         sh.next_chunk = kWarps;  // chunks 0 .. kWarps-1 go to warps 0 .. kWarps-1
-        for (int i = 0; i < 6; ++i) sh.cnt[i] = 0;
+        for (int i = 0; i < 8; ++i) sh.cnt[i] = 0;
     }
     __syncthreads();
 
     Emitter<MODE> em{base, span, smarks, a.marks, a.n_states, 1u | (a.cur_code == 2 ? 2u : 0u), a.wflag_next,
-                     a.window_bits, MODE == kTwoBit ? a.far : nullptr};
+                     a.window_bits, MODE == kTwoBit ? a.far : nullptr, a.far_all};
     uint32_t found = 0;
     // ORs a mask of unit x's states into the window's shared marks.
     auto mark_unit = [&](uint32_t x, uint64_t m) {
@@ -563,6 +583,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
         return gather_even(hi & (a.cur_code == 3 ? lo : ~lo));
     };
     uint32_t probes = 0, hits = 0, pbad = 0;  // bottom-up counters
+    uint32_t mult = 0;                         // sum of the frontier states' class sizes (sym_mult)
 
     // Each warp takes chunks on its own (its first chunk is its warp index,
     // later ones come from a shared counter): lane l sweeps unit 32*chunk + l,
@@ -816,6 +837,9 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
                 } else {
                     em.parent_off = ch * kChunk + wlist[e];
                     const uint64_t p = cbase + wlist[e];
+                    if constexpr (PZ::kSymMult) {
+                        if (a.sym_mult) mult += PZ::sym_mult(p);
+                    }
                     if constexpr (kPrefixed) {
                         uint32_t var;
                         const uint32_t r = split(p, var);
@@ -882,9 +906,15 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     // Two-bit: size of the next frontier (exact for bottom-up levels, an
     // upper estimate otherwise); steers the choice of the next direction.
     uint32_t c5 = 0;
+    uint32_t c6 = 0;  // two-bit: far-bitmap marks (the fold after the level has work only if some were made)
     if constexpr (MODE == kTwoBit) c5 = __reduce_add_sync(0xFFFFFFFFu, BU ? hits : em.marked + fresh);
+    if constexpr (MODE == kTwoBit && !BU) c6 = __reduce_add_sync(0xFFFFFFFFu, em.farmarks);
+    uint32_t c7 = 0;
+    if constexpr (PZ::kSymMult && !BU) c7 = __reduce_add_sync(0xFFFFFFFFu, mult);
     if (lane == 0) {
         if (c5) atomicAdd(&sh.cnt[5], (unsigned long long)c5);
+        if (c6) atomicAdd(&sh.cnt[6], (unsigned long long)c6);
+        if (c7) atomicAdd(&sh.cnt[7], (unsigned long long)c7);
         if (c0) atomicAdd(&sh.cnt[0], (unsigned long long)c0);
         if (c1) atomicAdd(&sh.cnt[1], (unsigned long long)c1);
         if (c2) atomicAdd(&sh.cnt[2], (unsigned long long)c2);
@@ -892,7 +922,7 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     }
     __syncthreads();  // the shared marks and lists may be reused for another window
     if (tid == 0) {
-        for (int i = 0; i < 6; ++i) {
+        for (int i = 0; i < 8; ++i) {
             if (!sh.cnt[i] || i == 4) continue;
             if (i == 3) atomicOr(&a.stats[3], 1ull);
             else atomicAdd(&a.stats[i], sh.cnt[i]);
@@ -912,7 +942,7 @@ __global__ void __launch_bounds__(Shape<MODE, BU>::threads, Shape<MODE, BU>::min
 template <class PZ>
 __global__ void seed_kernel(LevelArgs a, uint64_t initial) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Emitter<kFrontier> em{~uint64_t(0), 0, nullptr, a.marks, a.n_states, 0, a.wflag_next, a.window_bits, nullptr};
+    Emitter<kFrontier> em{~uint64_t(0), 0, nullptr, a.marks, a.n_states, 0, a.wflag_next, a.window_bits, nullptr, 0};
     PZ::template expand<true>(initial, 0u, a.pz, em);
     if (a.odd) a.excl_next[initial >> 6] |= 1ull << (initial & 63);
     a.stats[1] += em.children;
@@ -963,6 +993,69 @@ __global__ void __launch_bounds__(kThreads) expand_batch_kernel(const uint64_t* 
 }
 
 // ---------------------------------------------------------------------------
+// Segmented (out-of-core) search: expansion of one segment's states with a
+// segment filter (the two halves of DB_Opt3BitBFS_Solver::Expand,
+// Common/DiskBasedOptThreeBitBFS.cpp:73-137).  The states are the set bits
+// of `bits` (segment-relative, words word_lo .. word_hi).
+//   cross == 0: children inside the segment are ORed into `next` (RED);
+//   cross == 1: children outside it are appended, as global indexes, to
+//               `out` (warp-aggregated: one atomicAdd per converged group).
+// ---------------------------------------------------------------------------
+struct SegExpandArgs {
+    const uint64_t* bits;  // the segment's states (bit i = state seg_base + i)
+    uint64_t seg_base, seg_states;
+    uint64_t word_lo, word_hi;
+    uint64_t* next;             // cross == 0: the segment's next bitmap
+    uint64_t* out;              // cross == 1: children outside the segment
+    unsigned long long* out_n;  // cross == 1: entries appended (may exceed out_cap: overflow)
+    uint64_t out_cap;
+    uint64_t n_states;
+    int cross;
+    PuzzleArgs pz;
+    unsigned long long* err;  // set when a child index is >= n_states
+};
+
+struct SegEmitter {
+    const SegExpandArgs* a;
+    uint32_t bad = 0;
+    __device__ __forceinline__ void operator()(uint64_t c, uint32_t) {
+        if (c >= a->n_states) { bad = 1; return; }
+        const uint64_t o = c - a->seg_base;
+        const bool inside = o < a->seg_states;
+        if (!a->cross) {
+            if (inside) atomicOr(reinterpret_cast<unsigned int*>(a->next) + (o >> 5), 1u << (uint32_t(o) & 31u));
+            return;
+        }
+        if (inside) return;
+        // the lanes that reach this point together share one atomicAdd
+        const uint32_t mask = __activemask();
+        const int lane = int(threadIdx.x & 31);
+        const int leader = __ffs(mask) - 1;
+        const uint32_t rank = __popc(mask & ((1u << lane) - 1u));
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(a->out_n, (unsigned long long)__popc(mask));
+        base = __shfl_sync(mask, base, leader);
+        if (base + rank < a->out_cap) a->out[base + rank] = c;
+    }
+};
+
+template <class PZ>
+__global__ void __launch_bounds__(kThreads) segment_expand_kernel(SegExpandArgs a) {
+    SegEmitter em{&a};
+    for (uint64_t w = a.word_lo + blockIdx.x * uint64_t(kThreads) + threadIdx.x; w < a.word_hi;
+         w += uint64_t(gridDim.x) * kThreads) {
+        uint64_t v = a.bits[w];
+        while (v) {
+            const int b = __ffsll((long long)v) - 1;
+            v &= v - 1;
+            const uint64_t i = w * 64 + uint64_t(b);
+            if (i < a.seg_states) PZ::template expand<false>(a.seg_base + i, 0u, a.pz, em);
+        }
+    }
+    if (em.bad) atomicOr(a.err, 1ull);
+}
+
+// ---------------------------------------------------------------------------
 // Launch helpers and per-puzzle dispatch tables.
 // ---------------------------------------------------------------------------
 using LevelLaunch = cudaError_t (*)(const LevelArgs&, unsigned grid, size_t smem, cudaStream_t);
@@ -970,13 +1063,22 @@ using SeedLaunch = cudaError_t (*)(const LevelArgs&, uint64_t initial, cudaStrea
 using ExpandLaunch = cudaError_t (*)(const uint64_t*, const uint32_t*, uint64_t, uint64_t, uint64_t*, uint32_t*,
                                      PuzzleArgs, unsigned long long*, bool, cudaStream_t);
 
+using SegExpandLaunch = cudaError_t (*)(const SegExpandArgs&, unsigned grid, cudaStream_t);
+
 struct PuzzleKernels {
     LevelLaunch level[4];     // indexed by Mode
     LevelLaunch level_bu[4];  // bottom-up levels, indexed by Mode (none for frontier search)
     SeedLaunch seed;
     ExpandLaunch expand;
+    SegExpandLaunch segment_expand;
     int branching;
 };
+
+template <class PZ>
+cudaError_t launch_segment_expand(const SegExpandArgs& a, unsigned grid, cudaStream_t s) {
+    segment_expand_kernel<PZ><<<grid, kThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
 
 template <class PZ, int MODE, bool BU = false>
 cudaError_t launch_level(const LevelArgs& a, unsigned grid, size_t smem, cudaStream_t s) {
@@ -1021,6 +1123,7 @@ PuzzleKernels make_kernels() {
     k.level_bu[kFrontier] = nullptr;
     k.seed = &launch_seed<PZ>;
     k.expand = &launch_expand<PZ>;
+    k.segment_expand = &launch_segment_expand<PZ>;
     k.branching = PZ::kBranch;
     return k;
 }

@@ -2,7 +2,11 @@
 // the reference, which solves one puzzle per call).
 //
 // Clients submit solve requests (puzzle, start state) from any thread without
-// blocking.  One server thread owns a psb_engine and loops:
+// blocking.  Requests with more than large_states states go to the large
+// lane: a second thread runs them one at a time as single two-bit searches
+// (one reusable psb_bfs session per puzzle size, on its own stream), so a
+// large search never sets the pace of the small ones.  The batch lane's
+// server thread owns a psb_engine and loops:
 //   1. admit queued requests while an instance slot and pool space for the
 //      request's two-bit array are free (admission by HBM footprint: 2 bits x
 //      states, padded).  The smallest requests go first; a request that does
@@ -14,12 +18,16 @@
 //      requests that arrive while others are running overlap on the GPU;
 //   3. collect finished searches: per-depth counts, eccentricity (the last
 //      depth) and latency from submission to completion.
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -39,6 +47,7 @@ struct Request {
     Clock::time_point submitted;
     uint64_t footprint;   // engine pool bytes (0 if the puzzle is invalid: admission reports why)
     uint32_t bypassed;    // times a later request was admitted while this one did not fit
+    uint64_t states;      // IndexesCount() (0 if the puzzle is invalid)
 };
 
 // A request passed over this many times stops later admissions until it fits.
@@ -64,6 +73,12 @@ struct psb_server {
     std::unordered_map<uint64_t, Request> running;
     std::atomic<bool> stop{false};
     std::atomic<uint64_t> next_ticket{1};
+    // Large lane.
+    uint64_t large_states = 0;
+    std::deque<Request> large_queue;
+    std::condition_variable large_cv;
+    std::thread large_worker;
+    uint32_t large_running = 0;
     int fatal = PSB_OK;
     std::string fatal_msg;
     uint64_t admitted = 0, completed = 0, steps = 0;
@@ -168,6 +183,56 @@ void serve(psb_server* s) {
     }
 }
 
+// The large lane: one request at a time, first come first served, each as a
+// single two-bit search on this thread's stream.  Sessions are kept per
+// puzzle size, so a size's arrays are allocated once.
+void serve_large(psb_server* s) {
+    struct Sess {
+        psb_puzzle* puzzle = nullptr;
+        psb_bfs_session* session = nullptr;
+    };
+    std::map<std::tuple<int, int, int>, Sess> sessions;
+    cudaStream_t stream = nullptr;
+    cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    std::vector<uint64_t> counts(s->max_depths);
+    for (;;) {
+        Request r;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            s->large_cv.wait(lock, [&] { return s->stop.load() || !s->large_queue.empty(); });
+            if (s->stop.load()) break;
+            r = s->large_queue.front();
+            s->large_queue.pop_front();
+            s->large_running = 1;
+        }
+        psb_bfs_opts o{};
+        o.struct_size = sizeof(psb_bfs_opts);
+        o.device = -1;
+        o.stream = stream;
+        int rc = PSB_OK;
+        Sess& x = sessions[std::make_tuple(r.kind, r.a, r.b)];
+        if (!x.puzzle) rc = psb_puzzle_create(r.kind, r.a, r.b, &x.puzzle);
+        if (rc == PSB_OK && !x.session) rc = psb_bfs_session_create(x.puzzle, PSB_TWO_BIT, &o, &x.session);
+        uint32_t nd = 0;
+        if (rc == PSB_OK) rc = psb_bfs_session_run(x.session, r.initial, &o, counts.data(), s->max_depths, &nd, nullptr);
+        const double lat = std::chrono::duration<double>(Clock::now() - r.submitted).count();
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (rc == PSB_OK) {
+            s->done.push_back(Done{r.ticket, PSB_OK, std::vector<uint64_t>(counts.begin(), counts.begin() + nd), lat});
+            s->completed++;
+        } else {
+            s->done.push_back(Done{r.ticket, rc, {}, 0.0});
+        }
+        s->large_running = 0;
+    }
+    for (auto& kv : sessions) {
+        if (kv.second.session) psb_bfs_session_destroy(kv.second.session);
+        if (kv.second.puzzle) psb_puzzle_destroy(kv.second.puzzle);
+    }
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+}
+
 }  // namespace
 
 extern "C" {
@@ -178,11 +243,16 @@ int psb_server_start(const psb_server_opts* opts, psb_server** out) {
     if (int rc = psb_engine_create(&opts->engine, &s->engine)) { delete s; return rc; }
     s->max_depths = opts->engine.max_depths;
     s->levels_per_step = opts->levels_per_step ? opts->levels_per_step : 1;
+    s->large_states = opts->large_states ? opts->large_states : (uint64_t(1) << 26);
     int device = -1;
     cudaGetDevice(&device);
     s->worker = std::thread([s, device] {
         cudaSetDevice(device);
         serve(s);
+    });
+    s->large_worker = std::thread([s, device] {
+        cudaSetDevice(device);
+        serve_large(s);
     });
     *out = s;
     return PSB_OK;
@@ -190,15 +260,22 @@ int psb_server_start(const psb_server_opts* opts, psb_server** out) {
 
 int psb_server_submit(psb_server* s, int kind, int a, int b, uint64_t initial, uint64_t* ticket) {
     if (!s || !ticket) return psb_set_error(PSB_ERR_ARG, "bad argument");
-    uint64_t footprint = 0;
+    uint64_t footprint = 0, states = 0;
     if (psb_engine_footprint(kind, a, b, &footprint) != PSB_OK) footprint = 0;
-    Request r{s->next_ticket.fetch_add(1), kind, a, b, initial, Clock::now(), footprint, 0};
+    psb_puzzle* p = nullptr;
+    if (psb_puzzle_create(kind, a, b, &p) == PSB_OK) {
+        int ops = 0, br = 0, odd = 0;
+        psb_puzzle_info(p, &states, &ops, &br, &odd);
+        psb_puzzle_destroy(p);
+    }
+    Request r{s->next_ticket.fetch_add(1), kind, a, b, initial, Clock::now(), footprint, 0, states};
+    const bool large = states > s->large_states;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->stop.load()) return psb_set_error(s->fatal ? s->fatal : PSB_ERR_ARG, "server stopped");
-        s->queue.push_back(r);
+        (large ? s->large_queue : s->queue).push_back(r);
     }
-    s->cv.notify_one();
+    (large ? s->large_cv : s->cv).notify_one();
     *ticket = r.ticket;
     return PSB_OK;
 }
@@ -226,8 +303,8 @@ int psb_server_poll(psb_server* s, uint64_t* tickets, int* status, uint32_t* n_d
 int psb_server_info(psb_server* s, uint32_t* queued, uint32_t* running, uint64_t* completed, uint64_t* steps) {
     if (!s) return psb_set_error(PSB_ERR_ARG, "bad argument");
     std::lock_guard<std::mutex> lock(s->mu);
-    if (queued) *queued = uint32_t(s->queue.size());
-    if (running) *running = uint32_t(s->running.size());
+    if (queued) *queued = uint32_t(s->queue.size() + s->large_queue.size());
+    if (running) *running = uint32_t(s->running.size()) + s->large_running;
     if (completed) *completed = s->completed;
     if (steps) *steps = s->steps;
     return s->fatal;
@@ -240,7 +317,9 @@ int psb_server_stop(psb_server* s) {
         s->stop = true;
     }
     s->cv.notify_all();
+    s->large_cv.notify_all();
     if (s->worker.joinable()) s->worker.join();
+    if (s->large_worker.joinable()) s->large_worker.join();
     psb_engine_destroy(s->engine);
     delete s;
     return PSB_OK;

@@ -4,11 +4,15 @@
 //   bfs <kind> <a> <b> <classic|two_bit|three_bit|frontier> <state...>
 //   expand <kind> <a> <b> <state...>
 //   custom <n>
+//   hanoisearch <disks 8..19> <maxSteps>
+//   disk <kind> <a> <b> <Classic|TwoBit|ThreeBit|FrontierSearch|OptFrontierSearch|OptThreeBit> <segmentBits> <threads> <state...>
 // with kind one of sliding, sliding_gpu, pancake, hanoi4, hanoi4_gpu (the
 // *_gpu kinds construct the reference's GPU class names,
 // SlidingTilePuzzleGpu and FourPegHanoiGPU), and prints one result line per
 // command (space-separated counts, or "child-state|op" items separated by
-// ';').  `custom` drives a Puzzle subclass defined here, as a caller would:
+// ';').  `hanoisearch` runs HanoiSearch<disks> from all disks on peg 0, as
+// the reference's HanoiSearchTests do.  `custom` drives a Puzzle subclass
+// defined here, as a caller would:
 // it prints the number of children ExpandBuffer delivers over all n states,
 // then what InMemoryTwoBitBFS does with it.  tests/test_gpu_cpp_adapter.py
 // feeds it the reference's golden vectors.
@@ -78,10 +82,51 @@ int main() {
             std::cout.flush();
             continue;
         }
+        if (cmd == "hanoisearch") {
+            int disks = 0, steps = 0;
+            in >> disks >> steps;
+            try {
+                std::vector<uint64_t> r;
+                switch (disks) {
+#define HANOI_CASE(n)                                              \
+    case n: {                                                      \
+        SearchOptions opts;                                        \
+        if (steps > 0) opts.maxSteps = steps;                      \
+        r = HanoiSearch<HanoiTowers<n>::Size>(HanoiTowers<n>::ToString(0), opts); \
+        break;                                                     \
+    }
+                    HANOI_CASE(8) HANOI_CASE(9) HANOI_CASE(10) HANOI_CASE(11) HANOI_CASE(12) HANOI_CASE(13)
+                    HANOI_CASE(14) HANOI_CASE(15) HANOI_CASE(16) HANOI_CASE(17) HANOI_CASE(18) HANOI_CASE(19)
+#undef HANOI_CASE
+                default: std::cout << "ERROR -1 unsupported size\n"; std::cout.flush(); continue;
+                }
+                for (size_t i = 0; i < r.size(); i++) std::cout << (i ? " " : "") << r[i];
+                std::cout << "\n";
+            } catch (const psb200::Error& e) {
+                std::cout << "ERROR " << e.code() << " " << e.what() << "\n";
+            }
+            std::cout.flush();
+            continue;
+        }
         in >> kind >> a >> b;
         try {
             auto puzzle = make(kind, a, b);
-            if (cmd == "bfs") {
+            if (cmd == "disk") {  // a disk-based test body: PuzzleOptions with segmentBits and threads
+                std::string algo, state;
+                PuzzleOptions opts;
+                in >> algo >> opts.segmentBits >> opts.threads;
+                std::getline(in, state);
+                if (state.empty() || state == " ") state = puzzle->ToString(0);
+                std::vector<uint64_t> r;
+                if (algo == "Classic") r = DiskBasedClassicBFS(*puzzle, state, opts);
+                else if (algo == "TwoBit") r = DiskBasedTwoBitBFS(*puzzle, state, opts);
+                else if (algo == "ThreeBit") r = DiskBasedThreeBitBFS(*puzzle, state, opts);
+                else if (algo == "FrontierSearch") r = DiskBasedFrontierSearch(*puzzle, state, opts);
+                else if (algo == "OptFrontierSearch") r = DiskBasedOptFrontierSearch(*puzzle, state, opts);
+                else r = DiskBasedOptThreeBitBFS(*puzzle, state, opts);
+                for (size_t i = 0; i < r.size(); i++) std::cout << (i ? " " : "") << r[i];
+                std::cout << "\n";
+            } else if (cmd == "bfs") {
                 std::string algo, state;
                 in >> algo;
                 std::getline(in, state);

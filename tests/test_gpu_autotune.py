@@ -69,3 +69,8 @@ def test_engine_window_offsets(tmp_path):
     eng.close()
     for tag, (p, s) in enumerate(items[:8]):
         assert done[tag] == psb.bfs(p, "two_bit", s)["counts"]
+
+
+def test_far_marks():
+    best, timings = autotune.tune_far_marks(psb.PancakeSimple(10))
+    assert best in ("none", "near", "all") and set(timings) == {"none", "near", "all"}

@@ -179,6 +179,49 @@ def test_children_stat_equals_oracle_expand(spec, algo):
         assert want == 6 * 4 ** spec[1] - 6 * 2 ** spec[1]
 
 
+@pytest.mark.parametrize("disks", [1, 2, 3, 6, 9, 12])
+def test_hanoi_search_restored_counts(disks):
+    """HanoiSearch (HanoiTowers/HanoiSearch.cpp): the two-bit search over the
+    symmetric space, each canonical state counted by its class size
+    (PegsMult), gives the per-depth counts of the full space (the oracle's
+    search without symmetry); the canonical counts are the symmetric
+    search's own."""
+    r = psb.bfs(psb.FourPegHanoiSimple(disks, True), "two_bit", 0, restored=True)
+    assert r["counts"] == O.bfs(["hanoi4", disks, 1], "two_bit")[0]
+    assert r["restored"] == O.bfs(["hanoi4", disks, 0], "two_bit")[0]
+    assert sum(r["restored"]) == 4 ** disks
+
+
+@pytest.mark.parametrize("disks", [17, 18])
+def test_hanoi_search_golden(disks, golden):
+    """The reference's HanoiSearchTests (121 depths, maxSteps = 120)."""
+    v = [x for x in golden["legacy_hanoi"] if x["puzzle"] == ["hanoi4", disks, 0]][0]
+    r = psb.bfs(psb.FourPegHanoiSimple(disks, True), "two_bit", 0, max_depth=120, restored=True)
+    assert r["restored"] == v["counts"]
+
+
+def test_restored_counts_need_symmetric_hanoi():
+    with pytest.raises(psb.PsbError) as e:
+        psb.bfs(psb.FourPegHanoiSimple(8), "two_bit", 0, restored=True)
+    assert e.value.code == -5
+    with pytest.raises(psb.PsbError):
+        psb.bfs(psb.FourPegHanoiSimple(8, True), "three_bit", 0, restored=True)
+
+
+@pytest.mark.parametrize("spec", [["pancake", 10, 0], ["sliding", 3, 3], ["hanoi4", 9, 0], ["hanoi4", 8, 1]])
+def test_far_mark_modes_agree(spec):
+    """Two-bit long-range marks read-first, through the far bitmap for the
+    near marks, or for all of them: the same counts and final code array
+    as the oracle, top-down and with bottom-up levels."""
+    p = {"pancake": lambda: psb.PancakeSimple(spec[1]), "sliding": lambda: psb.SlidingTilePuzzleSimple(*spec[1:]),
+         "hanoi4": lambda: psb.FourPegHanoiSimple(spec[1], bool(spec[2]))}[spec[0]]()
+    counts, fin = O.bfs(spec, "two_bit", 0, final=True)
+    for mode in ("none", "near", "all", "auto"):
+        for direction in ("top_down", "auto"):
+            r = psb.bfs(p, "two_bit", 0, final=True, far_marks=mode, direction=direction, window_bits=10)
+            assert r["counts"] == counts and r["final"] == fin, (mode, direction)
+
+
 def test_trivial_puzzles():
     assert psb.bfs(psb.PancakeSimple(2), "three_bit", 0)["counts"] == [1, 1]
     assert psb.bfs(psb.FourPegHanoiSimple(1), "two_bit", 0)["counts"] == [1, 3]

@@ -103,3 +103,31 @@ def test_gpu_class_limits_and_names():
     got = run(["bfs hanoi4_gpu 25 0 two_bit", "expand sliding_gpu 3 2 1 0 2 3 4 5"])
     assert got[0].startswith("ERROR -1")
     assert got[1] == run(["expand sliding 3 2 1 0 2 3 4 5"])[0]
+
+
+@pytest.mark.gpu
+def test_hanoi_search_through_adapter(golden):
+    """HanoiSearch<size> as the reference's HanoiSearchTests call it
+    (HanoiTowers<17>::ToString(0), maxSteps = 120), and a full search whose
+    counts equal the oracle's search without symmetry."""
+    import oracle as O
+    v = [x for x in golden["legacy_hanoi"] if x["puzzle"] == ["hanoi4", 17, 0]][0]
+    got = run(["hanoisearch 17 120", "hanoisearch 11 0"])
+    assert [int(x) for x in got[0].split()] == v["counts"]
+    assert [int(x) for x in got[1].split()] == O.bfs(["hanoi4", 11, 0], "two_bit")[0]
+
+
+@pytest.mark.gpu
+def test_disk_based_bodies_through_adapter(golden):
+    """The reference's disk-based test bodies (PuzzlesTests/PuzzleSearchTests.cpp:
+    133-333): PuzzleOptions with segmentBits 15..22 and threads 1 or 4, on
+    SlidingTilePuzzleGpu(5, 2) and the Simple class, give ST5x2."""
+    v = [x for x in golden["search"] if x["puzzle"] == ["sliding", 5, 2]][0]
+    cmds = []
+    for kind in ("sliding_gpu", "sliding"):
+        for algo in ("Classic", "TwoBit", "ThreeBit", "FrontierSearch", "OptFrontierSearch", "OptThreeBit"):
+            for bits, threads in ((22, 1), (19, 1), (19, 4), (15, 1)):
+                cmds.append(f"disk {kind} 5 2 {algo} {bits} {threads} 0 1 2 3 4 5 6 7 8 9")
+    got = run(cmds)
+    for cmd, line in zip(cmds, got):
+        assert [int(x) for x in line.split()] == v["counts"], cmd

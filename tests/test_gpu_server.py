@@ -96,7 +96,7 @@ def test_request_larger_than_the_pool_fails_at_once():
     small = psb.PancakeSimple(9)
     big = psb.PancakeSimple(12)  # 120 MB of codes: never fits a 16 MB pool
     foot = psb.Engine.footprint(small)
-    srv = psb.Server(max_instances=8, pool_bytes=16 << 20)
+    srv = psb.Server(max_instances=8, pool_bytes=16 << 20, large_states=None)  # every request in the batch lane
     assert psb.Engine.footprint(big) > 16 << 20 > 2 * foot
     before = [srv.submit(small, s) for s in (0, 5)]
     bad = srv.submit(big, 0)
@@ -134,3 +134,28 @@ def test_small_requests_pass_a_waiting_large_one():
     assert done[waiting][1] == psb.bfs(large, "two_bit", 1)["counts"]
     for s, t in enumerate(smalls):
         assert done[t][0] == 0 and done[t][1] == psb.bfs(small, "two_bit", s)["counts"]
+
+
+def test_large_lane_and_batch_lane_together():
+    """Requests above large_states run one at a time as single searches on
+    their own stream while the others batch in the engine; every result
+    equals the search alone, whichever lane ran it."""
+    rng = random.Random(9)
+    small = [psb.PancakeSimple(8), psb.SlidingTilePuzzleSimple(3, 3), psb.FourPegHanoiSimple(8)]
+    large = [psb.PancakeSimple(10), psb.FourPegHanoiSimple(11)]
+    srv = psb.Server(max_instances=32, pool_bytes=1 << 30, large_states=1 << 20)
+    reqs = {}
+    for i in range(30):
+        p = (large if i % 5 == 0 else small)[rng.randrange(2 if i % 5 == 0 else 3)]
+        st = 0 if p.Name().startswith("Sliding") else rng.randrange(p.IndexesCount())
+        reqs[srv.submit(p, st)] = (p, st)
+    done = {}
+    deadline = time.time() + 120
+    while len(done) < len(reqs) and time.time() < deadline:
+        done.update(srv.poll())
+        time.sleep(0.002)
+    info = srv.info()
+    srv.stop()
+    assert len(done) == len(reqs), info
+    for t, (p, st) in reqs.items():
+        assert done[t][0] == 0 and done[t][1] == psb.bfs(p, "two_bit", st)["counts"]
