@@ -418,7 +418,7 @@ def profile_once(args):
     sink = psb.SPILL_FN(lambda *_: 0) if args.spill else None
     r = psb.bfs(puzzle, algo, 0, max_depth=args.max_depth, window_bits=args.window_bits, levels=True,
                 direction=args.direction, bottom_up_ratio=args.bottom_up_ratio, spill=sink,
-                segment_bits=args.segment_bits, far_marks=args.far_marks)
+                segment_bits=args.segment_bits, far_marks=args.far_marks, threads=args.threads)
     out = {"workload": args.workload, "counts": r["counts"], "level_ms": [round(x, 3) for x in r["level_ms"]],
            "level_children": r["level_children"], "stats": r["stats"]}
     print(json.dumps(out), flush=True)
@@ -442,6 +442,8 @@ def main():
                     help="encode every depth's frontier on the GPU (segment streams) and hand it over in pinned"
                          " host memory during the timed searches (default for pancake14-2bit and hanoi18-2bit)")
     ap.add_argument("--no-spill", action="store_true", help="no frontier spill, whatever the workload")
+    ap.add_argument("--threads", type=int, default=0, choices=[0, 128, 256, 512],
+                    help="threads per block of the top-down two-bit / three-bit level kernels (0 = 256)")
     ap.add_argument("--far-marks", default="auto", choices=["auto", "none", "near", "all"],
                     help="two-bit long-range marks (PSB_FAR_*); --autotune picks it for two-bit workloads")
     ap.add_argument("--e2e-calls", type=int, default=5,
@@ -492,10 +494,14 @@ def main():
         if algo == "two_bit":
             args.far_marks, ft = autotune.tune_far_marks(puzzle, 0, window_bits=args.window_bits)
             tuning.update({"far_marks": args.far_marks, "far_marks_ms": {k: round(v, 2) for k, v in ft.items()}})
+        if algo in ("two_bit", "three_bit"):
+            args.threads, tt = autotune.tune_threads(puzzle, algo, 0, window_bits=args.window_bits,
+                                                     far_marks=args.far_marks)
+            tuning.update({"threads": args.threads, "threads_ms": {str(k): round(v, 2) for k, v in tt.items()}})
     stream = torch.cuda.Stream()
     # Session on torch's stream so the CUDA events below bracket exactly the searches.
     opts = psb._opts(0, args.window_bits, local, stream.cuda_stream, direction=args.direction,
-                     far_marks=args.far_marks)
+                     far_marks=args.far_marks, threads=args.threads)
     h = ctypes.c_void_p()
     psb._check(psb.lib().psb_bfs_session_create(puzzle.handle, psb._algo(algo), ctypes.byref(opts), ctypes.byref(h)))
     cap = 1 << 16
@@ -518,7 +524,7 @@ def main():
         st.struct_size = ctypes.sizeof(psb.BfsStats)
         o = psb._opts(0, 0, local, stream.cuda_stream, direction=args.direction,
                       bottom_up_ratio=args.bottom_up_ratio, spill=spill_fn, segment_bits=args.segment_bits,
-                      far_marks=args.far_marks)
+                      far_marks=args.far_marks, threads=args.threads)
         psb._check(psb.lib().psb_bfs_session_run(h, 0, ctypes.byref(o), counts, cap, ctypes.byref(nd), ctypes.byref(st)))
         return list(counts[:nd.value]), st
 
@@ -554,7 +560,7 @@ def main():
     for _ in range(1):
         psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
                 spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits,
-                far_marks=args.far_marks)
+                far_marks=args.far_marks, threads=args.threads)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -564,7 +570,7 @@ def main():
         tc = time.perf_counter()
         r = psb.bfs(puzzle, algo, 0, device=local, direction=args.direction, bottom_up_ratio=args.bottom_up_ratio,
                     spill=spill_fn, segment_bits=args.segment_bits, window_bits=args.window_bits,
-                far_marks=args.far_marks)
+                far_marks=args.far_marks, threads=args.threads)
         calls.append(time.perf_counter() - tc)
         assert r["counts"] == ref_counts
         levels = r["stats"]["levels"]

@@ -51,7 +51,7 @@ class BfsOpts(ctypes.Structure):
                 ("level_ms", ctypes.POINTER(ctypes.c_float)), ("level_children", u64p),
                 ("direction", ctypes.c_int32), ("bottom_up_ratio", ctypes.c_float),
                 ("spill", SPILL_FN), ("spill_user", ctypes.c_void_p), ("segment_bits", ctypes.c_int32),
-                ("far_marks", ctypes.c_int32), ("restored_counts", u64p)]
+                ("far_marks", ctypes.c_int32), ("threads", ctypes.c_int32), ("restored_counts", u64p)]
 
 
 class BfsStats(ctypes.Structure):
@@ -356,8 +356,9 @@ FAR_MARKS = {"auto": 0, "none": 1, "near": 2, "all": 3}
 
 
 def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_ms=None, level_children=None,
-          direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0, far_marks="auto"):
+          direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0, far_marks="auto", threads=0):
     o = BfsOpts()
+    o.threads = threads
     o.far_marks = FAR_MARKS[far_marks] if isinstance(far_marks, str) else int(far_marks)
     if spill is not None:
         o.spill = spill  # a SPILL_FN the caller keeps alive for the call
@@ -380,7 +381,8 @@ def _opts(max_depth=0, window_bits=0, device=-1, stream=None, final=None, level_
 
 
 def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels=False, device=-1,
-        direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0, restored=False, far_marks="auto"):
+        direction="auto", bottom_up_ratio=0.0, spill=None, segment_bits=0, restored=False, far_marks="auto",
+        threads=0):
     """Runs psb_bfs.  Returns a dict with counts, stats and optionally the final
     arrays (list of 64-bit words in the reference's layout) and per-level data.
     direction: "auto", "top_down" or "bottom_up" (PSB_DIR_*).
@@ -389,6 +391,7 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
     states per segment, 0 = 2^32); a truthy return stops the search.  A
     SPILL_FN is passed through as is (it sees the pinned buffer itself).
     far_marks: two-bit long-range marks, "auto", "none", "near" or "all" (PSB_FAR_*).
+    threads: threads per block of the top-down two-bit / three-bit level kernels (128, 256, 512; 0 = 256).
     restored: 4-peg Hanoi with symmetry, two-bit: also return "restored", the
     per-depth counts weighted by each canonical state's class size
     (HanoiSearch's result)."""
@@ -404,7 +407,7 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
     lc = (ctypes.c_uint64 * cap)() if levels else None
     fn, runner = _spill_fn(spill)
     o = _opts(max_depth, window_bits, device, None, fin, lm, lc, direction, bottom_up_ratio, fn, segment_bits,
-              far_marks)
+              far_marks, threads)
     rc = (ctypes.c_uint64 * cap)() if restored else None
     if restored:
         o.restored_counts = ctypes.cast(rc, u64p)

@@ -2,8 +2,8 @@
 measurement rather than by rule: the batch engine's persistent grid (blocks
 per SM) and its instances' window size; the window of a single search's
 level kernel (states per thread-block window, the unit of work the kernel
-sweeps and marks in shared memory); and where a two-bit search's long-range
-marks go (PSB_FAR_*).
+sweeps and marks in shared memory) and its threads per block; and where a
+two-bit search's long-range marks go (PSB_FAR_*).
 
 Each candidate runs the same workload on this device.  The tuner checks that
 every candidate gives the same results, and returns the fastest one with all
@@ -16,7 +16,7 @@ import time
 
 from . import Engine, bfs, device_name, lib
 
-__all__ = ["tune", "tune_engine", "tune_window_bits", "tune_far_marks", "Cache"]
+__all__ = ["tune", "tune_engine", "tune_window_bits", "tune_far_marks", "tune_threads", "Cache"]
 
 
 def tune(candidates, measure):
@@ -131,6 +131,26 @@ def tune_far_marks(puzzle, initial=0, candidates=("none", "near", "all"), window
 
     def measure(mode):
         r = bfs(puzzle, "two_bit", initial, window_bits=window_bits, far_marks=mode)
+        return r["stats"]["total_ms"], r["counts"]
+
+    best, timings = tune(candidates, measure)
+    if cache and key:
+        cache.put(dev, key, best)
+    return best, timings
+
+
+def tune_threads(puzzle, algo, initial=0, candidates=(128, 256, 512), window_bits=0, far_marks="auto",
+                 cache=None, key=None):
+    """Threads per block of a single search's top-down level kernel (two-bit
+    and three-bit: shape variants compiled as separate kernel instances),
+    timed as the device time of the whole search.  Returns (best, {threads: ms})."""
+    dev = device_name()
+    if cache and key and cache.get(dev, key) is not None:
+        return cache.get(dev, key), {}
+    bfs(puzzle, algo, initial, window_bits=window_bits, far_marks=far_marks)  # warm-up (pool growth)
+
+    def measure(threads):
+        r = bfs(puzzle, algo, initial, window_bits=window_bits, far_marks=far_marks, threads=threads)
         return r["stats"]["total_ms"], r["counts"]
 
     best, timings = tune(candidates, measure)

@@ -839,8 +839,14 @@ int auto_window_bits(const psb_puzzle* p, int algo) {
     return wb;
 }
 
-size_t smem_bytes(int mode, int wb) {
-    return psb::level_smem_bytes(mode, size_t(1) << wb, psb::level_threads(mode));
+size_t smem_bytes(int mode, int wb, int threads = 0) {
+    return psb::level_smem_bytes(mode, size_t(1) << wb, threads ? threads : psb::level_threads(mode));
+}
+
+// Shape variant of the top-down level kernel for psb_bfs_opts.threads.
+int shape_variant(int mode, int threads) {
+    if (mode != psb::kTwoBit && mode != psb::kThreeBit) return 0;
+    return threads == 512 ? 1 : threads == 128 ? 2 : 0;
 }
 
 int set_bit(uint64_t* d_word_base, uint64_t bit, cudaStream_t s) {
@@ -1052,7 +1058,11 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
 
     const uint64_t W1 = words_for(N), W2 = words_for(2 * N), W4 = (N + 15) / 16;
     const unsigned grid = unsigned((N + (uint64_t(1) << S->window_bits) - 1) >> S->window_bits);
-    const size_t smem = smem_bytes(S->mode, S->window_bits);
+    const int threads_req = opts ? opts->threads : 0;
+    if (threads_req != 0 && threads_req != 128 && threads_req != 256 && threads_req != 512)
+        return fail(PSB_ERR_ARG, "threads must be 0, 128, 256 or 512");
+    const int variant = shape_variant(S->mode, threads_req);
+    const size_t smem = smem_bytes(S->mode, S->window_bits, psb::variant_threads(variant));
     // Bottom-up levels use windows twice as large (fewer window-end barriers
     // per state; 13-pancake depth 12: 74 ms instead of 77 ms); top-down levels
     // keep the smaller windows, whose long-range marks stay closer together.
@@ -1186,7 +1196,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
                 a.front_words = W4; a.mark_words = W4;
                 break;
             }
-            PSB_CUDA(P.k.level[S->mode](a, grid, smem, s));
+            PSB_CUDA((variant ? P.k.level_shape[variant][S->mode] : P.k.level[S->mode])(a, grid, smem, s));
             a.far = nullptr;
             launches++;
         }
@@ -1345,7 +1355,7 @@ done:
     if (stats && stats->struct_size >= sizeof(psb_bfs_stats)) {
         stats->levels = uint32_t(launches);
         stats->window_bits = uint32_t(S->window_bits);
-        stats->threads = uint32_t(psb::level_threads(S->mode));
+        stats->threads = uint32_t(variant ? psb::variant_threads(variant) : psb::level_threads(S->mode));
         stats->total_ms = total;
         stats->expand_ms = expand_ms;
         stats->finalize_ms = finalize_ms;

@@ -45,11 +45,22 @@ enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 // three-bit's marks are fire-and-forget, and it runs fastest without a
 // register cap.  Bottom-up levels wait on their probe loads, so they want
 // resident warps too (four blocks per SM).
-template <int MODE, bool BU = false>
+//
+// Variants 1 and 2 of the top-down two-bit and three-bit kernels (the
+// autotuner's threads-per-block dimension, psb_bfs_opts.threads): 512 and
+// 128 threads per block with the same register budget per thread (two-bit:
+// 1024 resident threads per SM at 64 registers; three-bit: no cap at 512,
+// two blocks at 128).
+template <int MODE, bool BU = false, int V = 0>
 struct Shape {
-    static constexpr int threads = 256;
-    static constexpr int min_blocks = BU ? 4 : MODE == kTwoBit ? 4 : MODE == kFrontier ? 2 : 1;
+    static constexpr int threads = V == 1 ? 512 : V == 2 ? 128 : 256;
+    static constexpr int min_blocks = BU ? 4
+                                    : MODE == kTwoBit ? (V == 1 ? 2 : V == 2 ? 8 : 4)
+                                    : MODE == kFrontier ? 2
+                                    : (V == 2 ? 2 : 1);
 };
+constexpr int kShapeVariants = 3;
+__host__ __device__ constexpr int variant_threads(int v) { return v == 1 ? 512 : v == 2 ? 128 : 256; }
 
 __host__ __device__ constexpr int level_threads(int mode) {
     return mode == kThreeBit ? Shape<kThreeBit>::threads
@@ -930,11 +941,12 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     }
 }
 
-template <class PZ, int MODE, bool BU = false>
-__global__ void __launch_bounds__(Shape<MODE, BU>::threads, Shape<MODE, BU>::min_blocks) level_kernel(LevelArgs a) {
+template <class PZ, int MODE, bool BU = false, int V = 0>
+__global__ void __launch_bounds__(Shape<MODE, BU, V>::threads, Shape<MODE, BU, V>::min_blocks)
+    level_kernel(LevelArgs a) {
     extern __shared__ __align__(16) unsigned long long smem64[];
     __shared__ WindowShared sh;
-    level_window<PZ, MODE, Shape<MODE, BU>::threads, BU>(a, blockIdx.x, smem64, sh);
+    level_window<PZ, MODE, Shape<MODE, BU, V>::threads, BU>(a, blockIdx.x, smem64, sh);
 }
 
 // Level 0 of frontier search (InMemoryFrontierSearch.cpp:81-88): expand the
@@ -1068,6 +1080,7 @@ using SegExpandLaunch = cudaError_t (*)(const SegExpandArgs&, unsigned grid, cud
 struct PuzzleKernels {
     LevelLaunch level[4];     // indexed by Mode
     LevelLaunch level_bu[4];  // bottom-up levels, indexed by Mode (none for frontier search)
+    LevelLaunch level_shape[kShapeVariants][4];  // top-down levels in shape variant v (two-bit, three-bit)
     SeedLaunch seed;
     ExpandLaunch expand;
     SegExpandLaunch segment_expand;
@@ -1080,12 +1093,12 @@ cudaError_t launch_segment_expand(const SegExpandArgs& a, unsigned grid, cudaStr
     return cudaGetLastError();
 }
 
-template <class PZ, int MODE, bool BU = false>
+template <class PZ, int MODE, bool BU = false, int V = 0>
 cudaError_t launch_level(const LevelArgs& a, unsigned grid, size_t smem, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(level_kernel<PZ, MODE, BU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(smem));
+    cudaError_t e = cudaFuncSetAttribute(level_kernel<PZ, MODE, BU, V>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    level_kernel<PZ, MODE, BU><<<grid, Shape<MODE, BU>::threads, smem, s>>>(a);
+    level_kernel<PZ, MODE, BU, V><<<grid, Shape<MODE, BU, V>::threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -1121,6 +1134,14 @@ PuzzleKernels make_kernels() {
     k.level_bu[kClassic] = &launch_level<PZ, kClassic, true>;
     k.level_bu[kTwoBit] = &launch_level<PZ, kTwoBit, true>;
     k.level_bu[kFrontier] = nullptr;
+    for (auto& row : k.level_shape)
+        for (auto& f : row) f = nullptr;
+    k.level_shape[0][kThreeBit] = &launch_level<PZ, kThreeBit>;
+    k.level_shape[0][kTwoBit] = &launch_level<PZ, kTwoBit>;
+    k.level_shape[1][kThreeBit] = &launch_level<PZ, kThreeBit, false, 1>;
+    k.level_shape[1][kTwoBit] = &launch_level<PZ, kTwoBit, false, 1>;
+    k.level_shape[2][kThreeBit] = &launch_level<PZ, kThreeBit, false, 2>;
+    k.level_shape[2][kTwoBit] = &launch_level<PZ, kTwoBit, false, 2>;
     k.seed = &launch_seed<PZ>;
     k.expand = &launch_expand<PZ>;
     k.segment_expand = &launch_segment_expand<PZ>;

@@ -74,3 +74,15 @@ def test_engine_window_offsets(tmp_path):
 def test_far_marks():
     best, timings = autotune.tune_far_marks(psb.PancakeSimple(10))
     assert best in ("none", "near", "all") and set(timings) == {"none", "near", "all"}
+
+
+def test_threads_per_block():
+    """The shape variants (128 / 256 / 512 threads per block) give the same
+    counts, and the tuner picks one of them."""
+    for algo in ("two_bit", "three_bit"):
+        best, timings = autotune.tune_threads(psb.PancakeSimple(10), algo)
+        assert best in (128, 256, 512) and set(timings) == {128, 256, 512}
+    r = psb.bfs(psb.SlidingTilePuzzleSimple(3, 3), "two_bit", 0, threads=512, levels=True)
+    assert r["stats"]["threads"] == 512
+    with pytest.raises(psb.PsbError):
+        psb.bfs(psb.PancakeSimple(8), "two_bit", 0, threads=300)

@@ -222,6 +222,21 @@ def test_far_mark_modes_agree(spec):
             assert r["counts"] == counts and r["final"] == fin, (mode, direction)
 
 
+@pytest.mark.parametrize("spec,algo", [(["pancake", 10, 0], "two_bit"), (["pancake", 10, 0], "three_bit"),
+                                       (["hanoi4", 9, 0], "two_bit"), (["sliding", 4, 2], "three_bit")])
+def test_thread_shapes_agree(spec, algo):
+    """128, 256 and 512 threads per block (separate kernel instances) give
+    the oracle's counts and final arrays, top-down and with bottom-up levels."""
+    p = {"pancake": lambda: psb.PancakeSimple(spec[1]), "sliding": lambda: psb.SlidingTilePuzzleSimple(*spec[1:]),
+         "hanoi4": lambda: psb.FourPegHanoiSimple(spec[1], bool(spec[2]))}[spec[0]]()
+    counts, fin = O.bfs(spec, algo, 0, final=True)
+    for threads in (128, 256, 512):
+        for direction in ("top_down", "auto"):
+            for wb in (10, 0):
+                r = psb.bfs(p, algo, 0, final=True, threads=threads, direction=direction, window_bits=wb)
+                assert r["counts"] == counts and r["final"] == fin, (threads, direction, wb)
+
+
 def test_trivial_puzzles():
     assert psb.bfs(psb.PancakeSimple(2), "three_bit", 0)["counts"] == [1, 1]
     assert psb.bfs(psb.FourPegHanoiSimple(1), "two_bit", 0)["counts"] == [1, 3]
