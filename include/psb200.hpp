@@ -11,6 +11,7 @@
 //   SlidingTilePuzzleSimple     Puzzles/SlidingTilePuzzleSimple.h:8-40
 //   SlidingTilePuzzleGpu        Puzzles/SlidingTilePuzzleGpu.h:7-30
 //   PancakeSimple               Puzzles/PancakeSimple.h:8-37
+//   PancakeOptimized            Puzzles/PancakeOptimized.h:8-52
 //   FourPegHanoiSimple          Puzzles/FourPegHanoiSimple.h:8-40
 //   FourPegHanoiGPU             Puzzles/FourPegHanoiGPU.h:8-22
 //   InMemoryClassicBFS, InMemoryTwoBitBFS, InMemoryThreeBitBFS,
@@ -232,6 +233,22 @@ private:
 class PancakeSimple : public DevicePuzzle {
 public:
     explicit PancakeSimple(int size) : DevicePuzzle(PSB_PANCAKE, size, 0) {}
+};
+
+// PancakeOptimized (Puzzles/PancakeOptimized.h:8-52): the pancake puzzle in
+// the reference's GPU pancake index (a 29-bit split above 11 pancakes).
+// inverseIndex only affects CrossSegmentPostProcess in the reference's
+// segmented drivers; it is kept and reported by Name().
+class PancakeOptimized : public DevicePuzzle {
+public:
+    explicit PancakeOptimized(int size, bool inverseIndex = false)
+        : DevicePuzzle(PSB_PANCAKE_OPT, size, inverseIndex ? 1 : 0), size_(size), inv_(inverseIndex) {}
+    int Size() const { return size_; }
+    bool InvIndex() const { return inv_; }
+
+private:
+    int size_;
+    bool inv_;
 };
 
 class FourPegHanoiSimple : public DevicePuzzle {
@@ -484,6 +501,7 @@ using psb200::InMemoryClassicBFS;
 using psb200::InMemoryFrontierSearch;
 using psb200::InMemoryThreeBitBFS;
 using psb200::InMemoryTwoBitBFS;
+using psb200::PancakeOptimized;
 using psb200::PancakeSimple;
 using psb200::Puzzle;
 using psb200::PuzzleOptions;

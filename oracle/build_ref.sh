@@ -39,7 +39,8 @@ COMMON="Util.h Util.cpp Puzzle.h Puzzle.cpp Buffer.h Array.h BitArray.h InMemory
         StreamVInt.h StreamVInt.cpp FrontierCompression.h FrontierCompression.cpp
         OpBitsCompression.h OpBitsCompression.cpp"
 PUZZLES="PermutationMap.h PermutationMap.cpp SlidingTilePuzzleSimple.h SlidingTilePuzzleSimple.cpp
-         PancakeSimple.h PancakeSimple.cpp FourPegHanoiSimple.h FourPegHanoiSimple.cpp"
+         PancakeSimple.h PancakeSimple.cpp FourPegHanoiSimple.h FourPegHanoiSimple.cpp
+         PancakeOptimized.h PancakeOptimized.cpp"
 for f in $COMMON; do cp "$REF/Common/$f" "$SRC/Common/$f"; done
 for f in $PUZZLES; do cp "$REF/Puzzles/$f" "$SRC/Puzzles/$f"; done
 find "$SRC" -type f \( -name '*.h' -o -name '*.cpp' \) -print0 | xargs -0 sed -E -i \

@@ -70,11 +70,27 @@ static uint64_t factorial(int n) {
     return r;
 }
 
+/* PancakeOptimized's index (Puzzles/PancakeOptimized.cpp:26-77): for n <= 12
+ * the permutation rank; above, the rank of the first n-12 Lehmer digits
+ * (radices n .. 13) times 2^29 plus the rank of the last 12 (radices 12 .. 1),
+ * i.e. (rank / 12!) << 29 | rank % 12!.  Offsets >= 12! in a 2^29 block
+ * name no permutation. */
+#define ORC_F12 479001600ull
+static uint64_t popt_from_rank(int n, uint64_t r) { return n <= 12 ? r : ((r / ORC_F12) << 29) | (r % ORC_F12); }
+static int popt_to_rank(int n, uint64_t i, uint64_t* r) {
+    if (n <= 12) { *r = i; return 1; }
+    uint64_t lo = i & ((1ull << 29) - 1);
+    if (lo >= ORC_F12) return 0;
+    *r = (i >> 29) * ORC_F12 + lo;
+    return 1;
+}
+
 static int valid(const orc_puzzle* p) {
     if (!p) return 0;
     switch (p->kind) {
     case ORC_SLIDING: return p->a >= 1 && p->b >= 1 && p->a * p->b >= 2 && p->a * p->b <= 16;
     case ORC_PANCAKE: return p->a >= 2 && p->a <= 16;   /* PancakeSimple.cpp:26 */
+    case ORC_PANCAKE_OPT: return p->a >= 2 && p->a <= 16;  /* PancakeOptimized.cpp:81-86 */
     case ORC_HANOI4: return p->a >= 1 && p->a <= 31;
     }
     return 0;
@@ -90,6 +106,10 @@ int orc_info(const orc_puzzle* p, uint64_t* indexes, int* ops, int* branching, i
         n = factorial(p->a); o = p->a - 1; br = p->a - 1; od = 1; break;
     case ORC_HANOI4: /* FourPegHanoiSimple.h:14-20, .cpp:141-143 */
         n = 1ull << (2 * p->a); o = 4; br = 6; od = 1; break;
+    case ORC_PANCAKE_OPT: /* PancakeOptimized.h:14-20, .cpp:94-105: n! below 12, else prod(13..n) << 29 */
+        if (p->a < 12) n = factorial(p->a);
+        else { n = 1; for (int k = 13; k <= p->a; k++) n *= (uint64_t)k; n <<= 29; }
+        o = p->a - 1; br = p->a - 1; od = 1; break;
     }
     if (indexes) *indexes = n;
     if (ops) *ops = o;
@@ -138,8 +158,8 @@ int orc_parse(const orc_puzzle* p, const char* state, uint64_t* index) {
     int vals[64];
     int cnt = read_ints(state, vals, 64);
     if (cnt < 0) return -1;
-    if (p->kind == ORC_SLIDING || p->kind == ORC_PANCAKE) {
-        /* SlidingTilePuzzleSimple.cpp:52-59, PancakeSimple.cpp:53-60 */
+    if (p->kind == ORC_SLIDING || p->kind == ORC_PANCAKE || p->kind == ORC_PANCAKE_OPT) {
+        /* SlidingTilePuzzleSimple.cpp:52-59, PancakeSimple.cpp:53-60, PancakeOptimized.cpp:118-125 */
         int size = p->kind == ORC_SLIDING ? p->a * p->b : p->a;
         if (cnt != size) return -1;
         unsigned seen = 0;
@@ -148,6 +168,7 @@ int orc_parse(const orc_puzzle* p, const char* state, uint64_t* index) {
             seen |= 1u << vals[i];
         }
         *index = orc_perm_rank(vals, size);
+        if (p->kind == ORC_PANCAKE_OPT) *index = popt_from_rank(size, *index);
         return 0;
     }
     /* FourPegHanoiSimple.cpp:85-102 (ParseState) + :104-113 (StateToIndex):
@@ -166,9 +187,10 @@ int orc_parse(const orc_puzzle* p, const char* state, uint64_t* index) {
 int orc_to_string(const orc_puzzle* p, uint64_t index, char* buf, int cap) {
     if (!valid(p) || !buf || cap <= 0) return -1;
     char tmp[512]; int pos = 0;
-    if (p->kind == ORC_SLIDING || p->kind == ORC_PANCAKE) {
+    if (p->kind == ORC_SLIDING || p->kind == ORC_PANCAKE || p->kind == ORC_PANCAKE_OPT) {
         int size = p->kind == ORC_SLIDING ? p->a * p->b : p->a;
         int arr[16];
+        if (p->kind == ORC_PANCAKE_OPT && !popt_to_rank(size, index, &index)) return -1;
         orc_perm_unrank(index, arr, size);
         for (int i = 0; i < size; i++) pos += snprintf(tmp + pos, sizeof tmp - pos, i ? " %d" : "%d", arr[i]);
     } else {
@@ -278,11 +300,22 @@ static void hanoi_expand(int n, int sym, uint64_t index, uint32_t op, emitter* e
     }
 }
 
+/* PancakeOptimized::Expand (.cpp:128-139): PancakeSimple's moves in its own
+ * index; an offset that names no permutation has no children. */
+static void pancake_opt_expand(int n, uint64_t index, uint32_t opbits, emitter* e) {
+    uint64_t r;
+    if (!popt_to_rank(n, index, &r)) return;
+    uint64_t first = e->n;
+    pancake_expand(n, r, opbits, e);
+    for (uint64_t k = first; k < e->n; k++) e->children[k] = popt_from_rank(n, e->children[k]);
+}
+
 static void expand_one(const orc_puzzle* p, uint64_t index, uint32_t op, emitter* e) {
     switch (p->kind) {
     case ORC_SLIDING: sliding_expand(p->a, p->b, index, op, e); break;
     case ORC_PANCAKE: pancake_expand(p->a, index, op, e); break;
     case ORC_HANOI4: hanoi_expand(p->a, p->b, index, op, e); break;
+    case ORC_PANCAKE_OPT: pancake_opt_expand(p->a, index, op, e); break;
     }
 }
 

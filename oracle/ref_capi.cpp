@@ -9,6 +9,7 @@
 #include "Common/OpBitsCompression.h"
 #include "Common/StreamVInt.h"
 #include "Puzzles/FourPegHanoiSimple.h"
+#include "Puzzles/PancakeOptimized.h"
 #include "Puzzles/PancakeSimple.h"
 #include "Puzzles/PermutationMap.h"
 #include "Puzzles/SlidingTilePuzzleSimple.h"
@@ -26,6 +27,7 @@ std::unique_ptr<Puzzle> MakePuzzle(int kind, int a, int b) {
     case 1: return std::make_unique<SlidingTilePuzzleSimple>(a, b);
     case 2: return std::make_unique<PancakeSimple>(a);
     case 3: return std::make_unique<FourPegHanoiSimple>(a, b != 0);
+    case 4: return std::make_unique<PancakeOptimized>(a, b != 0);
     }
     return nullptr;
 }

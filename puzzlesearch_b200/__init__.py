@@ -15,7 +15,7 @@ import ctypes
 import os
 
 __all__ = [
-    "PsbError", "lib", "SlidingTilePuzzleSimple", "PancakeSimple", "FourPegHanoiSimple",
+    "PsbError", "lib", "SlidingTilePuzzleSimple", "PancakeSimple", "PancakeOptimized", "FourPegHanoiSimple",
     "InMemoryTwoBitBFS", "InMemoryThreeBitBFS", "InMemoryFrontierSearch", "InMemoryClassicBFS",
     "bfs", "bfs_segmented", "BfsSession", "TWO_BIT", "THREE_BIT", "FRONTIER", "CLASSIC", "INVALID_INDEX",
 ]
@@ -23,7 +23,7 @@ __all__ = [
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PSB_LIB") or os.path.join(HERE, "libpsb200.so")
 
-SLIDING, PANCAKE, HANOI4 = 1, 2, 3
+SLIDING, PANCAKE, HANOI4, PANCAKE_OPT = 1, 2, 3, 4
 TWO_BIT, THREE_BIT, FRONTIER, CLASSIC = 1, 2, 3, 4
 ALGOS = {"two_bit": TWO_BIT, "three_bit": THREE_BIT, "frontier": FRONTIER, "classic": CLASSIC}
 INVALID_INDEX = (1 << 64) - 1
@@ -297,6 +297,14 @@ class PancakeSimple(Puzzle):
 
     def __init__(self, size):
         super().__init__(PANCAKE, size, 0)
+
+
+class PancakeOptimized(Puzzle):
+    """Puzzles/PancakeOptimized.h: the pancake moves in the reference's GPU
+    pancake index ((rank / 12!) << 29 | rank % 12! above 11 pancakes)."""
+
+    def __init__(self, size, inverseIndex=False):
+        super().__init__(PANCAKE_OPT, size, 1 if inverseIndex else 0)
 
 
 class FourPegHanoiSimple(Puzzle):

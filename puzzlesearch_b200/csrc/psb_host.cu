@@ -315,6 +315,17 @@ void unrank_host(uint64_t index, int* v, int n) {
     }
 }
 
+// PancakeOptimized's index from the permutation rank and back (n >= 12;
+// Puzzles/PancakeOptimized.cpp:26-77).
+constexpr uint64_t kF12 = 479001600ull;
+uint64_t opt_from_rank(uint64_t r) { return ((r / kF12) << 29) | (r % kF12); }
+bool opt_to_rank(uint64_t i, uint64_t* r) {
+    const uint64_t lo = i & ((uint64_t(1) << 29) - 1);
+    if (lo >= kF12) return false;
+    *r = (i >> 29) * kF12 + lo;
+    return true;
+}
+
 bool read_ints(const char* s, std::vector<int>& out) {
     std::istringstream in(s);
     std::string tok;
@@ -440,6 +451,18 @@ int psb_puzzle_create(int kind, int a, int b, psb_puzzle** out) {
         p->cells = a; p->n_states = factorial(a); p->ops = a - 1; p->branching = a - 1; p->odd = 1;
         ok = psb::pancake_kernels(a, &p->k);
         break;
+    case PSB_PANCAKE_OPT:  // PancakeOptimized.h:14-20, .cpp:81-105
+        if (a < 2 || a > 16) return fail(PSB_ERR_ARG, "pancake size %d: need 2..16", a);
+        p->cells = a; p->ops = a - 1; p->branching = a - 1; p->odd = 1;
+        if (a < 12) {
+            p->n_states = factorial(a);
+            ok = psb::pancake_kernels(a, &p->k);
+        } else {
+            p->n_states = uint64_t(1) << 29;
+            for (int k = 13; k <= a; k++) p->n_states *= uint64_t(k);
+            ok = psb::pancake_opt_kernels(a, &p->k);
+        }
+        break;
     case PSB_HANOI4:  // FourPegHanoiSimple.h:14-20, .cpp:141-143
         if (a < 1 || a > 31) return fail(PSB_ERR_ARG, "hanoi disks %d: need 1..31", a);
         p->cells = 0; p->n_states = uint64_t(1) << (2 * a); p->ops = 4; p->branching = 6; p->odd = 1;
@@ -475,6 +498,9 @@ int psb_puzzle_name(const psb_puzzle* p, char* buf, int cap) {
     case PSB_SLIDING: s << "Sliding-Tile simple: " << p->a << " x " << p->b; break;   // SlidingTilePuzzleSimple.cpp:27-32
     case PSB_PANCAKE: s << "Pancake simple, size: " << p->a; break;                   // PancakeSimple.cpp:29-33
     case PSB_HANOI4: s << "Four-Peg Hanoi Towers, size=" << p->a << "; symmetry=" << (p->b ? 1 : 0); break;  // FourPegHanoiSimple.cpp:129-135
+    case PSB_PANCAKE_OPT:  // PancakeOptimized.cpp:88-92
+        s << "Pancake optimized (29 bit segment), size: " << p->a << "; invIdx: " << (p->b ? 1 : 0);
+        break;
     }
     const std::string str = s.str();
     if (int(str.size()) + 1 > cap) return fail(PSB_ERR_CAPACITY, "name buffer too small");
@@ -495,6 +521,7 @@ int psb_parse(const psb_puzzle* p, const char* state, uint64_t* index) {
             seen |= 1u << x;
         }
         *index = rank_host(v.data(), p->cells);
+        if (p->kind == PSB_PANCAKE_OPT && p->cells >= 12) *index = opt_from_rank(*index);
         return PSB_OK;
     }
     // FourPegHanoiSimple.cpp:85-113: disks (1-based) listed peg by peg, a 0 between pegs.
@@ -515,6 +542,10 @@ int psb_to_string(const psb_puzzle* p, uint64_t index, char* buf, int cap) {
     std::ostringstream s;
     if (p->kind != PSB_HANOI4) {
         int v[16];
+        if (p->kind == PSB_PANCAKE_OPT && p->cells >= 12) {
+            if (!opt_to_rank(index, &index)) return fail(PSB_ERR_ARG, "offset %llu of its 2^29 block names no permutation",
+                                                          (unsigned long long)(index & ((1ull << 29) - 1)));
+        }
         unrank_host(index, v, p->cells);
         for (int i = 0; i < p->cells; i++) s << (i ? " " : "") << v[i];
     } else {

@@ -120,6 +120,53 @@ struct PancakeK {
         Pancake<N>::template expand_range<false>(i, 0u, first, last, e);
     }
 };
+// PancakeOptimized (Puzzles/PancakeOptimized.cpp:26-139): the pancake moves
+// in the reference's GPU pancake index, for n >= 12: (rank / 12!) << 29 |
+// (rank % 12!), where rank is PancakeSimple's index; offsets >= 12! inside a
+// 2^29 block name no permutation and have no children.  The level kernel
+// runs it through the generic per-state path (no per-word flip tricks:
+// their residue classes are those of the plain rank).
+template <int N>
+struct PancakeOptK {
+    static constexpr int kBranch = N - 1;
+    static constexpr int kOps = N - 1;
+    static constexpr int kProbeRound = 4 < N - 1 ? 4 : N - 1;
+    static constexpr bool kPairOp0 = false;
+    static constexpr bool kFlip3Op1 = false;
+    static constexpr bool kFlip4Op2 = false;
+    static constexpr bool kChunkPrefix = false;
+    static constexpr bool kSymMult = false;
+    static constexpr uint32_t kBlock = 1;
+    struct Prefix { uint32_t unused; };
+    static constexpr uint64_t kF12 = 479001600ull;  // 12!
+    __device__ __forceinline__ static bool to_rank(uint64_t i, uint64_t& r) {
+        const uint64_t lo = i & ((uint64_t(1) << 29) - 1);
+        if (lo >= kF12) return false;
+        r = (i >> 29) * kF12 + lo;
+        return true;
+    }
+    __device__ __forceinline__ static uint64_t from_rank(uint64_t r) { return ((r / kF12) << 29) | (r % kF12); }
+    template <class E>
+    struct Wrap {  // children come out as plain ranks; emit them in this index
+        E& e;
+        __device__ __forceinline__ void operator()(uint64_t c, uint32_t op) { e(from_rank(c), op); }
+    };
+    template <bool kOpBits, class E>
+    __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs&, E& e) {
+        uint64_t r;
+        if (!to_rank(i, r)) return;
+        Wrap<E> w{e};
+        Pancake<N>::template expand<kOpBits>(r, ob, w);
+    }
+    template <class E>
+    __device__ __forceinline__ static void probe_range(uint64_t i, int first, int last, const PuzzleArgs&, E& e) {
+        uint64_t r;
+        if (!to_rank(i, r)) return;
+        Wrap<E> w{e};
+        Pancake<N>::template expand_range<false>(r, 0u, first, last, w);
+    }
+};
+
 template <int N>
 struct SlidingK {
     static constexpr int kBranch = 4;
@@ -1151,6 +1198,7 @@ PuzzleKernels make_kernels() {
 
 // Defined in psb_pancake.cu, psb_sliding.cu, psb_hanoi.cu.
 bool pancake_kernels(int n, PuzzleKernels* out);
+bool pancake_opt_kernels(int n, PuzzleKernels* out);  // psb_pancake_opt.cu, n = 12..16
 bool sliding_kernels(int cells, PuzzleKernels* out);
 bool hanoi_kernels(PuzzleKernels* out);
 

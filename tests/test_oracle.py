@@ -296,3 +296,28 @@ def test_opbits_bytes_match_reference():
         for n in (8, 64, 4096):
             ops = [rng.randrange(1 << bits) for _ in range(n)]
             assert O.opbits_encode(bits, ops) == O.ref_opbits_encode(bits, ops), (bits, n)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_pancake_optimized_matches_reference():
+    """PancakeOptimized (Puzzles/PancakeOptimized.cpp): the oracle's index,
+    Expand and BFS equal the reference class's; below 12 pancakes the index is
+    PancakeSimple's, above it the 29-bit split of the same rank."""
+    rng = random.Random(12)
+    for n in (5, 8, 11, 12, 13, 14, 16):
+        spec = ["pancake_opt", n, 0]
+        N = n_states(spec)
+        parents = []
+        while len(parents) < 300:
+            p = rng.randrange(N)
+            if n < 12 or (p & ((1 << 29) - 1)) < math.factorial(12):
+                parents.append(p)
+        ops = [rng.randrange(1 << (n - 1)) if i % 2 else 0 for i in range(len(parents))]
+        assert O.expand(spec, parents, ops) == O.ref_expand(spec, parents, ops), n
+        for p in parents[:30]:
+            assert O.parse(spec, O.to_string(spec, p)) == p
+    for n in (6, 9, 10):
+        start = O.to_string(["pancake_opt", n, 0], 0)
+        assert O.bfs(["pancake_opt", n, 0], "three_bit")[0] == O.ref_bfs(["pancake_opt", n, 0], "three_bit", start)
+    assert n_states(["pancake_opt", 12, 0]) == 1 << 29
+    assert n_states(["pancake_opt", 14, 0]) == 13 * 14 << 29
