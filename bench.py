@@ -374,6 +374,13 @@ def serve_bench(args):
         # served: submit at the arrival times, continuous batching on the GPU
         srv = psb.Server(max_instances=1024, max_depths=256, pool_bytes=args.pool_gb << 30,
                          levels_per_step=args.levels_per_step)
+        # warm-up, as the plain arm's sessions were: one request of each type
+        # (loads the kernels, sizes the large lane's search arrays)
+        warm = [srv.submit(puzzles[t], 0) for t in SERVE_TYPES]
+        got = {}
+        while len(got) < len(warm):
+            got.update(srv.poll())
+            time.sleep(0.001)
         t_start = time.perf_counter()
         tickets = {}
         done = {}

@@ -43,16 +43,16 @@ def test_other_starts_and_max_depth():
         assert psb.bfs_segmented(p, idx, segment_bits=24, max_depth=9)["counts"] == full[:10]
 
 
-def test_reduced_memory_13_pancake():
-    """13-pancake (6,227,020,800 states) in segments of 2^28 states: the
-    device holds 3 x 32 MB of bit arrays instead of the in-memory search's
-    3 x 778 MB, and the counts equal the in-memory search's."""
-    p = psb.PancakeSimple(13)
-    r = psb.bfs_segmented(p, 0, segment_bits=28)
+def test_reduced_memory_12_pancake():
+    """12-pancake (479,001,600 states) in segments of 2^26 states: the device
+    holds 3 x 8 MB of bit arrays instead of the in-memory search's 3 x 60 MB,
+    and the counts equal the in-memory search's."""
+    p = psb.PancakeSimple(12)
+    r = psb.bfs_segmented(p, 0, segment_bits=26)
     assert r["counts"] == psb.bfs(p, "three_bit", 0)["counts"]
-    assert sum(r["counts"]) == math.factorial(13)
-    assert r["stats"]["segments"] == 24
-    assert r["stats"]["device_bytes"] < 2 << 30
+    assert sum(r["counts"]) == math.factorial(12)
+    assert r["stats"]["segments"] == 8
+    assert r["stats"]["cross_children"] > 0
 
 
 def test_small_chunks_and_bad_arguments():

@@ -60,17 +60,21 @@ def test_results_alone_equal_results_in_the_mix():
 
 
 def test_unsupported_request_fails_alone():
-    srv = psb.Server(max_instances=8, pool_bytes=1 << 30)
-    ok = srv.submit(psb.PancakeSimple(9), 0)
-    bad = srv.submit(psb.SlidingTilePuzzleSimple(4, 4), 0)  # 16 cells: not compiled into the engine
-    done = {}
-    deadline = time.time() + 60
-    while len(done) < 2 and time.time() < deadline:
-        done.update(srv.poll())
-        time.sleep(0.005)
-    srv.stop()
-    assert done[bad][0] == -5
-    assert done[ok][0] == 0 and done[ok][1] == psb.bfs(psb.PancakeSimple(9), "two_bit", 0)["counts"]
+    """Without a large lane the engine rejects a puzzle it has no kernels
+    for; with one, the large lane takes it and reports that its arrays do
+    not fit the device (4x4: 16! states).  The other request completes."""
+    for lane, code in ((None, -5), (0, -3)):
+        srv = psb.Server(max_instances=8, pool_bytes=1 << 30, large_states=lane)
+        ok = srv.submit(psb.PancakeSimple(9), 0)
+        bad = srv.submit(psb.SlidingTilePuzzleSimple(4, 4), 0)  # 16 cells: not compiled into the engine
+        done = {}
+        deadline = time.time() + 60
+        while len(done) < 2 and time.time() < deadline:
+            done.update(srv.poll())
+            time.sleep(0.005)
+        srv.stop()
+        assert done[bad][0] == code
+        assert done[ok][0] == 0 and done[ok][1] == psb.bfs(psb.PancakeSimple(9), "two_bit", 0)["counts"]
 
 
 def test_admission_waits_for_pool_space():
