@@ -48,14 +48,15 @@ enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 //
 // Variants 1 and 2 of the top-down two-bit and three-bit kernels (the
 // autotuner's threads-per-block dimension, psb_bfs_opts.threads): 512 and
-// 128 threads per block with the same register budget per thread (two-bit:
-// 1024 resident threads per SM at 64 registers; three-bit: no cap at 512,
-// two blocks at 128).
+// 128 threads per block.  For two-bit they also trade resident warps for
+// registers (up to 128 per thread, 512 resident threads per SM): the
+// 13- and 14-pancake kernels issue their far reads early and keep them in
+// flight across the near children, which needs registers rather than warps.
 template <int MODE, bool BU = false, int V = 0>
 struct Shape {
     static constexpr int threads = V == 1 ? 512 : V == 2 ? 128 : 256;
     static constexpr int min_blocks = BU ? 4
-                                    : MODE == kTwoBit ? (V == 1 ? 2 : V == 2 ? 8 : 4)
+                                    : MODE == kTwoBit ? (V == 1 ? 1 : 4)
                                     : MODE == kFrontier ? 2
                                     : (V == 2 ? 2 : 1);
 };
@@ -508,6 +509,32 @@ struct Emitter {
         const uint64_t o = c - base;
         if (o < span) mark_local(uint32_t(o), op);
         else mark_remote<true>(c, op);
+    }
+
+    // The same in two steps (see EmitSplitFar): a two-bit mark that must
+    // read its target first issues the read here and completes in
+    // far_finish, after the parent's near children; every other mark is
+    // made at once.
+    __device__ __forceinline__ FarTicket far_issue(uint64_t c, uint32_t op) {
+        const uint64_t o = c - base;
+        if constexpr (MODE == kTwoBit) {
+            if (o >= span && c < n_states && !(farbits && far_all))
+                return FarTicket{ld_cg_far(reinterpret_cast<const unsigned long long*>(gmarks) + (c >> 5)), true};
+        }
+        far(c, op);
+        return FarTicket{0, false};
+    }
+    __device__ __forceinline__ void far_finish(uint64_t c, uint32_t, const FarTicket& t) {
+        if constexpr (MODE == kTwoBit) {
+            if (!t.pending) return;
+            ++children;
+            if (((t.word >> (2u * (uint32_t(c) & 31u))) & 3u) == 0) {  // UNVISITED -> NEXT
+                flag_window(c);
+                atomicOr(reinterpret_cast<unsigned long long*>(gmarks) + (c >> 5),
+                         (unsigned long long)next_pat << (2u * (uint32_t(c) & 31u)));
+                ++marked;
+            }
+        }
     }
 
     // Child = parent + delta, with the parent at parent_off in the window.

@@ -38,6 +38,21 @@ struct EmitFar : std::false_type {};
 template <class E>
 struct EmitFar<E, decltype(void(&E::far))> : std::true_type {};
 
+// Emitters with members far_issue(child, op) and far_finish(child, op, ticket)
+// take the far children in two steps: the first starts whatever the mark
+// has to read and returns a ticket, the second completes the mark.  The
+// expander issues the far children first and finishes them after the near
+// ones, so the reads overlap the near children's arithmetic.
+template <class E, class = void>
+struct EmitSplitFar : std::false_type {};
+template <class E>
+struct EmitSplitFar<E, decltype(void(&E::far_issue))> : std::true_type {};
+
+struct FarTicket {
+    uint64_t word;  // the target's code word, when `pending`
+    bool pending;
+};
+
 __host__ __device__ constexpr uint64_t fact(int k) { return k <= 1 ? 1 : uint64_t(k) * fact(k - 1); }
 constexpr uint32_t kF12 = 479001600u;  // 12!
 
@@ -232,14 +247,44 @@ struct Pancake {
     __device__ __forceinline__ static void children(uint64_t index, const uint32_t (&d)[N], const uint32_t (&pre)[N],
                                                     const uint32_t (&pb)[N], uint32_t opbits, int first, int last,
                                                     Emit& emit) {
+        // Far children first, for emitters that take them in two steps.
+        constexpr bool kSplit = EmitSplitFar<Emit>::value && (N > 12);
+        constexpr int kFarN = N > 12 ? N - 12 : 1;
+        uint64_t far_child[kFarN];
+        FarTicket far_ticket[kFarN];
+        if constexpr (kSplit) {
+            uint64_t low = 0;
+#pragma unroll
+            for (int m = 2; m <= N; ++m) {
+                low += uint64_t(d[N - m]) * fact(m - 1);
+                if (m <= 12) continue;
+                const int op = m - 2, k = m - 13;
+                far_ticket[k].pending = false;
+                if (op < first || op >= last || (kOpBits && (opbits >> op) & 1u)) {
+                    far_child[k] = kInvalidIndex;
+                    continue;
+                }
+                const uint32_t excl = pre[N - m];
+                uint32_t s32 = 0, t = 0;
+#pragma unroll
+                for (int q = 1; q < m; ++q) {
+                    const uint32_t c = __popc(pb[N - m + q] & ~excl);
+                    if (q < 12) s32 += uint32_t(fact(q)) * c;
+                    else t += uint32_t(fact(q) / kF12) * c;
+                }
+                far_child[k] = index - low + (uint64_t(t) * kF12 + s32);
+                far_ticket[k] = emit.far_issue(far_child[k], uint32_t(op));
+            }
+        }
         uint32_t low32 = 0;  // low_m for m <= 12 (d[n-1] is always 0)
         uint64_t low64 = 0;  // low_m for m > 12
 #pragma unroll
         for (int m = 2; m <= N; ++m) {
+            if (kSplit && m > 12) break;
             if (m <= 12) low32 += d[N - m] * uint32_t(fact(m - 1));
             else low64 = (m == 13 ? uint64_t(low32) : low64) + uint64_t(d[N - m]) * fact(m - 1);
             const int op = m - 2;
-            if (op >= last) return;
+            if (op >= last) break;
             if (op < first || (kOpBits && (opbits >> op) & 1u)) continue;
             const uint32_t excl = pre[N - m];
             if (m <= 12) {  // m is a compile-time constant after unrolling
@@ -261,6 +306,11 @@ struct Pancake {
                 if constexpr (EmitFar<Emit>::value) emit.far(child, uint32_t(op));
                 else emit(child, uint32_t(op));
             }
+        }
+        if constexpr (kSplit) {
+#pragma unroll
+            for (int k = 0; k < N - 12; ++k)
+                if (far_child[k] != kInvalidIndex) emit.far_finish(far_child[k], uint32_t(k + 11), far_ticket[k]);
         }
     }
 };
