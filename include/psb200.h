@@ -46,9 +46,13 @@ enum {
     PSB_SLIDING = 1, /* SlidingTilePuzzleSimple(width=a, height=b), 2 <= a*b <= 16 */
     PSB_PANCAKE = 2, /* PancakeSimple(size=a), 2 <= a <= 16 */
     PSB_HANOI4 = 3,  /* FourPegHanoiSimple(disks=a, useSymmetry=b), 1 <= a <= 31 */
-    PSB_PANCAKE_OPT = 4 /* PancakeOptimized(size=a, inverseIndex=b), 2 <= a <= 16: for a >= 12 the index is
-                           (rank / 12!) << 29 | rank % 12! over prod(13..a) * 2^29 indexes
-                           (Puzzles/PancakeOptimized.cpp:26-105); offsets >= 12! are never reached */
+    PSB_PANCAKE_OPT = 4, /* PancakeOptimized(size=a, inverseIndex=b), 2 <= a <= 16: for a >= 12 the index is
+                            (rank / 12!) << 29 | rank % 12! over prod(13..a) * 2^29 indexes
+                            (Puzzles/PancakeOptimized.cpp:26-105); offsets >= 12! are never reached */
+    PSB_HANOI4_OPT = 5   /* FourPegHanoiOptimized(disks=a, useSymmetry=b): FourPegHanoiSimple's index; with
+                            symmetry it restores the peg order only when a move empties or fills a peg
+                            (Puzzles/FourPegHanoiOptimized.cpp:180-204), the same children for canonical
+                            states */
 };
 
 /* In-memory search algorithms (Common/InMemoryBFS.h:5-11). */

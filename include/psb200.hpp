@@ -14,6 +14,7 @@
 //   PancakeOptimized            Puzzles/PancakeOptimized.h:8-52
 //   FourPegHanoiSimple          Puzzles/FourPegHanoiSimple.h:8-40
 //   FourPegHanoiGPU             Puzzles/FourPegHanoiGPU.h:8-22
+//   FourPegHanoiOptimized       Puzzles/FourPegHanoiOptimized.h:8-40
 //   InMemoryClassicBFS, InMemoryTwoBitBFS, InMemoryThreeBitBFS,
 //   InMemoryFrontierSearch      Common/InMemoryBFS.h:5-11
 //   StoreOptions, PuzzleOptions, DiskBased*BFS / *FrontierSearch
@@ -263,6 +264,21 @@ private:
     bool sym_;
 };
 
+// FourPegHanoiOptimized (Puzzles/FourPegHanoiOptimized.h:8-40): the Simple
+// class's index space; with symmetry the peg order is restored only when a
+// move empties or fills a peg (the same children for every reachable state).
+class FourPegHanoiOptimized : public DevicePuzzle {
+public:
+    explicit FourPegHanoiOptimized(int size, bool useSymmetry = false)
+        : DevicePuzzle(PSB_HANOI4_OPT, size, useSymmetry ? 1 : 0), size_(size), sym_(useSymmetry) {}
+    int Size() const { return size_; }
+    bool UseSymmetry() const { return sym_; }
+
+private:
+    int size_;
+    bool sym_;
+};
+
 // The reference's GPU Hanoi class: the Simple class's 4^n index space, at
 // most 24 disks (Puzzles/FourPegHanoiGPU.h:10-14).
 class FourPegHanoiGPU : public DevicePuzzle {
@@ -494,6 +510,7 @@ using psb200::DiskBasedTwoBitBFS;
 using psb200::ExpandBuffer;
 using psb200::ExpandHint;
 using psb200::FourPegHanoiGPU;
+using psb200::FourPegHanoiOptimized;
 using psb200::FourPegHanoiSimple;
 using psb200::HanoiSearch;
 using psb200::HanoiTowers;

@@ -12,8 +12,8 @@
 #   * `static` dropped from explicit template specializations (MSVC accepts it,
 #     GCC does not)
 #   * a generated <intrin.h> mapping the MSVC intrinsics to GCC builtins, and
-#     the AVX-512VL byte load/store intrinsics to their SSE2 equivalents so the
-#     library runs on any x86-64-v3 host.
+#     the AVX-512VL load/store intrinsics to their SSE2 / AVX2 equivalents so
+#     the library runs on any x86-64-v3 host.
 # Outputs: oracle/_ref/libpsbref.so (C ABI from oracle/ref_capi.cpp),
 #          oracle/_ref/psbref (CLI used for the CPU baseline timing) and
 #          oracle/_ref/psbref_mt (multi-threaded level loop over the reference's
@@ -40,7 +40,7 @@ COMMON="Util.h Util.cpp Puzzle.h Puzzle.cpp Buffer.h Array.h BitArray.h InMemory
         OpBitsCompression.h OpBitsCompression.cpp"
 PUZZLES="PermutationMap.h PermutationMap.cpp SlidingTilePuzzleSimple.h SlidingTilePuzzleSimple.cpp
          PancakeSimple.h PancakeSimple.cpp FourPegHanoiSimple.h FourPegHanoiSimple.cpp
-         PancakeOptimized.h PancakeOptimized.cpp"
+         PancakeOptimized.h PancakeOptimized.cpp FourPegHanoiOptimized.h FourPegHanoiOptimized.cpp"
 for f in $COMMON; do cp "$REF/Common/$f" "$SRC/Common/$f"; done
 for f in $PUZZLES; do cp "$REF/Puzzles/$f" "$SRC/Puzzles/$f"; done
 find "$SRC" -type f \( -name '*.h' -o -name '*.cpp' \) -print0 | xargs -0 sed -E -i \
@@ -70,6 +70,7 @@ cat > "$SRC/msvc_compat.h" <<'EOF'
 #define _mm_loadu_epi8(p) _mm_loadu_si128((const __m128i*)(p))
 #define _mm_loadu_epi32(p) _mm_loadu_si128((const __m128i*)(p))
 #define _mm_storeu_epi8(p, v) _mm_storeu_si128((__m128i*)(p), (v))
+#define _mm256_storeu_epi64(p, v) _mm256_storeu_si256((__m256i*)(p), (v))
 #define __forceinline inline __attribute__((always_inline))
 static inline unsigned long long __popcnt64(unsigned long long v) { return __builtin_popcountll(v); }
 static inline unsigned int __popcnt(unsigned int v) { return __builtin_popcount(v); }

@@ -10,7 +10,7 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-KIND = {"sliding": 1, "pancake": 2, "hanoi4": 3, "pancake_opt": 4}
+KIND = {"sliding": 1, "pancake": 2, "hanoi4": 3, "pancake_opt": 4, "hanoi4_opt": 5}
 ALGO = {"two_bit": 1, "three_bit": 2, "frontier": 3, "classic": 4}
 
 u64p = ctypes.POINTER(ctypes.c_uint64)

@@ -91,7 +91,7 @@ static int valid(const orc_puzzle* p) {
     case ORC_SLIDING: return p->a >= 1 && p->b >= 1 && p->a * p->b >= 2 && p->a * p->b <= 16;
     case ORC_PANCAKE: return p->a >= 2 && p->a <= 16;   /* PancakeSimple.cpp:26 */
     case ORC_PANCAKE_OPT: return p->a >= 2 && p->a <= 16;  /* PancakeOptimized.cpp:81-86 */
-    case ORC_HANOI4: return p->a >= 1 && p->a <= 31;
+    case ORC_HANOI4: case ORC_HANOI4_OPT: return p->a >= 1 && p->a <= 31;
     }
     return 0;
 }
@@ -104,7 +104,7 @@ int orc_info(const orc_puzzle* p, uint64_t* indexes, int* ops, int* branching, i
         n = factorial(p->a * p->b); o = 4; br = 4; od = 0; break;
     case ORC_PANCAKE: /* PancakeSimple.h:13-19, .cpp:36-40 */
         n = factorial(p->a); o = p->a - 1; br = p->a - 1; od = 1; break;
-    case ORC_HANOI4: /* FourPegHanoiSimple.h:14-20, .cpp:141-143 */
+    case ORC_HANOI4: case ORC_HANOI4_OPT: /* FourPegHanoiSimple.h:14-20, .cpp:141-143; FourPegHanoiOptimized.cpp:164-166 */
         n = 1ull << (2 * p->a); o = 4; br = 6; od = 1; break;
     case ORC_PANCAKE_OPT: /* PancakeOptimized.h:14-20, .cpp:94-105: n! below 12, else prod(13..n) << 29 */
         if (p->a < 12) n = factorial(p->a);
@@ -279,7 +279,9 @@ static int hanoi_restore_symmetry(hstate* s, int dst) {
 
 /* FourPegHanoiSimple.cpp:156-174: for each peg pair (p1<p2) move the smaller
  * top disk; the operator bit tested is the source peg, the child's operator is
- * the destination peg (relabelled when symmetry is on). */
+ * the destination peg (relabelled when symmetry is on).  sym 2 is
+ * FourPegHanoiOptimized (.cpp:180-204): the order is restored only when the
+ * move lands on an empty peg or empties its source. */
 static void hanoi_expand(int n, int sym, uint64_t index, uint32_t op, emitter* e) {
     hstate st = hanoi_from_index(n, index);
     for (int a = 0; a < 4; a++) {
@@ -294,7 +296,8 @@ static void hanoi_expand(int n, int sym, uint64_t index, uint32_t op, emitter* e
             s2.m[src] &= ~(1ull << disk);
             s2.m[dst] |= 1ull << disk;
             int childOp = dst;
-            if (sym) childOp = hanoi_restore_symmetry(&s2, dst);
+            const int dst_was_empty = st.m[dst] == 0, src_now_empty = s2.m[src] == 0;
+            if (sym == 1 || (sym == 2 && (dst_was_empty || src_now_empty))) childOp = hanoi_restore_symmetry(&s2, dst);
             if (!(op & (1u << src))) emit(e, hanoi_to_index(&s2), (uint32_t)childOp);
         }
     }
@@ -314,7 +317,8 @@ static void expand_one(const orc_puzzle* p, uint64_t index, uint32_t op, emitter
     switch (p->kind) {
     case ORC_SLIDING: sliding_expand(p->a, p->b, index, op, e); break;
     case ORC_PANCAKE: pancake_expand(p->a, index, op, e); break;
-    case ORC_HANOI4: hanoi_expand(p->a, p->b, index, op, e); break;
+    case ORC_HANOI4: hanoi_expand(p->a, p->b ? 1 : 0, index, op, e); break;
+    case ORC_HANOI4_OPT: hanoi_expand(p->a, p->b ? 2 : 0, index, op, e); break;
     case ORC_PANCAKE_OPT: pancake_opt_expand(p->a, index, op, e); break;
     }
 }

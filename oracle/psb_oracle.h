@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-enum { ORC_SLIDING = 1, ORC_PANCAKE = 2, ORC_HANOI4 = 3, ORC_PANCAKE_OPT = 4 };
+enum { ORC_SLIDING = 1, ORC_PANCAKE = 2, ORC_HANOI4 = 3, ORC_PANCAKE_OPT = 4, ORC_HANOI4_OPT = 5 };
 enum { ORC_TWO_BIT = 1, ORC_THREE_BIT = 2, ORC_FRONTIER = 3, ORC_CLASSIC = 4 };
 
 #define ORC_INVALID_INDEX (~(uint64_t)0)

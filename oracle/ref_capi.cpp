@@ -8,6 +8,7 @@
 #include "Common/FrontierCompression.h"
 #include "Common/OpBitsCompression.h"
 #include "Common/StreamVInt.h"
+#include "Puzzles/FourPegHanoiOptimized.h"
 #include "Puzzles/FourPegHanoiSimple.h"
 #include "Puzzles/PancakeOptimized.h"
 #include "Puzzles/PancakeSimple.h"
@@ -28,6 +29,7 @@ std::unique_ptr<Puzzle> MakePuzzle(int kind, int a, int b) {
     case 2: return std::make_unique<PancakeSimple>(a);
     case 3: return std::make_unique<FourPegHanoiSimple>(a, b != 0);
     case 4: return std::make_unique<PancakeOptimized>(a, b != 0);
+    case 5: return std::make_unique<FourPegHanoiOptimized>(a, b != 0);
     }
     return nullptr;
 }

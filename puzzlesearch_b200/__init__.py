@@ -15,7 +15,7 @@ import ctypes
 import os
 
 __all__ = [
-    "PsbError", "lib", "SlidingTilePuzzleSimple", "PancakeSimple", "PancakeOptimized", "FourPegHanoiSimple",
+    "PsbError", "lib", "SlidingTilePuzzleSimple", "PancakeSimple", "PancakeOptimized", "FourPegHanoiOptimized", "FourPegHanoiSimple",
     "InMemoryTwoBitBFS", "InMemoryThreeBitBFS", "InMemoryFrontierSearch", "InMemoryClassicBFS",
     "bfs", "bfs_segmented", "BfsSession", "TWO_BIT", "THREE_BIT", "FRONTIER", "CLASSIC", "INVALID_INDEX",
 ]
@@ -23,7 +23,7 @@ __all__ = [
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PSB_LIB") or os.path.join(HERE, "libpsb200.so")
 
-SLIDING, PANCAKE, HANOI4, PANCAKE_OPT = 1, 2, 3, 4
+SLIDING, PANCAKE, HANOI4, PANCAKE_OPT, HANOI4_OPT = 1, 2, 3, 4, 5
 TWO_BIT, THREE_BIT, FRONTIER, CLASSIC = 1, 2, 3, 4
 ALGOS = {"two_bit": TWO_BIT, "three_bit": THREE_BIT, "frontier": FRONTIER, "classic": CLASSIC}
 INVALID_INDEX = (1 << 64) - 1
@@ -312,6 +312,14 @@ class FourPegHanoiSimple(Puzzle):
 
     def __init__(self, size, useSymmetry=False):
         super().__init__(HANOI4, size, 1 if useSymmetry else 0)
+
+
+class FourPegHanoiOptimized(Puzzle):
+    """Puzzles/FourPegHanoiOptimized.h: FourPegHanoiSimple's index; with
+    symmetry the peg order is restored only when a move empties or fills a peg."""
+
+    def __init__(self, size, useSymmetry=False):
+        super().__init__(HANOI4_OPT, size, 1 if useSymmetry else 0)
 
 
 def _algo(algo):

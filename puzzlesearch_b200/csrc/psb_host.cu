@@ -463,10 +463,11 @@ int psb_puzzle_create(int kind, int a, int b, psb_puzzle** out) {
             ok = psb::pancake_opt_kernels(a, &p->k);
         }
         break;
-    case PSB_HANOI4:  // FourPegHanoiSimple.h:14-20, .cpp:141-143
+    case PSB_HANOI4:      // FourPegHanoiSimple.h:14-20, .cpp:141-143
+    case PSB_HANOI4_OPT:  // FourPegHanoiOptimized.h:8-20, .cpp:164-166: the same index space
         if (a < 1 || a > 31) return fail(PSB_ERR_ARG, "hanoi disks %d: need 1..31", a);
         p->cells = 0; p->n_states = uint64_t(1) << (2 * a); p->ops = 4; p->branching = 6; p->odd = 1;
-        p->pz.disks = a; p->pz.sym = b ? 1 : 0;
+        p->pz.disks = a; p->pz.sym = b ? (kind == PSB_HANOI4_OPT ? 2 : 1) : 0;
         ok = psb::hanoi_kernels(&p->k);
         break;
     default:
@@ -498,6 +499,9 @@ int psb_puzzle_name(const psb_puzzle* p, char* buf, int cap) {
     case PSB_SLIDING: s << "Sliding-Tile simple: " << p->a << " x " << p->b; break;   // SlidingTilePuzzleSimple.cpp:27-32
     case PSB_PANCAKE: s << "Pancake simple, size: " << p->a; break;                   // PancakeSimple.cpp:29-33
     case PSB_HANOI4: s << "Four-Peg Hanoi Towers, size=" << p->a << "; symmetry=" << (p->b ? 1 : 0); break;  // FourPegHanoiSimple.cpp:129-135
+    case PSB_HANOI4_OPT:  // FourPegHanoiOptimized.cpp:151-157
+        s << "Four-Peg Hanoi Towers Optimized, size=" << p->a << "; symmetry=" << (p->b ? 1 : 0);
+        break;
     case PSB_PANCAKE_OPT:  // PancakeOptimized.cpp:88-92
         s << "Pancake optimized (29 bit segment), size: " << p->a << "; invIdx: " << (p->b ? 1 : 0);
         break;
@@ -512,7 +516,7 @@ int psb_parse(const psb_puzzle* p, const char* state, uint64_t* index) {
     if (!p || !state || !index) return fail(PSB_ERR_ARG, "bad argument");
     std::vector<int> v;
     if (!read_ints(state, v)) return fail(PSB_ERR_ARG, "cannot parse state '%s'", state);
-    if (p->kind != PSB_HANOI4) {
+    if (p->kind != PSB_HANOI4 && p->kind != PSB_HANOI4_OPT) {
         // SlidingTilePuzzleSimple.cpp:52-59, PancakeSimple.cpp:53-60: a permutation of 0..n-1.
         if (int(v.size()) != p->cells) return fail(PSB_ERR_ARG, "state '%s' needs %d values", state, p->cells);
         unsigned seen = 0;
@@ -540,7 +544,7 @@ int psb_to_string(const psb_puzzle* p, uint64_t index, char* buf, int cap) {
     if (!p || !buf || cap <= 0) return fail(PSB_ERR_ARG, "bad argument");
     if (index >= p->n_states) return fail(PSB_ERR_ARG, "index out of range");
     std::ostringstream s;
-    if (p->kind != PSB_HANOI4) {
+    if (p->kind != PSB_HANOI4 && p->kind != PSB_HANOI4_OPT) {
         int v[16];
         if (p->kind == PSB_PANCAKE_OPT && p->cells >= 12) {
             if (!opt_to_rank(index, &index)) return fail(PSB_ERR_ARG, "offset %llu of its 2^29 block names no permutation",
@@ -847,14 +851,14 @@ constexpr double kBottomUpRatio = 1.0;
 int far_mode(const psb_puzzle* p, int algo, int requested) {
     if (algo != PSB_TWO_BIT) return PSB_FAR_NONE;
     if (requested >= PSB_FAR_NONE && requested <= PSB_FAR_ALL) return requested;
-    if (p->kind == PSB_HANOI4) return PSB_FAR_NONE;
+    if (p->kind == PSB_HANOI4 || p->kind == PSB_HANOI4_OPT) return PSB_FAR_NONE;
     if (p->kind == PSB_PANCAKE && p->n_states <= 6227020800ull) return PSB_FAR_ALL;
     return PSB_FAR_NEAR;
 }
 
 bool supports_bottom_up(const psb_puzzle* p, int algo) {
     if (algo != PSB_THREE_BIT && algo != PSB_TWO_BIT && algo != PSB_CLASSIC) return false;
-    return !(p->kind == PSB_HANOI4 && p->pz.sym);
+    return !((p->kind == PSB_HANOI4 || p->kind == PSB_HANOI4_OPT) && p->pz.sym);
 }
 
 // Window of 2^16 states for the permutation puzzles and 2^17 for Hanoi
@@ -864,7 +868,7 @@ bool supports_bottom_up(const psb_puzzle* p, int algo) {
 int auto_window_bits(const psb_puzzle* p, int algo) {
     int lg = 0;
     while (lg < 63 && (uint64_t(1) << (lg + 1)) <= p->n_states) lg++;
-    const int cap = p->kind == PSB_HANOI4 ? 17 : 16;
+    const int cap = (p->kind == PSB_HANOI4 || p->kind == PSB_HANOI4_OPT) ? 17 : 16;
     int wb = std::max(10, std::min(cap, lg - 10));
     if (algo == PSB_FRONTIER) wb = std::min(wb, 16);  // 4 mark bits per state
     return wb;
@@ -1064,7 +1068,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     const uint32_t max_depth = opts ? opts->max_depth : 0;
     uint64_t* restored = opts ? opts->restored_counts : nullptr;
     const int far_marks = S->far ? far_mode(&P, S->algo, opts ? opts->far_marks : PSB_FAR_AUTO) : PSB_FAR_NONE;
-    if (restored && !(P.kind == PSB_HANOI4 && P.pz.sym && S->algo == PSB_TWO_BIT))
+    if (restored && !((P.kind == PSB_HANOI4 || P.kind == PSB_HANOI4_OPT) && P.pz.sym && S->algo == PSB_TWO_BIT))
         return fail(PSB_ERR_UNSUPPORTED, "restored_counts: 4-peg Hanoi with symmetry, two-bit searches only");
     const bool spill = opts && opts->spill;
     if (spill && opts->segment_bits && (opts->segment_bits < 6 || opts->segment_bits > 32))

@@ -73,7 +73,7 @@ __host__ __device__ constexpr int level_threads(int mode) {
 struct PuzzleArgs {
     int width;  // sliding tile: board width
     int disks;  // Hanoi: number of disks
-    int sym;    // Hanoi: symmetry flag
+    int sym;    // Hanoi: 0 no symmetry, 1 FourPegHanoiSimple's, 2 FourPegHanoiOptimized's (see Hanoi::expand)
 };
 
 // Adapters giving the three puzzles one device interface.  probe_range
@@ -213,11 +213,11 @@ struct HanoiK {
     struct Prefix { uint32_t unused; };
     template <bool kOpBits, class E>
     __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs& a, E& e) {
-        Hanoi::template expand<kOpBits>(i, ob, a.disks, a.sym != 0, e);
+        Hanoi::template expand<kOpBits>(i, ob, a.disks, a.sym, e);
     }
     template <class E>
     __device__ __forceinline__ static void probe_range(uint64_t i, int, int, const PuzzleArgs& a, E& e) {
-        Hanoi::template expand<false>(i, 0u, a.disks, a.sym != 0, e);
+        Hanoi::template expand<false>(i, 0u, a.disks, a.sym, e);
     }
 };
 

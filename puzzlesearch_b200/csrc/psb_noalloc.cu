@@ -73,7 +73,7 @@ uint64_t padded(uint64_t words) { return (words + 31) / 32 * 32; }
 int window_bits_for(const psb_puzzle* p, int algo) {  // same policy as psb_bfs
     int lg = 0;
     while (lg < 63 && (uint64_t(1) << (lg + 1)) <= p->n_states) lg++;
-    const int cap = p->kind == PSB_HANOI4 ? 17 : 16;
+    const int cap = (p->kind == PSB_HANOI4 || p->kind == PSB_HANOI4_OPT) ? 17 : 16;
     int wb = std::max(10, std::min(cap, lg - 10));
     if (algo == PSB_FRONTIER) wb = std::min(wb, 16);
     return wb;

@@ -365,7 +365,11 @@ struct Hanoi {
     static constexpr int kOps = 4;
 
     template <bool kOpBits, class Emit>
-    __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, int disks, bool sym,
+    // sym: 0 none; 1 FourPegHanoiSimple (restore after every move); 2
+    // FourPegHanoiOptimized (restore only when the move empties the source
+    // peg or lands on an empty one, FourPegHanoiOptimized.cpp:190-197; the
+    // same children for canonical states, different ones for the others).
+    __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, int disks, int sym,
                                                   Emit& emit) {
         const uint64_t even = disks >= 32 ? 0x5555555555555555ull
                                           : (0x5555555555555555ull & ((uint64_t(1) << (2 * disks)) - 1));
@@ -389,7 +393,7 @@ struct Hanoi {
                 if (kOpBits && ((opbits >> src) & 1u)) continue;
                 uint64_t child = index ^ (uint64_t(src ^ dst) << pos);
                 uint32_t op = uint32_t(dst);
-                if (sym) {
+                if (sym == 1 || (sym == 2 && (top[dst] == 64 || m[src] == (uint64_t(1) << pos)))) {
                     const uint64_t bitpos = uint64_t(1) << pos;
                     uint64_t mm[4];
 #pragma unroll

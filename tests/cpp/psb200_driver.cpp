@@ -6,7 +6,7 @@
 //   custom <n>
 //   hanoisearch <disks 8..19> <maxSteps>
 //   disk <kind> <a> <b> <Classic|TwoBit|ThreeBit|FrontierSearch|OptFrontierSearch|OptThreeBit> <segmentBits> <threads> <state...>
-// with kind one of sliding, sliding_gpu, pancake, pancake_opt, hanoi4, hanoi4_gpu (the
+// with kind one of sliding, sliding_gpu, pancake, pancake_opt, hanoi4, hanoi4_gpu, hanoi4_opt (the
 // *_gpu kinds construct the reference's GPU class names,
 // SlidingTilePuzzleGpu and FourPegHanoiGPU), and prints one result line per
 // command (space-separated counts, or "child-state|op" items separated by
@@ -30,6 +30,7 @@ static std::unique_ptr<Puzzle> make(const std::string& kind, int a, int b) {
     if (kind == "pancake") return std::make_unique<PancakeSimple>(a);
     if (kind == "pancake_opt") return std::make_unique<PancakeOptimized>(a, b != 0);
     if (kind == "hanoi4_gpu") return std::make_unique<FourPegHanoiGPU>(a, b != 0);
+    if (kind == "hanoi4_opt") return std::make_unique<FourPegHanoiOptimized>(a, b != 0);
     return std::make_unique<FourPegHanoiSimple>(a, b != 0);
 }
 

@@ -55,3 +55,23 @@ def test_13_pancake_optimized_three_bit():
     assert sum(r["counts"]) == math.factorial(13)
     assert psb.bfs_segmented(psb.PancakeOptimized(12), 0, segment_bits=29)["counts"] == \
         psb.bfs(psb.PancakeSimple(12), "three_bit", 0)["counts"]
+
+
+@pytest.mark.parametrize("n,sym", [(6, 1), (10, 1), (18, 1), (18, 0)])
+def test_hanoi_optimized_expand(n, sym):
+    """FourPegHanoiOptimized: Expand equals the oracle's (pinned to the
+    reference class), on random parents, canonical or not."""
+    p = psb.FourPegHanoiOptimized(n, bool(sym))
+    rng = random.Random(n)
+    parents = [rng.randrange(4 ** n) for _ in range(3000)]
+    ops = [rng.randrange(16) if i % 3 else 0 for i in range(3000)]
+    assert p.Expand(parents, ops) == O.expand(["hanoi4_opt", n, sym], parents, ops)
+
+
+def test_hanoi_optimized_searches():
+    for algo in ("two_bit", "three_bit", "frontier", "classic"):
+        for sym in (0, 1):
+            want = O.bfs(["hanoi4_opt", 9, sym], algo)[0]
+            assert psb.bfs(psb.FourPegHanoiOptimized(9, bool(sym)), algo, 0)["counts"] == want, (algo, sym)
+    r = psb.bfs(psb.FourPegHanoiOptimized(12, True), "two_bit", 0, restored=True)
+    assert r["restored"] == O.bfs(["hanoi4", 12, 0], "two_bit")[0]

@@ -321,3 +321,24 @@ def test_pancake_optimized_matches_reference():
         assert O.bfs(["pancake_opt", n, 0], "three_bit")[0] == O.ref_bfs(["pancake_opt", n, 0], "three_bit", start)
     assert n_states(["pancake_opt", 12, 0]) == 1 << 29
     assert n_states(["pancake_opt", 14, 0]) == 13 * 14 << 29
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_hanoi_optimized_matches_reference():
+    """FourPegHanoiOptimized (Puzzles/FourPegHanoiOptimized.cpp:164-204):
+    FourPegHanoiSimple's index; with symmetry it restores the peg order only
+    when a move empties or fills a peg.  The oracle's kind 5 equals the
+    reference class on any parent, and on the canonical (reachable) states
+    it equals the Simple class."""
+    rng = random.Random(24)
+    for n, sym in ((5, 0), (10, 1), (18, 0), (18, 1), (24, 1)):
+        parents = [rng.randrange(4 ** n) for _ in range(400)]
+        ops = [rng.randrange(16) if i % 2 else 0 for i in range(400)]
+        assert O.expand(["hanoi4_opt", n, sym], parents, ops) == O.ref_expand(["hanoi4_opt", n, sym], parents, ops)
+    import numpy as np
+    d, _ = O.depths(["hanoi4", 8, 1], 0)
+    reached = [int(x) for x in np.nonzero(d != 255)[0]]
+    assert O.expand(["hanoi4_opt", 8, 1], reached) == O.expand(["hanoi4", 8, 1], reached)
+    for n, sym in ((8, 0), (9, 1)):
+        start = O.to_string(["hanoi4", n, sym], 0)
+        assert O.ref_bfs(["hanoi4_opt", n, sym], "three_bit", start) == O.bfs(["hanoi4_opt", n, sym], "three_bit")[0]
