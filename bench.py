@@ -607,8 +607,7 @@ def main():
     peak, peak_kind = load_peaks()
     # level kernels + one finalize per level (three-bit, classic) or one
     # CUR -> OLD pass per bottom-up level (two-bit)
-    launches_per_step = st.levels + (st.levels if algo in ("three_bit", "classic") else st.bottom_up_levels)
-    launches_per_step += st.spill_launches
+    launches_per_step = st.levels + st.other_launches + st.spill_launches
 
     if args.spill:
         desc += "; every depth's frontier encoded on the GPU and spilled to pinned host memory"

@@ -213,6 +213,8 @@ typedef struct {
     uint64_t spill_launches;  /* kernels the spill launched (extraction and encoding) */
     double spill_encode_ms;   /* host time encoding depths (the search waits for it) */
     double spill_copy_ms;     /* device time of the copies to pinned host memory */
+    uint64_t other_launches;  /* kernels besides the level kernels and the spill's: finalize, retire and
+                                 far-bitmap fold passes */
 } psb_bfs_stats;
 
 /* Size in 64-bit words of the final arrays that psb_bfs copies out:

@@ -64,7 +64,7 @@ class BfsStats(ctypes.Structure):
                 ("bottom_up_levels", ctypes.c_uint64), ("spill_ms", ctypes.c_double),
                 ("spill_bytes", ctypes.c_uint64), ("spill_segments", ctypes.c_uint64),
                 ("spill_launches", ctypes.c_uint64), ("spill_encode_ms", ctypes.c_double),
-                ("spill_copy_ms", ctypes.c_double)]
+                ("spill_copy_ms", ctypes.c_double), ("other_launches", ctypes.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}

@@ -1155,7 +1155,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
 
     std::vector<uint64_t> res;
     double expand_ms = 0, finalize_ms = 0;
-    uint64_t expanded = 0, children = 0, local = 0, launches = 0, bu_levels = 0;
+    uint64_t expanded = 0, children = 0, local = 0, launches = 0, bu_levels = 0, others = 0;
     uint64_t seen = 0;       // states at depth < the frontier's depth
     uint64_t frontier = 1;   // states at the frontier's depth (two-bit: the kernel's estimate)
     const bool want_final = opts && opts->final_words;
@@ -1268,10 +1268,12 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
                 psb::finalize_classic<<<fgrid, psb::kThreads, 0, s>>>(
                     reinterpret_cast<ulonglong2*>(nopen), reinterpret_cast<ulonglong2*>(closed), n2, S->d_stats + 4);
             PSB_CUDA(cudaGetLastError());
+            others++;
         } else if (S->algo == PSB_TWO_BIT && bu) {
             psb::retire_two_bit<<<148 * 8, psb::kThreads, 0, s>>>(reinterpret_cast<ulonglong2*>(codes), (W2 + 1) / 2,
                                                                  cur_code, S->d_stats + 4);
             PSB_CUDA(cudaGetLastError());
+            others++;
         } else if (S->algo == PSB_TWO_BIT && S->far && far_marks != PSB_FAR_NONE) {
             const uint64_t n4 = (W2 + 3) / 4;
             const uint32_t next_lo = cur_code == 2 ? 1u : 0u;  // NEXT = 5 - CUR
@@ -1285,6 +1287,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
                                                                    reinterpret_cast<uint4*>(S->far), n4, next_lo,
                                                                    S->d_stats + 6, S->d_stats + 5);
             PSB_CUDA(cudaGetLastError());
+            others++;
         }
         PSB_CUDA(cudaEventRecord(S->ev[3], s));
         if (spill) if (int rc = spill_drain(S->spill, opts, &spilled)) return rc;  // overlaps this level
@@ -1406,6 +1409,7 @@ done:
         stats->spill_bytes = spilled.bytes;
         stats->spill_segments = spilled.segments;
         stats->spill_launches = spilled.launches;
+        stats->other_launches = others;
     }
     return PSB_OK;
 }
