@@ -878,9 +878,18 @@ size_t smem_bytes(int mode, int wb, int threads = 0) {
     return psb::level_smem_bytes(mode, size_t(1) << wb, threads ? threads : psb::level_threads(mode));
 }
 
-// Shape variant of the top-down level kernel for psb_bfs_opts.threads.
-int shape_variant(int mode, int threads) {
+// Shape variant of the top-down level kernel for psb_bfs_opts.threads.  With
+// threads = 0, large two-bit pancake and Hanoi searches take 128-thread
+// blocks with 128 registers a thread (B200 sweep, whole search: 14-pancake
+// 4.14 s at 128 threads vs 4.38 s at 256 and 4.49 s at 512; 13-pancake
+// 231 vs 237 vs 242 ms; 18-disk Hanoi 1.58 vs 1.77 vs 1.95 s).  Three-bit
+// (13-pancake 195 vs 193 ms) and the sliding-tile puzzles (3x4 two-bit
+// 45 vs 40 ms) keep 256.
+int shape_variant(const psb_puzzle* p, int mode, int threads) {
     if (mode != psb::kTwoBit && mode != psb::kThreeBit) return 0;
+    if (threads == 0 && mode == psb::kTwoBit && p->n_states >= (uint64_t(1) << 32) &&
+        (p->kind == PSB_PANCAKE || p->kind == PSB_PANCAKE_OPT || p->kind == PSB_HANOI4 || p->kind == PSB_HANOI4_OPT))
+        return 2;
     return threads == 512 ? 1 : threads == 128 ? 2 : 0;
 }
 
@@ -1096,7 +1105,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     const int threads_req = opts ? opts->threads : 0;
     if (threads_req != 0 && threads_req != 128 && threads_req != 256 && threads_req != 512)
         return fail(PSB_ERR_ARG, "threads must be 0, 128, 256 or 512");
-    const int variant = shape_variant(S->mode, threads_req);
+    const int variant = shape_variant(&P, S->mode, threads_req);
     const size_t smem = smem_bytes(S->mode, S->window_bits, psb::variant_threads(variant));
     // Bottom-up levels use windows twice as large (fewer window-end barriers
     // per state; 13-pancake depth 12: 74 ms instead of 77 ms); top-down levels

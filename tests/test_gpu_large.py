@@ -1,7 +1,7 @@
 """Full-size parity on the large configurations: per-depth counts of every
 depth equal the reference's own CPU code's (tests/golden/large_counts.json,
 made by tests/golden/make_large_fixtures.py):
-  * 13-pancake three-bit (6,227,020,800 states, 16 depths);
+  * 13-pancake three-bit and two-bit (6,227,020,800 states, 16 depths);
   * 14-pancake two-bit (87,178,291,200 states, 17 depths), with every
     depth's frontier spilled as the reference's segment streams;
   * 18-disk 4-peg Hanoi two-bit (68,719,476,736 states, 226 depths), and
@@ -35,6 +35,18 @@ def test_pancake13_three_bit():
     r = psb.bfs(psb.PancakeSimple(13), "three_bit", 0)
     assert r["counts"] == want
     assert sum(want) == math.factorial(13)
+
+
+def test_pancake13_two_bit_shapes():
+    """The default two-bit search (far marks ALL, 128 threads per block at
+    this size) and the 256-thread shape with read-first far marks."""
+    want = fixture("pancake13")
+    p = psb.PancakeSimple(13)
+    r = psb.bfs(p, "two_bit", 0)
+    assert r["counts"] == want and r["stats"]["threads"] == 128
+    r = psb.bfs(p, "two_bit", 0, threads=256, far_marks="none")
+    assert r["counts"] == want and r["stats"]["threads"] == 256
+    psb.lib().psb_release_cached_memory(0)
 
 
 def test_pancake14_two_bit_with_spill():

@@ -39,7 +39,7 @@ def test_other_starts_and_max_depth():
     for start in ("1 2 0 3 4 5 6 7 8 9 10 11", "11 10 9 8 7 6 5 4 3 2 1 0"):
         idx = p.Parse(start)
         full = psb.bfs(p, "two_bit", idx)["counts"]
-        assert psb.bfs_segmented(p, idx, segment_bits=20)["counts"] == full
+        assert psb.bfs_segmented(p, idx, segment_bits=22)["counts"] == full
         assert psb.bfs_segmented(p, idx, segment_bits=24, max_depth=9)["counts"] == full[:10]
 
 
