@@ -49,10 +49,15 @@ enum {
     PSB_PANCAKE_OPT = 4, /* PancakeOptimized(size=a, inverseIndex=b), 2 <= a <= 16: for a >= 12 the index is
                             (rank / 12!) << 29 | rank % 12! over prod(13..a) * 2^29 indexes
                             (Puzzles/PancakeOptimized.cpp:26-105); offsets >= 12! are never reached */
-    PSB_HANOI4_OPT = 5   /* FourPegHanoiOptimized(disks=a, useSymmetry=b): FourPegHanoiSimple's index; with
+    PSB_HANOI4_OPT = 5,  /* FourPegHanoiOptimized(disks=a, useSymmetry=b): FourPegHanoiSimple's index; with
                             symmetry it restores the peg order only when a move empties or fills a peg
                             (Puzzles/FourPegHanoiOptimized.cpp:180-204), the same children for canonical
                             states */
+    PSB_SLIDING_OPT = 6  /* SlidingTilePuzzleOptimized<width=a, height=b>, a*b in {4, 6, 8, 9, 10, 12, 14, 15,
+                            16}: blank + 16 * (the tiles' left-smaller digits 2..11, mixed radix), digits
+                            12..14 as nibbles above bit 32 (Puzzles/SlidingTilePuzzleOptimized.cpp:99-212);
+                            16 * (a*b-1)!/2 indexes up to 13 cells, 13, 221 or 3805 segments of 2^32 above.
+                            Blank positions >= a*b and digit patterns above 13 cells name no board */
 };
 
 /* In-memory search algorithms (Common/InMemoryBFS.h:5-11). */
@@ -128,9 +133,9 @@ typedef int (*psb_spill_fn)(void* user, uint32_t depth, uint32_t segment, const 
  * flips up to 12; every long-range mark of the other puzzles) set a bit in a
  * 1-bit-per-state far bitmap, folded into the codes after the level; the
  * flips of more than 12 read first.  PSB_FAR_ALL: every long-range mark goes
- * to the far bitmap.  PSB_FAR_AUTO picks by measurement on B200: ALL for
- * pancake up to 13, NEAR for 14 and more and for sliding tiles, NONE for
- * Hanoi (its marks are local; the fold would not pay).  NEAR and ALL hold the
+ * to the far bitmap.  PSB_FAR_AUTO picks by measurement on B200: NEAR for
+ * pancake and sliding tiles, NONE for Hanoi (its marks are local; the fold
+ * would not pay).  NEAR and ALL hold the
  * bitmap (N/8 bytes) in device memory; without room for it the search runs
  * as NONE. */
 enum { PSB_FAR_AUTO = 0, PSB_FAR_NONE = 1, PSB_FAR_NEAR = 2, PSB_FAR_ALL = 3 };
@@ -154,7 +159,7 @@ typedef struct {
                               PuzzleOptions::segmentBits, Common/DiskBasedBFS.h:11) */
     int32_t far_marks;     /* PSB_TWO_BIT top-down levels: where long-range marks go (PSB_FAR_*) */
     int32_t threads;       /* threads per block of the top-down two-bit and three-bit level kernels: 128, 256 or
-                              512 (0 = 128 for two-bit pancake and Hanoi searches of 2^32 states or more, else
+                              512 (0 = 128 for two-bit pancake and Hanoi searches of 2^36 states or more, else
                               256); the other kernels use 256 */
     uint64_t* restored_counts; /* optional, counts_cap entries; 4-peg Hanoi with symmetry and PSB_TWO_BIT only:
                               the counts HanoiSearch reports (HanoiTowers/HanoiSearch.cpp:247-262), i.e. each

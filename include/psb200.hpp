@@ -231,6 +231,17 @@ private:
     int width_, height_;
 };
 
+// SlidingTilePuzzleOptimized<width, height> (Puzzles/SlidingTilePuzzleOptimized.h:
+// 13-53): the sliding-tile puzzle in the reference's packed index (the tiles'
+// left-smaller digits, the blank in the low nibble; 16 * (cells-1)!/2 indexes
+// up to 13 cells, segments of 2^32 above).
+template <int width, int height>
+class SlidingTilePuzzleOptimized : public DevicePuzzle {
+public:
+    static constexpr int size = width * height;
+    SlidingTilePuzzleOptimized() : DevicePuzzle(PSB_SLIDING_OPT, width, height) {}
+};
+
 class PancakeSimple : public DevicePuzzle {
 public:
     explicit PancakeSimple(int size) : DevicePuzzle(PSB_PANCAKE, size, 0) {}
@@ -524,6 +535,7 @@ using psb200::Puzzle;
 using psb200::PuzzleOptions;
 using psb200::SearchOptions;
 using psb200::SlidingTilePuzzleGpu;
+using psb200::SlidingTilePuzzleOptimized;
 using psb200::SlidingTilePuzzleSimple;
 using psb200::StoreOptions;
 #endif

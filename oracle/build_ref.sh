@@ -11,9 +11,13 @@
 #     for it; GCC assumes 16-byte alignment)
 #   * `static` dropped from explicit template specializations (MSVC accepts it,
 #     GCC does not)
+#   * a forward declaration of SlidingTilePuzzleOptimized.cpp's Parity, which
+#     MSVC finds at instantiation time and GCC's two-phase lookup does not
 #   * a generated <intrin.h> mapping the MSVC intrinsics to GCC builtins, and
 #     the AVX-512VL load/store intrinsics to their SSE2 / AVX2 equivalents so
 #     the library runs on any x86-64-v3 host.
+# SlidingTilePuzzleOptimized is built for its index mapping only: its GPU
+# expand entry points are stand-ins that throw (oracle/ref_gpu_stubs.cpp).
 # Outputs: oracle/_ref/libpsbref.so (C ABI from oracle/ref_capi.cpp),
 #          oracle/_ref/psbref (CLI used for the CPU baseline timing) and
 #          oracle/_ref/psbref_mt (multi-threaded level loop over the reference's
@@ -40,7 +44,8 @@ COMMON="Util.h Util.cpp Puzzle.h Puzzle.cpp Buffer.h Array.h BitArray.h InMemory
         OpBitsCompression.h OpBitsCompression.cpp"
 PUZZLES="PermutationMap.h PermutationMap.cpp SlidingTilePuzzleSimple.h SlidingTilePuzzleSimple.cpp
          PancakeSimple.h PancakeSimple.cpp FourPegHanoiSimple.h FourPegHanoiSimple.cpp
-         PancakeOptimized.h PancakeOptimized.cpp FourPegHanoiOptimized.h FourPegHanoiOptimized.cpp"
+         PancakeOptimized.h PancakeOptimized.cpp FourPegHanoiOptimized.h FourPegHanoiOptimized.cpp
+         PuzzleGpu.h GPU.h SlidingPuzzleGpu.h SlidingTilePuzzleOptimized.h SlidingTilePuzzleOptimized.cpp"
 for f in $COMMON; do cp "$REF/Common/$f" "$SRC/Common/$f"; done
 for f in $PUZZLES; do cp "$REF/Puzzles/$f" "$SRC/Puzzles/$f"; done
 find "$SRC" -type f \( -name '*.h' -o -name '*.cpp' \) -print0 | xargs -0 sed -E -i \
@@ -50,6 +55,10 @@ find "$SRC" -type f \( -name '*.h' -o -name '*.cpp' \) -print0 | xargs -0 sed -E
     -e 's/high_resolution_clock/steady_clock/g' \
     -e 's/^__forceinline static int (_(En|De)codeTuple<[0-9]>)/__forceinline int \1/' \
     -e 's/\*\(__m128i\*\)\(([^)]*)\) = ([a-z_]+);/_mm_storeu_si128((__m128i*)(\1), \2);/g'
+# MSVC resolves SlidingTilePuzzleOptimized's Parity at instantiation time;
+# GCC's two-phase lookup needs it declared before ParseState uses it.
+sed -i -e 's/^\(\s*\)constexpr int BLANK_POS = 15;/&\n\1template<int width, int height> bool Parity(struct VPuzzleState state);/' \
+    "$SRC/Puzzles/SlidingTilePuzzleOptimized.cpp"
 
 cat > "$SRC/intrin.h" <<'EOF'
 /* Generated by oracle/build_ref.sh: the MSVC intrinsics live in msvc_compat.h. */
@@ -81,10 +90,14 @@ static inline unsigned char _BitScanReverse64(unsigned long* idx, unsigned long 
 EOF
 
 CXX="${PSB_CXX:-/usr/bin/g++}"  # the system compiler: a CXX wrapper that links libstdc++ statically breaks loading next to numpy
-FLAGS="-std=c++20 -O3 -march=x86-64-v3 -fPIC -w -I$SRC -I$SRC/Common -include $SRC/msvc_compat.h"
+# SlidingTilePuzzleOptimized's headers name CUDA runtime types (declarations
+# only: its GPU entry points are stand-ins, oracle/ref_gpu_stubs.cpp).
+CUDA_INC="${CUDA_HOME:-/usr/local/cuda}/include"
+FLAGS="-std=c++20 -O3 -march=x86-64-v3 -fPIC -w -I$SRC -I$SRC/Common -I$CUDA_INC -include $SRC/msvc_compat.h"
 SOURCES=""
 for f in $COMMON $PUZZLES; do case "$f" in *.cpp)
     d=Common; [ -f "$SRC/Puzzles/$f" ] && d=Puzzles; SOURCES="$SOURCES $SRC/$d/$f";; esac; done
+SOURCES="$SOURCES $HERE/ref_gpu_stubs.cpp"
 $CXX $FLAGS -shared -o "$OUT/libpsbref.so" "$HERE/ref_capi.cpp" $SOURCES
 $CXX $FLAGS -o "$OUT/psbref" "$HERE/ref_main.cpp" "$HERE/ref_capi.cpp" $SOURCES
 $CXX $FLAGS -pthread -o "$OUT/psbref_mt" "$HERE/ref_mt_bfs.cpp" $SOURCES

@@ -10,7 +10,7 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-KIND = {"sliding": 1, "pancake": 2, "hanoi4": 3, "pancake_opt": 4, "hanoi4_opt": 5}
+KIND = {"sliding": 1, "pancake": 2, "hanoi4": 3, "pancake_opt": 4, "hanoi4_opt": 5, "sliding_opt": 6}
 ALGO = {"two_bit": 1, "three_bit": 2, "frontier": 3, "classic": 4}
 
 u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -246,12 +246,38 @@ def ref():
         L.ref_expand.restype = ctypes.c_int64
         L.ref_expand.argtypes = [ctypes.c_int] * 3 + [u64p, u32p, ctypes.c_uint64, u64p, u32p, ctypes.c_uint64]
         L.ref_to_string.argtypes = [ctypes.c_int] * 3 + [ctypes.c_uint64, ctypes.c_char_p, ctypes.c_int]
+        L.ref_parse.argtypes = [ctypes.c_int] * 3 + [ctypes.c_char_p, u64p]
+        L.ref_indexes_count.restype = ctypes.c_uint64
+        L.ref_indexes_count.argtypes = [ctypes.c_int] * 3
         L.ref_svi_encode.argtypes = [ctypes.c_int, u32p, u8p, ctypes.c_int]
         L.ref_fc_encode.argtypes = [ctypes.c_int, u32p, u8p, ctypes.c_int]
         L.ref_fc_encode_with_check.argtypes = [ctypes.c_int, u32p, u8p, ctypes.c_int]
         L.ref_svi_encode_bounds.argtypes = [ctypes.c_int, u32p, u8p, u8p, ctypes.c_int]
         _ref = L
     return _ref
+
+
+def ref_parse(spec, state):
+    """The reference class's own Parse (it exits the process on a board of the
+    wrong parity: pass solvable states only)."""
+    kind, a, b = spec
+    out = ctypes.c_uint64()
+    if ref().ref_parse(KIND[kind], a, b, state.encode(), ctypes.byref(out)):
+        raise RuntimeError("ref_parse failed")
+    return out.value
+
+
+def ref_to_string(spec, index):
+    kind, a, b = spec
+    buf = ctypes.create_string_buffer(512)
+    if ref().ref_to_string(KIND[kind], a, b, index, buf, 512) < 0:
+        raise RuntimeError("ref_to_string failed")
+    return buf.value.decode()
+
+
+def ref_indexes_count(spec):
+    kind, a, b = spec
+    return ref().ref_indexes_count(KIND[kind], a, b)
 
 
 def ref_bfs(spec, algo, start):

@@ -85,6 +85,70 @@ static int popt_to_rank(int n, uint64_t i, uint64_t* r) {
     return 1;
 }
 
+/* SlidingTilePuzzleOptimized's index (Puzzles/SlidingTilePuzzleOptimized.cpp).
+ * The board's tiles in board order with the blank left out, tile t held as
+ * t-1 (ParseState, :64-77); slot 15 holds the blank's position.  Pack
+ * (:99-116) turns tile i into digit d_i = number of earlier tiles smaller
+ * than it (0 <= d_i <= i) and drops d_0 and d_1: d_0 is always 0 and the
+ * parity rule (:79-97) decides d_1.  GetIndex (:142-158): the low 32 bits are
+ * blank + 16 * (d_2 + 3 * (d_3 + 4 * (d_4 + ... + 11 * d_11))), the segment
+ * (bits 32 and up) is d_12 | d_13 << 4 | d_14 << 8. */
+static uint64_t sopt_states(int size) {  /* IndexesCount (:205-211), MaxSegments / MaxIndexesPerSegment (:12-26) */
+    if (size >= 14) return (uint64_t)(size == 14 ? 0xC + 1 : size == 15 ? 0xDC + 1 : 0xEDC + 1) << 32;
+    uint64_t m = 16;
+    for (int i = 3; i < size; i++) m *= (uint64_t)i;
+    return m;
+}
+
+/* Parity (:79-97): the tile list's inversions, plus the blank's row when the
+ * width is even, must be even. */
+static int sopt_parity_ok(int w, int ntiles, const int* t, int blank) {
+    int inv = 0;
+    for (int i = 0; i < ntiles; i++)
+        for (int j = 0; j < i; j++) inv += t[j] > t[i];
+    return ((inv + (w % 2 == 0 ? blank / w : 0)) & 1) == 0;
+}
+
+static uint64_t sopt_index(int ntiles, const int* t, int blank) {  /* Pack + GetIndex */
+    int d[16] = { 0 };
+    for (int i = 2; i < ntiles; i++)
+        for (int j = 0; j < i; j++) d[i] += t[j] < t[i];
+    uint64_t low = 0;
+    for (int i = (ntiles - 1 < 11 ? ntiles - 1 : 11); i >= 2; i--) low = low * (uint64_t)(i + 1) + (uint64_t)d[i];
+    uint64_t seg = 0;
+    for (int i = 12; i < ntiles; i++) seg |= (uint64_t)d[i] << (4 * (i - 12));
+    return (seg << 32) | (low * 16 + (uint64_t)blank);
+}
+
+/* FromIndex (:160-187) + Unpack (:118-140): 0 when the index names no board. */
+static int sopt_board(int w, int size, uint64_t index, int* t, int* blank) {
+    const int ntiles = size - 1;
+    int d[16] = { 0 };
+    *blank = (int)(index & 15);
+    if (*blank >= size) return 0;
+    uint64_t low = (index & 0xFFFFFFFFull) >> 4;
+    for (int i = 2; i <= 11; i++) {
+        d[i] = (int)(low % (uint64_t)(i + 1));
+        low /= (uint64_t)(i + 1);
+    }
+    if (low) return 0;
+    uint64_t seg = index >> 32;
+    for (int i = 12; i <= 14; i++) { d[i] = (int)(seg & 15); seg >>= 4; }
+    if (seg) return 0;
+    for (int i = 0; i < 16; i++) if (d[i] > i || (i >= ntiles && d[i])) return 0;
+    /* values from the digits, last tile first: d_i selects among the unused values */
+    uint64_t left = 0xFEDCBA9876543210ull;
+    for (int i = ntiles - 1; i >= 2; i--) {
+        t[i] = (int)((left >> (4 * d[i])) & 15);
+        uint64_t lo = d[i] == 0 ? 0 : (left & ((1ull << (4 * d[i])) - 1));
+        left = ((left >> (4 * d[i] + 4)) << (4 * d[i])) | lo;
+    }
+    t[0] = (int)((left >> 4) & 15); /* d_1 = 0: tile 1 below tile 0 */
+    t[1] = (int)(left & 15);
+    if (!sopt_parity_ok(w, ntiles, t, *blank)) { int x = t[0]; t[0] = t[1]; t[1] = x; }
+    return 1;
+}
+
 static int valid(const orc_puzzle* p) {
     if (!p) return 0;
     switch (p->kind) {
@@ -92,6 +156,7 @@ static int valid(const orc_puzzle* p) {
     case ORC_PANCAKE: return p->a >= 2 && p->a <= 16;   /* PancakeSimple.cpp:26 */
     case ORC_PANCAKE_OPT: return p->a >= 2 && p->a <= 16;  /* PancakeOptimized.cpp:81-86 */
     case ORC_HANOI4: case ORC_HANOI4_OPT: return p->a >= 1 && p->a <= 31;
+    case ORC_SLIDING_OPT: return p->a >= 1 && p->b >= 1 && p->a * p->b >= 4 && p->a * p->b <= 16;
     }
     return 0;
 }
@@ -110,6 +175,8 @@ int orc_info(const orc_puzzle* p, uint64_t* indexes, int* ops, int* branching, i
         if (p->a < 12) n = factorial(p->a);
         else { n = 1; for (int k = 13; k <= p->a; k++) n *= (uint64_t)k; n <<= 29; }
         o = p->a - 1; br = p->a - 1; od = 1; break;
+    case ORC_SLIDING_OPT: /* SlidingTilePuzzleOptimized.h:14-24 */
+        n = sopt_states(p->a * p->b); o = 4; br = 4; od = 0; break;
     }
     if (indexes) *indexes = n;
     if (ops) *ops = o;
@@ -171,6 +238,23 @@ int orc_parse(const orc_puzzle* p, const char* state, uint64_t* index) {
         if (p->kind == ORC_PANCAKE_OPT) *index = popt_from_rank(size, *index);
         return 0;
     }
+    if (p->kind == ORC_SLIDING_OPT) {
+        /* SlidingTilePuzzleOptimized.cpp:27-77 (ParseStandardState, ParseState)
+         * and :224-236 (Parse): a board of an unsolvable parity is rejected. */
+        const int size = p->a * p->b;
+        if (cnt != size) return -1;
+        int t[16], k = 0, blank = -1;
+        unsigned seen = 0;
+        for (int i = 0; i < size; i++) {
+            if (vals[i] < 0 || vals[i] >= size || (seen >> vals[i]) & 1) return -1;
+            seen |= 1u << vals[i];
+            if (vals[i] == 0) blank = i;
+            else t[k++] = vals[i] - 1;
+        }
+        if (!sopt_parity_ok(p->a, size - 1, t, blank)) return -1;
+        *index = sopt_index(size - 1, t, blank);
+        return 0;
+    }
     /* FourPegHanoiSimple.cpp:85-102 (ParseState) + :104-113 (StateToIndex):
      * tokens are disk numbers starting at 1; a 0 moves to the next peg. */
     hstate s; memset(&s, 0, sizeof s);
@@ -193,6 +277,13 @@ int orc_to_string(const orc_puzzle* p, uint64_t index, char* buf, int cap) {
         if (p->kind == ORC_PANCAKE_OPT && !popt_to_rank(size, index, &index)) return -1;
         orc_perm_unrank(index, arr, size);
         for (int i = 0; i < size; i++) pos += snprintf(tmp + pos, sizeof tmp - pos, i ? " %d" : "%d", arr[i]);
+    } else if (p->kind == ORC_SLIDING_OPT) {
+        /* ToString (:213-217) via ToStandardState (:46-59): the blank as 0, tile t as t+1 */
+        const int size = p->a * p->b;
+        int t[16], blank, k = 0;
+        if (!sopt_board(p->a, size, index, t, &blank)) return -1;
+        for (int i = 0; i < size; i++)
+            pos += snprintf(tmp + pos, sizeof tmp - pos, i ? " %d" : "%d", i == blank ? 0 : t[k++] + 1);
     } else {
         /* FourPegHanoiSimple.cpp:71-83: disks top-down (1-based) then a 0 per peg,
          * trailing " 0 " removed. */
@@ -303,6 +394,33 @@ static void hanoi_expand(int n, int sym, uint64_t index, uint32_t op, emitter* e
     }
 }
 
+/* GPU expand kernel_sliding_tile_optimized (Puzzles/SlidingPuzzleGpu.cu:211-269):
+ * blank up / down rotate the tiles between the old and the new blank
+ * position; left / right only change the blank digit (index -+ 1).  The
+ * op codes are SlidingTilePuzzleSimple's (UP 0, LEFT 1, RIGHT 2, DOWN 3). */
+static void sliding_opt_expand(int w, int h, uint64_t index, uint32_t op, emitter* e) {
+    enum { UP = 0, LEFT = 1, RIGHT = 2, DOWN = 3 };
+    const int size = w * h, ntiles = size - 1;
+    int t[16], u[16], z;
+    if (!sopt_board(w, size, index, t, &z)) return;
+    if (z >= w && !(op & (1u << UP))) {  /* RotateUp (:190-197) */
+        memcpy(u, t, sizeof t);
+        int x = u[z - w];
+        for (int i = z - w; i < z - 1; i++) u[i] = u[i + 1];
+        u[z - 1] = x;
+        emit(e, sopt_index(ntiles, u, z - w), DOWN);
+    }
+    if (z < size - w && !(op & (1u << DOWN))) {  /* RotateDn (:199-206) */
+        memcpy(u, t, sizeof t);
+        int x = u[z + w - 1];
+        for (int i = z + w - 1; i > z; i--) u[i] = u[i - 1];
+        u[z] = x;
+        emit(e, sopt_index(ntiles, u, z + w), UP);
+    }
+    if (z % w > 0 && !(op & (1u << LEFT))) emit(e, index - 1, RIGHT);
+    if (z % w < w - 1 && !(op & (1u << RIGHT))) emit(e, index + 1, LEFT);
+}
+
 /* PancakeOptimized::Expand (.cpp:128-139): PancakeSimple's moves in its own
  * index; an offset that names no permutation has no children. */
 static void pancake_opt_expand(int n, uint64_t index, uint32_t opbits, emitter* e) {
@@ -320,6 +438,7 @@ static void expand_one(const orc_puzzle* p, uint64_t index, uint32_t op, emitter
     case ORC_HANOI4: hanoi_expand(p->a, p->b ? 1 : 0, index, op, e); break;
     case ORC_HANOI4_OPT: hanoi_expand(p->a, p->b ? 2 : 0, index, op, e); break;
     case ORC_PANCAKE_OPT: pancake_opt_expand(p->a, index, op, e); break;
+    case ORC_SLIDING_OPT: sliding_opt_expand(p->a, p->b, index, op, e); break;
     }
 }
 

@@ -22,13 +22,13 @@
 extern "C" {
 #endif
 
-enum { ORC_SLIDING = 1, ORC_PANCAKE = 2, ORC_HANOI4 = 3, ORC_PANCAKE_OPT = 4, ORC_HANOI4_OPT = 5 };
+enum { ORC_SLIDING = 1, ORC_PANCAKE = 2, ORC_HANOI4 = 3, ORC_PANCAKE_OPT = 4, ORC_HANOI4_OPT = 5, ORC_SLIDING_OPT = 6 };
 enum { ORC_TWO_BIT = 1, ORC_THREE_BIT = 2, ORC_FRONTIER = 3, ORC_CLASSIC = 4 };
 
 #define ORC_INVALID_INDEX (~(uint64_t)0)
 
 typedef struct {
-    int kind; /* ORC_SLIDING / ORC_PANCAKE / ORC_HANOI4 / ORC_PANCAKE_OPT */
+    int kind; /* ORC_SLIDING / ORC_PANCAKE / ORC_HANOI4 / ORC_PANCAKE_OPT / ORC_HANOI4_OPT / ORC_SLIDING_OPT */
     int a;    /* sliding: width;  pancake: size;  hanoi: disks */
     int b;    /* sliding: height; pancake: 0;     hanoi: symmetry flag; pancake opt: inverse-index flag */
 } orc_puzzle;

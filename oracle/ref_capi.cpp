@@ -13,6 +13,7 @@
 #include "Puzzles/PancakeOptimized.h"
 #include "Puzzles/PancakeSimple.h"
 #include "Puzzles/PermutationMap.h"
+#include "Puzzles/SlidingTilePuzzleOptimized.h"
 #include "Puzzles/SlidingTilePuzzleSimple.h"
 
 #include <cstring>
@@ -23,6 +24,26 @@
 
 namespace {
 
+// The shapes the reference instantiates (SlidingTilePuzzleOptimized.cpp:293-307).
+// Only their Parse / ToString / IndexesCount run here: their Expand needs the
+// reference's CUDA kernel (see ref_gpu_stubs.cpp).
+std::unique_ptr<Puzzle> MakeSlidingOptimized(int w, int h) {
+    switch (w * 16 + h) {
+    case 0x22: return std::make_unique<SlidingTilePuzzleOptimized<2, 2>>();
+    case 0x32: return std::make_unique<SlidingTilePuzzleOptimized<3, 2>>();
+    case 0x42: return std::make_unique<SlidingTilePuzzleOptimized<4, 2>>();
+    case 0x52: return std::make_unique<SlidingTilePuzzleOptimized<5, 2>>();
+    case 0x62: return std::make_unique<SlidingTilePuzzleOptimized<6, 2>>();
+    case 0x72: return std::make_unique<SlidingTilePuzzleOptimized<7, 2>>();
+    case 0x82: return std::make_unique<SlidingTilePuzzleOptimized<8, 2>>();
+    case 0x33: return std::make_unique<SlidingTilePuzzleOptimized<3, 3>>();
+    case 0x43: return std::make_unique<SlidingTilePuzzleOptimized<4, 3>>();
+    case 0x53: return std::make_unique<SlidingTilePuzzleOptimized<5, 3>>();
+    case 0x44: return std::make_unique<SlidingTilePuzzleOptimized<4, 4>>();
+    }
+    return nullptr;
+}
+
 std::unique_ptr<Puzzle> MakePuzzle(int kind, int a, int b) {
     switch (kind) {
     case 1: return std::make_unique<SlidingTilePuzzleSimple>(a, b);
@@ -30,6 +51,7 @@ std::unique_ptr<Puzzle> MakePuzzle(int kind, int a, int b) {
     case 3: return std::make_unique<FourPegHanoiSimple>(a, b != 0);
     case 4: return std::make_unique<PancakeOptimized>(a, b != 0);
     case 5: return std::make_unique<FourPegHanoiOptimized>(a, b != 0);
+    case 6: return MakeSlidingOptimized(a, b);
     }
     return nullptr;
 }
@@ -107,10 +129,19 @@ int64_t ref_expand(int kind, int a, int b, const uint64_t* parents, const uint32
     std::vector<uint64_t> idx(parents, parents + n), ci;
     std::vector<int> ob(n), co;
     for (uint64_t i = 0; i < n; i++) ob[i] = opbits ? (int)opbits[i] : 0;
-    puzzle->Expand(idx, ob, ci, co, {});
+    try {
+        puzzle->Expand(idx, ob, ci, co, {});
+    } catch (const std::exception&) {
+        return -3;  // an Expand that needs the GPU
+    }
     if (ci.size() > cap) return -2;
     for (size_t i = 0; i < ci.size(); i++) { children[i] = ci[i]; ops[i] = (uint32_t)co[i]; }
     return (int64_t)ci.size();
+}
+
+uint64_t ref_indexes_count(int kind, int a, int b) {
+    auto puzzle = MakePuzzle(kind, a, b);
+    return puzzle ? puzzle->IndexesCount() : 0;
 }
 
 int ref_parse(int kind, int a, int b, const char* state, uint64_t* index) {

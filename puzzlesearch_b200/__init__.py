@@ -15,7 +15,7 @@ import ctypes
 import os
 
 __all__ = [
-    "PsbError", "lib", "SlidingTilePuzzleSimple", "PancakeSimple", "PancakeOptimized", "FourPegHanoiOptimized", "FourPegHanoiSimple",
+    "PsbError", "lib", "SlidingTilePuzzleSimple", "SlidingTilePuzzleOptimized", "PancakeSimple", "PancakeOptimized", "FourPegHanoiOptimized", "FourPegHanoiSimple",
     "InMemoryTwoBitBFS", "InMemoryThreeBitBFS", "InMemoryFrontierSearch", "InMemoryClassicBFS",
     "bfs", "bfs_segmented", "BfsSession", "TWO_BIT", "THREE_BIT", "FRONTIER", "CLASSIC", "INVALID_INDEX",
 ]
@@ -23,7 +23,7 @@ __all__ = [
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PSB_LIB") or os.path.join(HERE, "libpsb200.so")
 
-SLIDING, PANCAKE, HANOI4, PANCAKE_OPT, HANOI4_OPT = 1, 2, 3, 4, 5
+SLIDING, PANCAKE, HANOI4, PANCAKE_OPT, HANOI4_OPT, SLIDING_OPT = 1, 2, 3, 4, 5, 6
 TWO_BIT, THREE_BIT, FRONTIER, CLASSIC = 1, 2, 3, 4
 ALGOS = {"two_bit": TWO_BIT, "three_bit": THREE_BIT, "frontier": FRONTIER, "classic": CLASSIC}
 INVALID_INDEX = (1 << 64) - 1
@@ -292,6 +292,16 @@ class SlidingTilePuzzleSimple(Puzzle):
         super().__init__(SLIDING, width, height)
 
 
+class SlidingTilePuzzleOptimized(Puzzle):
+    """Puzzles/SlidingTilePuzzleOptimized.h (the reference's class template
+    SlidingTilePuzzleOptimized<width, height>): the tiles' left-smaller digits
+    2..11 in mixed radix times 16 plus the blank, digits 12..14 as nibbles
+    above bit 32; 16 * (cells-1)!/2 indexes up to 13 cells."""
+
+    def __init__(self, width, height):
+        super().__init__(SLIDING_OPT, width, height)
+
+
 class PancakeSimple(Puzzle):
     """Puzzles/PancakeSimple.h: operator k reverses the last k+2 values."""
 
@@ -408,7 +418,7 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
     SPILL_FN is passed through as is (it sees the pinned buffer itself).
     far_marks: two-bit long-range marks, "auto", "none", "near" or "all" (PSB_FAR_*).
     threads: threads per block of the top-down two-bit / three-bit level kernels (128, 256, 512; 0 = 128 for
-        two-bit pancake and Hanoi searches of 2^32 states or more, else 256).
+        two-bit pancake and Hanoi searches of 2^36 states or more, else 256).
     restored: 4-peg Hanoi with symmetry, two-bit: also return "restored", the
     per-depth counts weighted by each canonical state's class size
     (HanoiSearch's result)."""

@@ -902,6 +902,16 @@ extern "C" int psb_frontier_index(const uint8_t* in, uint64_t in_bytes, psb_code
     return PSB_OK;
 }
 
+namespace psb {
+int frontier_decode_async(const uint8_t* d_in, const psb_codec_block* d_blocks, uint32_t n_blocks, uint64_t* d_bits,
+                          uint64_t n_bits, unsigned long long* d_err, cudaStream_t s) {
+    if (n_blocks == 0) return PSB_OK;
+    k_decode<<<n_blocks, 32, 0, s>>>(d_in, d_blocks, n_blocks, d_bits, n_bits, d_err);
+    CD_CUDA(cudaGetLastError());
+    return PSB_OK;
+}
+}  // namespace psb
+
 extern "C" int psb_frontier_decode(const uint8_t* d_in, const psb_codec_block* blocks, uint32_t n_blocks,
                                    uint64_t* d_bits, uint64_t first_bit, uint64_t n_bits, void* stream) {
     if (!d_bits || (n_blocks && (!d_in || !blocks))) return psb_set_error(PSB_ERR_ARG, "bad argument");

@@ -326,6 +326,71 @@ bool opt_to_rank(uint64_t i, uint64_t* r) {
     return true;
 }
 
+// SlidingTilePuzzleOptimized's index (Puzzles/SlidingTilePuzzleOptimized.cpp:
+// 12-26 sizes, 79-97 parity, 99-158 Pack / GetIndex, 160-187 FromIndex,
+// 118-140 Unpack), host side: `tiles` are the board's tiles in board order,
+// the blank left out, tile t held as t-1.
+uint64_t sopt_indexes(int cells) {
+    if (cells >= 14) return uint64_t(cells == 14 ? 0xC + 1 : cells == 15 ? 0xDC + 1 : 0xEDC + 1) << 32;
+    uint64_t m = 16;
+    for (int i = 3; i < cells; i++) m *= uint64_t(i);
+    return m;
+}
+bool sopt_parity_ok(int width, const int* tiles, int ntiles, int blank) {
+    int inv = 0;
+    for (int i = 0; i < ntiles; i++)
+        for (int j = 0; j < i; j++) inv += tiles[j] > tiles[i];
+    return ((inv + (width % 2 == 0 ? blank / width : 0)) & 1) == 0;
+}
+uint64_t sopt_index(const int* tiles, int ntiles, int blank) {
+    uint64_t low = 0, seg = 0;
+    for (int i = std::min(ntiles - 1, 11); i >= 2; i--) {
+        int d = 0;
+        for (int j = 0; j < i; j++) d += tiles[j] < tiles[i];
+        low = low * uint64_t(i + 1) + uint64_t(d);
+    }
+    for (int i = 12; i < ntiles; i++) {
+        int d = 0;
+        for (int j = 0; j < i; j++) d += tiles[j] < tiles[i];
+        seg |= uint64_t(d) << (4 * (i - 12));
+    }
+    return (seg << 32) | (low * 16 + uint64_t(blank));
+}
+bool sopt_board(int width, int cells, uint64_t index, int* tiles, int* blank) {
+    const int ntiles = cells - 1;
+    int d[16] = {0};
+    *blank = int(index & 15);
+    if (*blank >= cells) return false;
+    uint64_t low = (index & 0xFFFFFFFFull) >> 4;
+    for (int i = 2; i <= 11; i++) {
+        d[i] = int(low % uint64_t(i + 1));
+        low /= uint64_t(i + 1);
+    }
+    uint64_t seg = index >> 32;
+    for (int i = 12; i <= 14; i++, seg >>= 4) d[i] = int(seg & 15);
+    if (low || seg) return false;
+    for (int i = 0; i < 16; i++)
+        if (d[i] > i || (i >= ntiles && d[i])) return false;
+    unsigned used = 0;  // values placed so far, last tile first: d_i picks the d_i-th unused one
+    for (int i = ntiles - 1; i >= 2; i--) {
+        int k = d[i], val = 0;
+        for (;; val++) {
+            if (used & (1u << val)) continue;
+            if (k-- == 0) break;
+        }
+        tiles[i] = val;
+        used |= 1u << val;
+    }
+    int lo = 0;
+    while (used & (1u << lo)) lo++;
+    int hi = lo + 1;
+    while (used & (1u << hi)) hi++;
+    tiles[0] = hi;  // d_1 = 0; the other parity class swaps the first two
+    tiles[1] = lo;
+    if (!sopt_parity_ok(width, tiles, ntiles, *blank)) std::swap(tiles[0], tiles[1]);
+    return true;
+}
+
 bool read_ints(const char* s, std::vector<int>& out) {
     std::istringstream in(s);
     std::string tok;
@@ -463,6 +528,13 @@ int psb_puzzle_create(int kind, int a, int b, psb_puzzle** out) {
             ok = psb::pancake_opt_kernels(a, &p->k);
         }
         break;
+    case PSB_SLIDING_OPT:  // SlidingTilePuzzleOptimized.h:13-24, .cpp:205-211
+        if (a < 1 || b < 1 || a * b < 4 || a * b > 16)
+            return fail(PSB_ERR_ARG, "sliding tile %dx%d: need 4 <= w*h <= 16", a, b);
+        p->cells = a * b; p->n_states = sopt_indexes(a * b); p->ops = 4; p->branching = 4; p->odd = 0;
+        p->pz.width = a;
+        ok = psb::sliding_opt_kernels(a * b, &p->k);
+        break;
     case PSB_HANOI4:      // FourPegHanoiSimple.h:14-20, .cpp:141-143
     case PSB_HANOI4_OPT:  // FourPegHanoiOptimized.h:8-20, .cpp:164-166: the same index space
         if (a < 1 || a > 31) return fail(PSB_ERR_ARG, "hanoi disks %d: need 1..31", a);
@@ -505,6 +577,9 @@ int psb_puzzle_name(const psb_puzzle* p, char* buf, int cap) {
     case PSB_PANCAKE_OPT:  // PancakeOptimized.cpp:88-92
         s << "Pancake optimized (29 bit segment), size: " << p->a << "; invIdx: " << (p->b ? 1 : 0);
         break;
+    case PSB_SLIDING_OPT:  // SlidingTilePuzzleOptimized.cpp:196-202
+        s << "Sliding-Tile GPU Optimized (for 32-bit segment): " << p->a << " x " << p->b;
+        break;
     }
     const std::string str = s.str();
     if (int(str.size()) + 1 > cap) return fail(PSB_ERR_CAPACITY, "name buffer too small");
@@ -516,6 +591,24 @@ int psb_parse(const psb_puzzle* p, const char* state, uint64_t* index) {
     if (!p || !state || !index) return fail(PSB_ERR_ARG, "bad argument");
     std::vector<int> v;
     if (!read_ints(state, v)) return fail(PSB_ERR_ARG, "cannot parse state '%s'", state);
+    if (p->kind == PSB_SLIDING_OPT) {
+        // SlidingTilePuzzleOptimized.cpp:27-77, 224-236: a permutation of 0..n-1 (0 = blank) of the
+        // solvable parity class (the reference's Parse stops the program on the other one).
+        if (int(v.size()) != p->cells) return fail(PSB_ERR_ARG, "state '%s' needs %d values", state, p->cells);
+        unsigned seen = 0;
+        int tiles[16], k = 0, blank = -1;
+        for (int i = 0; i < p->cells; i++) {
+            const int x = v[i];
+            if (x < 0 || x >= p->cells || (seen >> x) & 1u) return fail(PSB_ERR_ARG, "state '%s' is not a permutation", state);
+            seen |= 1u << x;
+            if (x == 0) blank = i;
+            else tiles[k++] = x - 1;
+        }
+        if (!sopt_parity_ok(p->a, tiles, p->cells - 1, blank))
+            return fail(PSB_ERR_ARG, "state '%s' is not solvable from the standard state", state);
+        *index = sopt_index(tiles, p->cells - 1, blank);
+        return PSB_OK;
+    }
     if (p->kind != PSB_HANOI4 && p->kind != PSB_HANOI4_OPT) {
         // SlidingTilePuzzleSimple.cpp:52-59, PancakeSimple.cpp:53-60: a permutation of 0..n-1.
         if (int(v.size()) != p->cells) return fail(PSB_ERR_ARG, "state '%s' needs %d values", state, p->cells);
@@ -544,7 +637,13 @@ int psb_to_string(const psb_puzzle* p, uint64_t index, char* buf, int cap) {
     if (!p || !buf || cap <= 0) return fail(PSB_ERR_ARG, "bad argument");
     if (index >= p->n_states) return fail(PSB_ERR_ARG, "index out of range");
     std::ostringstream s;
-    if (p->kind != PSB_HANOI4 && p->kind != PSB_HANOI4_OPT) {
+    if (p->kind == PSB_SLIDING_OPT) {
+        // ToString via ToStandardState (SlidingTilePuzzleOptimized.cpp:46-59, 213-217).
+        int tiles[16], blank, k = 0;
+        if (!sopt_board(p->a, p->cells, index, tiles, &blank))
+            return fail(PSB_ERR_ARG, "index %llu names no board", (unsigned long long)index);
+        for (int i = 0; i < p->cells; i++) s << (i ? " " : "") << (i == blank ? 0 : tiles[k++] + 1);
+    } else if (p->kind != PSB_HANOI4 && p->kind != PSB_HANOI4_OPT) {
         int v[16];
         if (p->kind == PSB_PANCAKE_OPT && p->cells >= 12) {
             if (!opt_to_rank(index, &index)) return fail(PSB_ERR_ARG, "offset %llu of its 2^29 block names no permutation",
@@ -852,7 +951,6 @@ int far_mode(const psb_puzzle* p, int algo, int requested) {
     if (algo != PSB_TWO_BIT) return PSB_FAR_NONE;
     if (requested >= PSB_FAR_NONE && requested <= PSB_FAR_ALL) return requested;
     if (p->kind == PSB_HANOI4 || p->kind == PSB_HANOI4_OPT) return PSB_FAR_NONE;
-    if (p->kind == PSB_PANCAKE && p->n_states <= 6227020800ull) return PSB_FAR_ALL;
     return PSB_FAR_NEAR;
 }
 
@@ -879,15 +977,15 @@ size_t smem_bytes(int mode, int wb, int threads = 0) {
 }
 
 // Shape variant of the top-down level kernel for psb_bfs_opts.threads.  With
-// threads = 0, large two-bit pancake and Hanoi searches take 128-thread
-// blocks with 128 registers a thread (B200 sweep, whole search: 14-pancake
-// 4.14 s at 128 threads vs 4.38 s at 256 and 4.49 s at 512; 13-pancake
-// 231 vs 237 vs 242 ms; 18-disk Hanoi 1.58 vs 1.77 vs 1.95 s).  Three-bit
-// (13-pancake 195 vs 193 ms) and the sliding-tile puzzles (3x4 two-bit
-// 45 vs 40 ms) keep 256.
+// threads = 0, two-bit pancake and Hanoi searches of 2^36 states or more take
+// 128-thread blocks with 128 registers a thread (B200 sweeps, whole search:
+// 14-pancake 4.15 s at 128 threads vs 4.40 s at 256, far marks NEAR;
+// 18-disk Hanoi 1.58 vs 1.77 s).  Smaller ones keep 256 (13-pancake two-bit
+// 219 vs 225 ms), as do three-bit (13-pancake 193 vs 195 ms) and the
+// sliding-tile puzzles (3x4 two-bit 40 vs 45 ms).
 int shape_variant(const psb_puzzle* p, int mode, int threads) {
     if (mode != psb::kTwoBit && mode != psb::kThreeBit) return 0;
-    if (threads == 0 && mode == psb::kTwoBit && p->n_states >= (uint64_t(1) << 32) &&
+    if (threads == 0 && mode == psb::kTwoBit && p->n_states >= (uint64_t(1) << 36) &&
         (p->kind == PSB_PANCAKE || p->kind == PSB_PANCAKE_OPT || p->kind == PSB_HANOI4 || p->kind == PSB_HANOI4_OPT))
         return 2;
     return threads == 512 ? 1 : threads == 128 ? 2 : 0;

@@ -62,6 +62,11 @@ void encoder_set_ops(SegmentEncoder* e, bool on, const uint64_t* nibbles, uint64
 int encoder_chunk_sums(SegmentEncoder* e, uint64_t n_bits, unsigned long long** sums);
 // Kernels the encoder launched since the last call.
 uint64_t encoder_take_launches(SegmentEncoder* e);
+// Decodes a segment stream (block table `d_blocks` in device memory) into
+// the cleared bitmap d_bits[0, n_bits) on stream s, without allocating or
+// synchronising; an offset outside the segment sets *d_err.
+int frontier_decode_async(const uint8_t* d_in, const psb_codec_block* d_blocks, uint32_t n_blocks, uint64_t* d_bits,
+                          uint64_t n_bits, unsigned long long* d_err, cudaStream_t s);
 // One-bit frontier bitmaps (ceil(n_states/64) words at out; first_state a
 // multiple of 64) of a two-bit array (states with code `code`) and of a
 // frontier-search array (states with an operator bit set, less `excl`),

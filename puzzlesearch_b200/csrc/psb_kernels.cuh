@@ -168,6 +168,30 @@ struct PancakeOptK {
     }
 };
 
+// SlidingTilePuzzleOptimized's index (see SlidingOpt); its moves have no
+// per-word structure, so the level kernel runs the generic per-state path.
+template <int N>
+struct SlidingOptK {
+    static constexpr int kBranch = 4;
+    static constexpr int kOps = 4;
+    static constexpr int kProbeRound = 4;  // one round: four cheap children
+    static constexpr bool kPairOp0 = false;
+    static constexpr bool kFlip3Op1 = false;
+    static constexpr bool kFlip4Op2 = false;
+    static constexpr bool kChunkPrefix = false;
+    static constexpr bool kSymMult = false;
+    static constexpr uint32_t kBlock = 1;
+    struct Prefix { uint32_t unused; };
+    template <bool kOpBits, class E>
+    __device__ __forceinline__ static void expand(uint64_t i, uint32_t ob, const PuzzleArgs& a, E& e) {
+        SlidingOpt<N>::template expand<kOpBits>(i, ob, a.width, e);
+    }
+    template <class E>
+    __device__ __forceinline__ static void probe_range(uint64_t i, int, int, const PuzzleArgs& a, E& e) {
+        SlidingOpt<N>::template expand<false>(i, 0u, a.width, e);
+    }
+};
+
 template <int N>
 struct SlidingK {
     static constexpr int kBranch = 4;
@@ -1227,6 +1251,7 @@ PuzzleKernels make_kernels() {
 bool pancake_kernels(int n, PuzzleKernels* out);
 bool pancake_opt_kernels(int n, PuzzleKernels* out);  // psb_pancake_opt.cu, n = 12..16
 bool sliding_kernels(int cells, PuzzleKernels* out);
+bool sliding_opt_kernels(int cells, PuzzleKernels* out);  // psb_sliding_opt.cu: 4, 6, 8, 9, 10, 12, 14, 15, 16 cells
 bool hanoi_kernels(PuzzleKernels* out);
 
 }  // namespace psb

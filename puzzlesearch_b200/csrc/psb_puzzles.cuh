@@ -351,6 +351,107 @@ struct Sliding {
 };
 
 // --------------------------------------------------------------------------
+// Sliding tile in SlidingTilePuzzleOptimized's index
+// (Puzzles/SlidingTilePuzzleOptimized.cpp:99-236; GPU expand
+// kernel_sliding_tile_optimized, Puzzles/SlidingPuzzleGpu.cu:211-269).  The
+// board's T = N-1 tiles in board order, the blank left out; digit i of tile
+// i (i >= 2) = how many earlier tiles are smaller.  Digit 0 is always 0 and
+// digit 1 follows from the parity rule (:79-97), so neither is stored.  Low
+// 32 bits: blank + 16 * sum_{i=2..11} d_i * i!/2; bits 32 and up (14..16
+// cells): d_12 | d_13 << 4 | d_14 << 8.  Moving the blank up or down rotates
+// the tiles between the two blank positions by one place; moving it left or
+// right only changes the blank digit (index -+ 1).
+// --------------------------------------------------------------------------
+template <int N>
+struct SlidingOpt {
+    static constexpr int kBranch = 4;
+    static constexpr int kOps = 4;
+    static constexpr int T = N - 1;                    // tiles
+    static constexpr int kTop = T - 1 < 11 ? T - 1 : 11;  // last digit of the low word
+    static_assert(N >= 4 && N <= 16, "2x2 .. 4x4 boards");
+
+    // The tiles (values 0..T-1, list position i in nibble i) and blank of an
+    // index; false when the index names no board.
+    __device__ __forceinline__ static bool board(uint64_t index, int width, uint64_t& tiles, uint32_t& blank) {
+        blank = uint32_t(index) & 15u;
+        if (blank >= uint32_t(N)) return false;
+        uint32_t d[16];
+        uint32_t low = uint32_t(index) >> 4;
+#pragma unroll
+        for (int i = 2; i <= kTop; ++i) {
+            d[i] = low % uint32_t(i + 1);
+            low /= uint32_t(i + 1);
+        }
+        if (low) return false;
+        uint64_t seg = index >> 32;
+#pragma unroll
+        for (int i = 12; i < T; ++i) {
+            d[i] = uint32_t(seg) & 15u;
+            seg >>= 4;
+            if (d[i] > uint32_t(i)) return false;
+        }
+        if (seg) return false;
+        // Values, last tile first: d_i picks among the values still unused
+        // (ascending in a nibble list; the first i+1 entries are the unused ones).
+        uint64_t left = 0xFEDCBA9876543210ull;
+        uint32_t odd = 1;  // inversions of the tile list with d_1 = 0: sum (i - d_i) + 1
+        tiles = 0;
+#pragma unroll
+        for (int i = T - 1; i >= 2; --i) {
+            const uint32_t s = 4u * d[i];
+            tiles |= ((left >> s) & 15u) << (4 * i);
+            left = (((left >> s) >> 4) << s) | (left & ((uint64_t(1) << s) - 1));
+            odd += uint32_t(i) - d[i];
+        }
+        const uint32_t lo = uint32_t(left) & 15u, hi = (uint32_t(left) >> 4) & 15u;
+        if (width % 2 == 0) odd += blank / uint32_t(width);
+        // d_1 = 0 puts the larger of the last two values first; the other
+        // parity class swaps them (Unpack, :133-137)
+        tiles |= (odd & 1u) ? uint64_t(lo | (hi << 4)) : uint64_t(hi | (lo << 4));
+        return true;
+    }
+
+    // Index of tiles / blank (Pack + GetIndex, :99-158).
+    __device__ __forceinline__ static uint64_t index_of(uint64_t tiles, uint32_t blank) {
+        uint32_t seen = (1u << (tiles & 15u)) | (1u << ((tiles >> 4) & 15u));
+        uint32_t low = 0;
+        uint64_t seg = 0;
+#pragma unroll
+        for (int i = 2; i < T; ++i) {
+            const uint32_t v = uint32_t(tiles >> (4 * i)) & 15u;
+            const uint32_t d = __popc(seen & ((1u << v) - 1u));
+            seen |= 1u << v;
+            if (i <= 11) low += d * uint32_t(fact(i) / 2);
+            else seg |= uint64_t(d) << (4 * (i - 12));
+        }
+        return (seg << 32) | (uint64_t(low) * 16u + blank);
+    }
+
+    template <bool kOpBits, class Emit>
+    __device__ __forceinline__ static void expand(uint64_t index, uint32_t opbits, int width, Emit& emit) {
+        uint64_t tiles;
+        uint32_t z;
+        if (!board(index, width, tiles, z)) return;
+        const uint32_t w = uint32_t(width);
+        const uint64_t mask = (uint64_t(1) << (4 * w)) - 1;  // w <= 8 tiles
+        if (z >= w && !(kOpBits && (opbits & 1u))) {  // blank up: tiles z-w .. z-1 rotate left
+            const uint32_t a = 4u * (z - w);
+            const uint64_t seg = (tiles >> a) & mask;
+            const uint64_t rot = (seg >> 4) | ((seg & 15u) << (4 * (w - 1)));
+            emit(index_of((tiles & ~(mask << a)) | (rot << a), z - w), 3u);
+        }
+        if (z + w < uint32_t(N) && !(kOpBits && (opbits & 8u))) {  // blank down: tiles z .. z+w-1 rotate right
+            const uint32_t a = 4u * z;
+            const uint64_t seg = (tiles >> a) & mask;
+            const uint64_t rot = ((seg << 4) & mask) | (seg >> (4 * (w - 1)));
+            emit(index_of((tiles & ~(mask << a)) | (rot << a), z + w), 0u);
+        }
+        if (z % w > 0 && !(kOpBits && (opbits & 2u))) emit(index - 1, 2u);
+        if (z % w < w - 1 && !(kOpBits && (opbits & 4u))) emit(index + 1, 1u);
+    }
+};
+
+// --------------------------------------------------------------------------
 // Four-peg Towers of Hanoi (FourPegHanoiSimple.cpp:104-124,156-174): disk d
 // (0 = smallest) sits on peg (index >> 2d) & 3.  For each peg pair a<b the
 // smaller of the two top disks moves; the operator bit tested is the source

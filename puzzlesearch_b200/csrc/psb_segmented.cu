@@ -123,21 +123,31 @@ struct Run {
     uint64_t chunk_words = 0;
     DevBuf<uint64_t> next, cur, old, kids;
     DevBuf<uint32_t> offs;
-    DevBuf<uint8_t> stream_buf;
+    DevBuf<uint8_t> stream_buf[2];  // the two layers decoded for one segment
+    DevBuf<psb_codec_block> block_tab[2];
     DevBuf<unsigned int> hist;
-    DevBuf<unsigned long long> scalars;  // [0] count, [1] children appended, [2] error flag
+    DevBuf<unsigned long long> scalars;  // [0] count, [1] children appended, [2] error flag, [3] decode error
+    psb::SegmentEncoder* enc = nullptr;  // device scratch kept from segment to segment
     psb_segmented_stats st{};
+
+    ~Run() { if (enc) psb::encoder_destroy(enc); }
 
     uint64_t states_in(uint64_t g) const { return std::min(seg_states, P->n_states - g * seg_states); }
 
-    // Decodes a layer into a cleared segment bitmap.
-    int decode(const Layer& L, uint64_t* bits, uint64_t g) {
+    // Decodes a layer into a cleared segment bitmap (slot 0 or 1: the two
+    // layers of one segment are in flight together).  Nothing waits: a bad
+    // offset sets scalars[3], read at the end of the depth.
+    int decode(const Layer& L, uint64_t* bits, uint64_t g, int slot) {
         SG_CUDA(cudaMemsetAsync(bits, 0, seg_words * 8, s));
         if (L.count == 0) return PSB_OK;
-        if (int rc = stream_buf.grow(L.bytes.size())) return rc;
-        SG_CUDA(cudaMemcpyAsync(stream_buf.p, L.bytes.data(), L.bytes.size(), cudaMemcpyHostToDevice, s));
+        if (int rc = stream_buf[slot].grow(L.bytes.size())) return rc;
+        if (int rc = block_tab[slot].grow(L.blocks.size())) return rc;
+        SG_CUDA(cudaMemcpyAsync(stream_buf[slot].p, L.bytes.data(), L.bytes.size(), cudaMemcpyHostToDevice, s));
+        SG_CUDA(cudaMemcpyAsync(block_tab[slot].p, L.blocks.data(), L.blocks.size() * sizeof(psb_codec_block),
+                                cudaMemcpyHostToDevice, s));
         st.h2d_bytes += L.bytes.size();
-        return psb_frontier_decode(stream_buf.p, L.blocks.data(), uint32_t(L.blocks.size()), bits, 0, states_in(g), s);
+        return psb::frontier_decode_async(stream_buf[slot].p, block_tab[slot].p, uint32_t(L.blocks.size()), bits,
+                                          states_in(g), scalars.p + 3, s);
     }
 
     // Encodes a segment bitmap holding `count` states into a layer.
@@ -146,21 +156,19 @@ struct Run {
         L->blocks.clear();
         L->count = count;
         if (count == 0) return PSB_OK;
-        L->blocks.resize(count / 262144 + 2);
-        uint64_t bytes = 0;
-        uint32_t nb = 0;
-        int rc = psb_frontier_encode(bits, 0, states_in(g), stream_buf.p, stream_buf.cap, &bytes, L->blocks.data(),
-                                     uint32_t(L->blocks.size()), &nb, s);
-        if (rc == PSB_ERR_CAPACITY && bytes > stream_buf.cap) {
-            if (int g2 = stream_buf.grow(bytes)) return g2;
-            rc = psb_frontier_encode(bits, 0, states_in(g), stream_buf.p, stream_buf.cap, &bytes, L->blocks.data(),
-                                     uint32_t(L->blocks.size()), &nb, s);
-        }
-        if (rc) return rc;
-        L->blocks.resize(nb);
+        uint64_t bytes = 0, n = 0;
+        if (int rc = psb::encoder_plan(enc, bits, states_in(g), s, false, &bytes, &n)) return rc;
+        if (n != count) return psb_set_error(PSB_ERR_DEVICE, "segmented search: layer count mismatch");
+        if (int rc = stream_buf[0].grow(bytes)) return rc;
+        if (int rc = psb::encoder_write(enc, stream_buf[0].p, s)) return rc;
         L->bytes.resize(bytes);
-        SG_CUDA(cudaMemcpyAsync(L->bytes.data(), stream_buf.p, bytes, cudaMemcpyDeviceToHost, s));
+        SG_CUDA(cudaMemcpyAsync(L->bytes.data(), stream_buf[0].p, bytes, cudaMemcpyDeviceToHost, s));
         SG_CUDA(cudaStreamSynchronize(s));
+        // The block table, for the decoder: read back from the stream's own headers.
+        uint32_t nb = 0;
+        if (int rc = psb_frontier_index(L->bytes.data(), bytes, nullptr, 0, &nb)) return rc;
+        L->blocks.resize(nb);
+        if (int rc = psb_frontier_index(L->bytes.data(), bytes, L->blocks.data(), nb, &nb)) return rc;
         st.d2h_bytes += bytes;
         return PSB_OK;
     }
@@ -279,7 +287,8 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
     if (int rc = R.offs.grow(uint64_t(1) << 22)) return rc;
     if (int rc = R.hist.grow(R.n_segments)) return rc;
     if (int rc = R.scalars.grow(4)) return rc;
-    if (int rc = R.stream_buf.grow(uint64_t(1) << 20)) return rc;
+    if (int rc = R.stream_buf[0].grow(uint64_t(1) << 20)) return rc;
+    if (!(R.enc = psb::encoder_create())) return psb_set_error(PSB_ERR_NOMEM, "segmented search: encoder");
     SG_CUDA(cudaMemsetAsync(R.scalars.p, 0, 4 * 8, R.s));
 
     const uint64_t S = R.n_segments;
@@ -312,10 +321,10 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
             SG_CUDA(cudaMemsetAsync(R.next.p, 0, R.seg_words * 8, R.s));
             if (int rc = R.receive(recv[g], R.next.p)) return rc;
             std::vector<uint32_t>().swap(recv[g]);
-            if (int rc = R.decode(cur_l[g], R.cur.p, g)) return rc;
+            if (int rc = R.decode(cur_l[g], R.cur.p, g, 0)) return rc;
             if (cur_l[g].count)
                 if (int rc = R.expand(R.cur.p, g, 0, nullptr)) return rc;
-            if (int rc = R.decode(old_l[g], R.old.p, g)) return rc;
+            if (int rc = R.decode(old_l[g], R.old.p, g, 1)) return rc;
             SG_CUDA(cudaMemsetAsync(R.scalars.p, 0, 8, R.s));
             psb::seg_finish<<<148 * 8, psb::kThreads, 0, R.s>>>(R.next.p, R.old.p, R.cur.p, R.seg_words, odd ? 1 : 0,
                                                                R.scalars.p);
@@ -329,10 +338,11 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
                 if (int rc = R.expand(R.next.p, g, 1, &recv_next)) return rc;
             R.st.peak_host_bytes = std::max(R.st.peak_host_bytes, host_bytes(old_l, cur_l, new_l, recv, recv_next));
         }
-        unsigned long long err = 0;
-        SG_CUDA(cudaMemcpyAsync(&err, R.scalars.p + 2, 8, cudaMemcpyDeviceToHost, R.s));
+        unsigned long long err[2] = {0, 0};
+        SG_CUDA(cudaMemcpyAsync(err, R.scalars.p + 2, 16, cudaMemcpyDeviceToHost, R.s));
         SG_CUDA(cudaStreamSynchronize(R.s));
-        if (err) return psb_set_error(PSB_ERR_DEVICE, "segmented search produced a child index >= IndexesCount()");
+        if (err[0]) return psb_set_error(PSB_ERR_DEVICE, "segmented search produced a child index >= IndexesCount()");
+        if (err[1]) return psb_set_error(PSB_ERR_DEVICE, "segmented search: a layer decoded outside its segment");
         if (total == 0) break;
         if (res.size() >= cap) return psb_set_error(PSB_ERR_CAPACITY, "more depths than counts_cap");
         res.push_back(total);
@@ -347,7 +357,8 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
     if (stats && stats->struct_size >= sizeof(psb_segmented_stats)) {
         R.st.struct_size = stats->struct_size;
         R.st.segments = S;
-        R.st.device_bytes = (R.next.cap + R.cur.cap + R.old.cap + R.kids.cap) * 8 + R.offs.cap * 4 + R.stream_buf.cap;
+        R.st.device_bytes = (R.next.cap + R.cur.cap + R.old.cap + R.kids.cap) * 8 + R.offs.cap * 4 +
+                            R.stream_buf[0].cap + R.stream_buf[1].cap;
         R.st.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         *stats = R.st;
     }

@@ -6,7 +6,7 @@
 //   custom <n>
 //   hanoisearch <disks 8..19> <maxSteps>
 //   disk <kind> <a> <b> <Classic|TwoBit|ThreeBit|FrontierSearch|OptFrontierSearch|OptThreeBit> <segmentBits> <threads> <state...>
-// with kind one of sliding, sliding_gpu, pancake, pancake_opt, hanoi4, hanoi4_gpu, hanoi4_opt (the
+// with kind one of sliding, sliding_gpu, sliding_opt, pancake, pancake_opt, hanoi4, hanoi4_gpu, hanoi4_opt (the
 // *_gpu kinds construct the reference's GPU class names,
 // SlidingTilePuzzleGpu and FourPegHanoiGPU), and prints one result line per
 // command (space-separated counts, or "child-state|op" items separated by
@@ -24,8 +24,27 @@
 #include <sstream>
 #include <string>
 
+// SlidingTilePuzzleOptimized<w, h> for the shapes the reference builds it for.
+static std::unique_ptr<Puzzle> make_sliding_opt(int w, int h) {
+    switch (w * 16 + h) {
+    case 0x22: return std::make_unique<SlidingTilePuzzleOptimized<2, 2>>();
+    case 0x32: return std::make_unique<SlidingTilePuzzleOptimized<3, 2>>();
+    case 0x42: return std::make_unique<SlidingTilePuzzleOptimized<4, 2>>();
+    case 0x52: return std::make_unique<SlidingTilePuzzleOptimized<5, 2>>();
+    case 0x62: return std::make_unique<SlidingTilePuzzleOptimized<6, 2>>();
+    case 0x72: return std::make_unique<SlidingTilePuzzleOptimized<7, 2>>();
+    case 0x82: return std::make_unique<SlidingTilePuzzleOptimized<8, 2>>();
+    case 0x33: return std::make_unique<SlidingTilePuzzleOptimized<3, 3>>();
+    case 0x43: return std::make_unique<SlidingTilePuzzleOptimized<4, 3>>();
+    case 0x53: return std::make_unique<SlidingTilePuzzleOptimized<5, 3>>();
+    case 0x44: return std::make_unique<SlidingTilePuzzleOptimized<4, 4>>();
+    }
+    throw std::runtime_error("no SlidingTilePuzzleOptimized<" + std::to_string(w) + ", " + std::to_string(h) + ">");
+}
+
 static std::unique_ptr<Puzzle> make(const std::string& kind, int a, int b) {
     if (kind == "sliding") return std::make_unique<SlidingTilePuzzleSimple>(a, b);
+    if (kind == "sliding_opt") return make_sliding_opt(a, b);
     if (kind == "sliding_gpu") return std::make_unique<SlidingTilePuzzleGpu>(a, b);
     if (kind == "pancake") return std::make_unique<PancakeSimple>(a);
     if (kind == "pancake_opt") return std::make_unique<PancakeOptimized>(a, b != 0);

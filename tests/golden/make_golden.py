@@ -119,10 +119,16 @@ def expand_kats(ref):
         for m in re.finditer(r"TEST\((\w+), (\w+)\) \{(.*?)\n\}", text, re.S):
             body = m.group(3)
             ctor = re.search(r"(\w+) puz\(([^)]*)\);", body)
-            if not ctor:
+            tctor = re.search(r"(\w+)<(\d+), (\d+)> puz;", body)  # SlidingTilePuzzleOptimized<w, h>
+            if not ctor and not tctor:
                 continue
-            cls, args = ctor.group(1), [a.strip() for a in ctor.group(2).split(",") if a.strip()]
-            if kind == "pancake":
+            if tctor:
+                cls, args = tctor.group(1), [tctor.group(2), tctor.group(3)]
+            else:
+                cls, args = ctor.group(1), [a.strip() for a in ctor.group(2).split(",") if a.strip()]
+            if tctor:
+                spec = ["sliding_opt", int(args[0]), int(args[1])]
+            elif kind == "pancake":
                 spec = ["pancake", int(args[0]), 0]
             elif kind == "hanoi4":
                 spec = ["hanoi4", int(args[0]), 1 if len(args) > 1 and args[1] == "true" else 0]

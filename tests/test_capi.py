@@ -12,6 +12,7 @@ import pytest
 
 import oracle as O
 import puzzlesearch_b200 as psb
+from _puzzles import make
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SPECS = [["sliding", 3, 2], ["sliding", 4, 4], ["sliding", 3, 4], ["sliding", 2, 8], ["sliding", 1, 2],
@@ -19,13 +20,6 @@ SPECS = [["sliding", 3, 2], ["sliding", 4, 4], ["sliding", 3, 4], ["sliding", 2,
          ["hanoi4", 1, 0], ["hanoi4", 7, 1], ["hanoi4", 18, 0], ["hanoi4", 31, 0]]
 
 
-def make(spec):
-    kind, a, b = spec
-    if kind == "sliding":
-        return psb.SlidingTilePuzzleSimple(a, b)
-    if kind == "pancake":
-        return psb.PancakeSimple(a)
-    return psb.FourPegHanoiSimple(a, bool(b))
 
 
 def declared_functions():

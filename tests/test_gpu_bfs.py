@@ -11,19 +11,13 @@ import pytest
 
 import oracle as O
 import puzzlesearch_b200 as psb
+from _puzzles import make
 
 pytestmark = pytest.mark.gpu
 
 ALGOS = ["two_bit", "three_bit", "frontier", "classic"]
 
 
-def make(spec):
-    kind, a, b = spec
-    if kind == "sliding":
-        return psb.SlidingTilePuzzleSimple(a, b)
-    if kind == "pancake":
-        return psb.PancakeSimple(a)
-    return psb.FourPegHanoiSimple(a, bool(b))
 
 
 def algos_for(p):

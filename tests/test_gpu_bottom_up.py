@@ -13,6 +13,7 @@ import pytest
 
 import oracle as O
 import puzzlesearch_b200 as psb
+from _puzzles import make
 
 pytestmark = pytest.mark.gpu
 
@@ -26,13 +27,6 @@ def oracle_bfs(spec, algo, init):
     return O.bfs(list(spec), algo, init, final=True)
 
 
-def make(spec):
-    kind, a, b = spec
-    if kind == "sliding":
-        return psb.SlidingTilePuzzleSimple(a, b)
-    if kind == "pancake":
-        return psb.PancakeSimple(a)
-    return psb.FourPegHanoiSimple(a, bool(b))
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0][0]}{c[0][1]}x{c[0][2]}")

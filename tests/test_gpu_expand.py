@@ -9,17 +9,11 @@ import pytest
 
 import oracle as O
 import puzzlesearch_b200 as psb
+from _puzzles import make
 
 pytestmark = pytest.mark.gpu
 
 
-def make(spec):
-    kind, a, b = spec
-    if kind == "sliding":
-        return psb.SlidingTilePuzzleSimple(a, b)
-    if kind == "pancake":
-        return psb.PancakeSimple(a)
-    return psb.FourPegHanoiSimple(a, bool(b))
 
 
 ALL_SPECS = ([["pancake", n, 0] for n in range(2, 17)] +

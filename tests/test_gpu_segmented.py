@@ -11,14 +11,11 @@ import pytest
 
 import oracle as O
 import puzzlesearch_b200 as psb
+from _puzzles import make
 
 pytestmark = pytest.mark.gpu
 
 
-def make(spec):
-    kind, a, b = spec
-    return {"sliding": lambda: psb.SlidingTilePuzzleSimple(a, b), "pancake": lambda: psb.PancakeSimple(a),
-            "hanoi4": lambda: psb.FourPegHanoiSimple(a, bool(b))}[kind]()
 
 
 @pytest.mark.parametrize("spec,bits", [(["sliding", 5, 2], 19), (["sliding", 5, 2], 15), (["sliding", 5, 2], 22),

@@ -12,14 +12,11 @@ import pytest
 
 import oracle as O
 import puzzlesearch_b200 as psb
+from _puzzles import make
 
 pytestmark = pytest.mark.gpu
 
 
-def make(spec):
-    kind, a, b = spec
-    return {"sliding": lambda: psb.SlidingTilePuzzleSimple(a, b), "pancake": lambda: psb.PancakeSimple(a),
-            "hanoi4": lambda: psb.FourPegHanoiSimple(a, bool(b))}[kind]()
 
 
 def run_spill(spec, algo, start=0, segment_bits=0, **kw):

@@ -342,3 +342,61 @@ def test_hanoi_optimized_matches_reference():
     for n, sym in ((8, 0), (9, 1)):
         start = O.to_string(["hanoi4", n, sym], 0)
         assert O.ref_bfs(["hanoi4_opt", n, sym], "three_bit", start) == O.bfs(["hanoi4_opt", n, sym], "three_bit")[0]
+
+
+SLIDING_OPT_SHAPES = [(2, 2), (3, 2), (4, 2), (5, 2), (6, 2), (7, 2), (8, 2), (3, 3), (4, 3), (5, 3), (4, 4)]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_sliding_optimized_index_matches_reference():
+    """SlidingTilePuzzleOptimized's index (Puzzles/SlidingTilePuzzleOptimized.cpp:
+    99-236): the oracle's Parse, ToString and IndexesCount equal the reference
+    class's own on random solvable boards of every shape the reference
+    instantiates (the reference's Expand runs on a GPU and is not built into
+    the oracle; the expand is pinned by the Opt3x2 / Opt4x4 known answers and
+    by search counts)."""
+    rng = random.Random(31)
+    for w, h in SLIDING_OPT_SHAPES:
+        spec = ["sliding_opt", w, h]
+        assert O.info(spec)["indexes"] == O.ref_indexes_count(spec), spec
+        checked = 0
+        while checked < 60:
+            perm = list(range(w * h))
+            rng.shuffle(perm)
+            state = " ".join(map(str, perm))
+            try:
+                index = O.parse(spec, state)
+            except ValueError:
+                continue  # the other parity class: the reference's Parse exits on it
+            assert index == O.ref_parse(spec, state), (spec, state)
+            assert O.to_string(spec, index) == state == O.ref_to_string(spec, index), (spec, state)
+            checked += 1
+
+
+def test_sliding_optimized_searches_equal_simple(golden):
+    """Search counts are index-independent: the optimized index gives the
+    golden ST vectors (PuzzleSearchTests.cpp:294-333 run DiskBasedOpt* on
+    SlidingTilePuzzleOptimized<5, 2> and expect ST5x2), and left / right
+    moves are the index -+ 1 of the blank digit."""
+    ran = 0
+    for v in golden["search"]:
+        spec = v["puzzle"]
+        if spec[0] != "sliding" or not v["full"] or n_states(spec) > SMALL:
+            continue
+        ospec = ["sliding_opt", spec[1], spec[2]]
+        init = O.parse(ospec, v["start"])
+        for algo in ("two_bit", "three_bit", "frontier", "classic"):
+            assert O.bfs(ospec, algo, init)[0] == v["counts"], (ospec, algo, v["source"])
+            ran += 1
+    assert ran >= 8
+    rng = random.Random(5)
+    spec = ["sliding_opt", 4, 3]
+    parents = []
+    while len(parents) < 300:
+        i = rng.randrange(O.info(spec)["indexes"])
+        if (i & 15) < 12:
+            parents.append(i)
+    ch, ops = O.expand(spec, parents)
+    simple = ["sliding", 4, 3]
+    sch, sops = O.expand(simple, [O.parse(simple, O.to_string(spec, p)) for p in parents])
+    assert [O.to_string(spec, c) for c in ch] == [O.to_string(simple, c) for c in sch] and ops == sops
