@@ -38,7 +38,9 @@ enum {
     PSB_ERR_UNSUPPORTED = -5, /* combination not supported (e.g. frontier search with > 4 operators) */
     PSB_ERR_DEVICE = -6,      /* a kernel reported an internal error (index out of range) */
     PSB_ERR_NO_DEVICE = -7,   /* no CUDA device visible */
-    PSB_ERR_ABORTED = -8      /* a callback (psb_spill_fn) returned non-zero */
+    PSB_ERR_ABORTED = -8,     /* a callback (psb_spill_fn) returned non-zero */
+    PSB_ERR_IO = -9           /* a file of a segment store could not be created, written, read or removed
+                                 (the reference's file layer exits instead, Common/File.cpp) */
 };
 
 /* Puzzle kinds (the reference's *Simple classes). */
@@ -325,34 +327,64 @@ int psb_frontier_decode(const uint8_t* d_stream, const psb_codec_block* blocks, 
 int psb_opbits_encode(int bits, const uint8_t* d_op_bits, uint64_t count, uint8_t* d_out, void* stream);
 int psb_opbits_decode(int bits, const uint8_t* d_in, uint64_t count, uint8_t* d_op_bits, void* stream);
 
+/* --- Segment store -----------------------------------------------------------------
+ * The reference's Store (Common/Store.h:13-178): numbered segments, each a
+ * list of chunks read back in the order they were written.  With
+ * directories, the segments go round-robin over the directories (one per
+ * disk, StoreOptions::directories) and, in each, to files_per_path files of
+ * consecutive segments (StoreOptions::filesPerPath: 0 = one file per
+ * segment, <dir>/<name>_<segment>; 1 = <dir>/<name>; k = <dir>/<name>_p0 ..
+ * _p<k-1>).  A file exists while one of its segments holds data: it is
+ * removed once they are all deleted, and by psb_store_destroy.  Without
+ * directories the chunks stay in host memory.  Not thread-safe for
+ * concurrent reads of one segment. */
+typedef struct psb_store psb_store;
+int psb_store_create(int max_segments, const char* name, const char* const* directories, int n_directories,
+                     int files_per_path, psb_store** out);
+int psb_store_destroy(psb_store* store);  /* removes its files */
+int psb_store_write(psb_store* store, int segment, const void* buf, uint64_t size);  /* appends one chunk */
+/* Next chunk of the segment into buf: *got = its size, 0 after the last one;
+ * PSB_ERR_CAPACITY if the chunk is larger than cap. */
+int psb_store_read(psb_store* store, int segment, void* buf, uint64_t cap, uint64_t* got);
+int psb_store_rewind(psb_store* store, int segment);                   /* read from the first chunk again */
+int psb_store_length(const psb_store* store, int segment, uint64_t* bytes);  /* segment < 0: all of them */
+int psb_store_delete(psb_store* store, int segment);                   /* segment < 0: all of them */
+
 /* --- Segmented (out-of-core) search -------------------------------------------
  * The reference's disk-based search, DiskBasedOptThreeBitBFS
- * (Common/DiskBasedOptThreeBitBFS.cpp:12-252), with host memory in place of
- * its segment files: the state space is split into segments of
- * 2^segment_bits states (SegmentedOptions::GetSegIdx, Common/DiskBasedBFS.h:
- * 22-24) and only one segment's three bit arrays (3 x 2^segment_bits bits)
- * plus an expansion buffer sit in device memory.  Every segment's last three
- * frontier layers are kept in host memory as the reference's compressed
- * segment streams, and the children a segment's states have in other
- * segments as 4-byte offsets per target segment.  Per-depth counts equal the
- * in-memory searches'.  A search larger than device memory runs this way;
- * PCIe carries the layers and the cross-segment children. */
+ * (Common/DiskBasedOptThreeBitBFS.cpp:12-252): the state space is split into
+ * segments of 2^segment_bits states (SegmentedOptions::GetSegIdx,
+ * Common/DiskBasedBFS.h:22-24) and only one segment's three bit arrays
+ * (3 x 2^segment_bits bits) plus an expansion buffer sit in device memory.
+ * Every segment's last three frontier layers are kept as the reference's
+ * compressed segment streams, and the children a segment's states have in
+ * other segments as 4-byte offsets per target segment, in segment stores:
+ * files in opts->directories (the reference's StoreOptions), else host
+ * memory.  Per-depth counts equal the in-memory searches'.  A search larger
+ * than device memory runs this way, and one larger than host memory with
+ * directories; PCIe carries the layers and the cross-segment children. */
 typedef struct {
     uint32_t struct_size;   /* sizeof(psb_segmented_opts) */
     uint32_t max_depth;     /* stop after this depth (0 = until the frontier is empty) */
     int32_t segment_bits;   /* 10..32 (0 = 32, PuzzleOptions::segmentBits' default) */
     int32_t device;         /* CUDA device (-1 = current) */
     uint64_t chunk_states;  /* states expanded per launch (bounds the child buffer; 0 = 2^22) */
+    const char* const* directories; /* StoreOptions::directories: the layers and the cross-segment children go
+                                       to files there (segment stores, above); none = host memory */
+    int32_t n_directories;
+    int32_t files_per_path; /* StoreOptions::filesPerPath (Common/Store.h:20-27); -1 = its default, 5 */
 } psb_segmented_opts;
 typedef struct {
     uint32_t struct_size;     /* sizeof(psb_segmented_stats) */
     uint32_t pad;
     uint64_t segments;        /* segments of the state space */
     uint64_t device_bytes;    /* device memory the search held */
-    uint64_t peak_host_bytes; /* largest host memory held by layers and cross-segment children */
+    uint64_t peak_host_bytes; /* largest host memory held by layers and cross-segment children (with
+                                 directories: the staging of the cross-segment children only) */
     uint64_t h2d_bytes, d2h_bytes;
     uint64_t cross_children;  /* children that landed in another segment than their parent's */
     double total_ms;          /* wall time of the call */
+    uint64_t peak_disk_bytes; /* largest size of the store files (with directories) */
 } psb_segmented_stats;
 int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial_index, const psb_segmented_opts* opts,
                       uint64_t* depth_counts, uint32_t counts_cap, uint32_t* n_depths, psb_segmented_stats* stats);

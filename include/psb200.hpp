@@ -385,7 +385,10 @@ struct PuzzleOptions {
 // The reference's disk-based searches (Common/DiskBasedBFS.h:40-46) all
 // return the per-depth counts of the whole space; here each is the segmented
 // out-of-core search of psb_bfs_segmented (one segment's arrays on the
-// device at a time, DiskBasedOptThreeBitBFS's three-layer scheme).
+// device at a time, DiskBasedOptThreeBitBFS's three-layer scheme), whose
+// segment files go to opts.storeOptions.directories (filesPerPath files of
+// consecutive segments per directory) as the reference's do; an empty
+// directory list keeps them in host memory.
 inline std::vector<uint64_t> RunSegmented(Puzzle& puzzle, const std::string& initialState, const PuzzleOptions& opts) {
     if (!puzzle.handle())
         throw Error(PSB_ERR_UNSUPPORTED, "psb200: the segmented searches run on the GPU for this library's puzzle "
@@ -396,6 +399,11 @@ inline std::vector<uint64_t> RunSegmented(Puzzle& puzzle, const std::string& ini
     o.segment_bits = opts.segmentBits;
     o.device = -1;
     o.max_depth = opts.maxSteps < 10000 ? uint32_t(opts.maxSteps) : 0;
+    std::vector<const char*> dirs;
+    for (const std::string& d : opts.storeOptions.directories) dirs.push_back(d.c_str());
+    o.directories = dirs.empty() ? nullptr : dirs.data();
+    o.n_directories = int32_t(dirs.size());
+    o.files_per_path = opts.storeOptions.filesPerPath;
     std::vector<uint64_t> counts(1 << 16);
     uint32_t n = 0;
     check(psb_bfs_segmented(puzzle.handle(), init, &o, counts.data(), uint32_t(counts.size()), &n, nullptr));

@@ -17,7 +17,7 @@ import os
 __all__ = [
     "PsbError", "lib", "SlidingTilePuzzleSimple", "SlidingTilePuzzleOptimized", "PancakeSimple", "PancakeOptimized", "FourPegHanoiOptimized", "FourPegHanoiSimple",
     "InMemoryTwoBitBFS", "InMemoryThreeBitBFS", "InMemoryFrontierSearch", "InMemoryClassicBFS",
-    "bfs", "bfs_segmented", "BfsSession", "TWO_BIT", "THREE_BIT", "FRONTIER", "CLASSIC", "INVALID_INDEX",
+    "bfs", "bfs_segmented", "BfsSession", "Store", "TWO_BIT", "THREE_BIT", "FRONTIER", "CLASSIC", "INVALID_INDEX",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -84,14 +84,16 @@ class ServerOpts(ctypes.Structure):
 
 class SegmentedOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("segment_bits", ctypes.c_int32),
-                ("device", ctypes.c_int32), ("chunk_states", ctypes.c_uint64)]
+                ("device", ctypes.c_int32), ("chunk_states", ctypes.c_uint64),
+                ("directories", ctypes.POINTER(ctypes.c_char_p)), ("n_directories", ctypes.c_int32),
+                ("files_per_path", ctypes.c_int32)]
 
 
 class SegmentedStats(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("segments", ctypes.c_uint64),
                 ("device_bytes", ctypes.c_uint64), ("peak_host_bytes", ctypes.c_uint64),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("cross_children", ctypes.c_uint64),
-                ("total_ms", ctypes.c_double)]
+                ("total_ms", ctypes.c_double), ("peak_disk_bytes", ctypes.c_uint64)]
 
 
 class CodecBlock(ctypes.Structure):
@@ -150,6 +152,15 @@ def lib():
                                         ctypes.c_void_p]
         L.psb_bfs_segmented.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(SegmentedOpts), u64p, ctypes.c_uint32,
                                         u32p, ctypes.POINTER(SegmentedStats)]
+        cpp = ctypes.POINTER(ctypes.c_char_p)
+        L.psb_store_create.argtypes = [ctypes.c_int, ctypes.c_char_p, cpp, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(P)]
+        L.psb_store_destroy.argtypes = [P]
+        L.psb_store_write.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64]
+        L.psb_store_read.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, u64p]
+        L.psb_store_rewind.argtypes = [P, ctypes.c_int]
+        L.psb_store_length.argtypes = [P, ctypes.c_int, u64p]
+        L.psb_store_delete.argtypes = [P, ctypes.c_int]
         L.psb_engine_create.argtypes = [ctypes.POINTER(EngineOpts), ctypes.POINTER(P)]
         L.psb_engine_destroy.argtypes = [P]
         L.psb_engine_footprint.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, u64p]
@@ -453,21 +464,72 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
     return out
 
 
-def bfs_segmented(puzzle, initial=0, segment_bits=0, max_depth=0, chunk_states=0, device=-1):
+def bfs_segmented(puzzle, initial=0, segment_bits=0, max_depth=0, chunk_states=0, device=-1, directories=(),
+                  files_per_path=-1):
     """psb_bfs_segmented: the out-of-core three-layer search (one segment's
-    bit arrays on the device at a time).  Returns {"counts", "stats"}."""
+    bit arrays on the device at a time).  directories / files_per_path: the
+    reference's StoreOptions (segment files there; none = host memory).
+    Returns {"counts", "stats"}."""
     if isinstance(initial, str):
         initial = puzzle.Parse(initial)
     cap = 1 << 16
     counts = (ctypes.c_uint64 * cap)()
     nd = ctypes.c_uint32()
-    o = SegmentedOpts(ctypes.sizeof(SegmentedOpts), max_depth, segment_bits, device, chunk_states)
+    dirs = (ctypes.c_char_p * max(1, len(directories)))(*[os.fsencode(d) for d in directories])
+    o = SegmentedOpts(ctypes.sizeof(SegmentedOpts), max_depth, segment_bits, device, chunk_states,
+                      ctypes.cast(dirs, ctypes.POINTER(ctypes.c_char_p)), len(directories), files_per_path)
     st = SegmentedStats()
     st.struct_size = ctypes.sizeof(SegmentedStats)
     _check(lib().psb_bfs_segmented(puzzle.handle, initial, ctypes.byref(o), counts, cap, ctypes.byref(nd),
                                    ctypes.byref(st)))
     return {"counts": list(counts[:nd.value]),
             "stats": {k: getattr(st, k) for k, _ in SegmentedStats._fields_ if k not in ("struct_size", "pad")}}
+
+
+class Store:
+    """psb_store: the reference's Store (Common/Store.h:13-178) -- numbered
+    segments, each a list of chunks read back in write order; files in
+    `directories` (StoreOptions), or host memory without any."""
+
+    def __init__(self, max_segments, name, directories=(), files_per_path=5):
+        dirs = (ctypes.c_char_p * max(1, len(directories)))(*[os.fsencode(d) for d in directories])
+        h = ctypes.c_void_p()
+        _check(lib().psb_store_create(max_segments, name.encode(), dirs, len(directories), files_per_path,
+                                      ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            h, self._h = self._h, None
+            _check(lib().psb_store_destroy(h))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def Write(self, segment, data):
+        buf = (ctypes.c_uint8 * max(1, len(data))).from_buffer_copy(bytes(data) or b"\0")
+        _check(lib().psb_store_write(self._h, segment, buf, len(data)))
+
+    def Read(self, segment, cap=1 << 24):
+        """The next chunk of the segment (b"" after the last one)."""
+        buf = (ctypes.c_uint8 * cap)()
+        got = ctypes.c_uint64()
+        _check(lib().psb_store_read(self._h, segment, buf, cap, ctypes.byref(got)))
+        return bytes(buf[:got.value])
+
+    def Rewind(self, segment):
+        _check(lib().psb_store_rewind(self._h, segment))
+
+    def Length(self, segment=-1):
+        n = ctypes.c_uint64()
+        _check(lib().psb_store_length(self._h, segment, ctypes.byref(n)))
+        return n.value
+
+    def Delete(self, segment=-1):
+        _check(lib().psb_store_delete(self._h, segment))
 
 
 class BfsSession:

@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
 
 #include "psb_kernels.cuh"
 
@@ -62,6 +65,22 @@ void encoder_set_ops(SegmentEncoder* e, bool on, const uint64_t* nibbles, uint64
 int encoder_chunk_sums(SegmentEncoder* e, uint64_t n_bits, unsigned long long** sums);
 // Kernels the encoder launched since the last call.
 uint64_t encoder_take_launches(SegmentEncoder* e);
+// Segment store (psb_store.cu): the reference's Store over files in some
+// directories, or over host memory when there are none.
+class StoreImpl;
+void store_destroy(StoreImpl* s);
+struct StoreDeleter { void operator()(StoreImpl* s) const { store_destroy(s); } };
+using StorePtr = std::unique_ptr<StoreImpl, StoreDeleter>;
+int store_create(int max_segments, const std::string& name, const std::vector<std::string>& directories,
+                 int files_per_path, StorePtr* out);
+uint64_t store_length(const StoreImpl& s, int segment);
+uint64_t store_total(const StoreImpl& s);
+void store_rewind(StoreImpl& s, int segment);
+int store_write(StoreImpl& s, int segment, const void* buf, uint64_t size);
+int store_read(StoreImpl& s, int segment, void* buf, uint64_t cap, uint64_t* got);
+int store_erase(StoreImpl& s, int segment);
+int store_erase_all(StoreImpl& s);
+
 // Decodes a segment stream (block table `d_blocks` in device memory) into
 // the cleared bitmap d_bits[0, n_bits) on stream s, without allocating or
 // synchronising; an offset outside the segment sets *d_err.

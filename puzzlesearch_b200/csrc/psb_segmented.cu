@@ -90,13 +90,11 @@ namespace {
             return psb_set_error(PSB_ERR_CUDA, (std::string(#call) + ": " + cudaGetErrorString(e_)).c_str()); \
     } while (0)
 
-// One segment's frontier layer: the reference's compressed segment stream
-// and its block table (for the device decoder).
-struct Layer {
-    std::vector<uint8_t> bytes;
-    std::vector<psb_codec_block> blocks;
-    uint64_t count = 0;
-};
+// Staged cross-segment children of one target segment are written to the
+// store in chunks of up to this many offsets (the reference's Multiplexor
+// buffers, Common/Multiplexor.cpp:5-33), fewer when there are many segments.
+constexpr uint64_t kStageMax = 16384;
+constexpr uint64_t kStageBudget = uint64_t(1) << 26;  // bytes of staging over all segments
 
 template <class T>
 struct DevBuf {
@@ -128,69 +126,118 @@ struct Run {
     DevBuf<unsigned int> hist;
     DevBuf<unsigned long long> scalars;  // [0] count, [1] children appended, [2] error flag, [3] decode error
     psb::SegmentEncoder* enc = nullptr;  // device scratch kept from segment to segment
+    std::vector<uint8_t> host_stream;    // one layer between the store and the device
+    std::vector<psb_codec_block> blocks;
+    std::vector<uint32_t> host_offs;     // cross-segment children between the device and the staging
+    // Multiplexor staging: per target segment, the offsets not yet written.
+    uint64_t stage_cap = 0;
+    std::vector<uint32_t> stage;
+    std::vector<uint32_t> stage_len;
+    bool files = false;                  // the stores are files (else host memory)
     psb_segmented_stats st{};
 
     ~Run() { if (enc) psb::encoder_destroy(enc); }
 
     uint64_t states_in(uint64_t g) const { return std::min(seg_states, P->n_states - g * seg_states); }
 
-    // Decodes a layer into a cleared segment bitmap (slot 0 or 1: the two
-    // layers of one segment are in flight together).  Nothing waits: a bad
-    // offset sets scalars[3], read at the end of the depth.
-    int decode(const Layer& L, uint64_t* bits, uint64_t g, int slot) {
+    // Decodes segment g's layer from `store` into a cleared segment bitmap
+    // (slot 0 or 1: the two layers of one segment are in flight together).
+    // Nothing waits on the device: a bad offset sets scalars[3], read at the
+    // end of the depth.
+    int decode(psb::StoreImpl& store, uint64_t* bits, uint64_t g, int slot) {
         SG_CUDA(cudaMemsetAsync(bits, 0, seg_words * 8, s));
-        if (L.count == 0) return PSB_OK;
-        if (int rc = stream_buf[slot].grow(L.bytes.size())) return rc;
-        if (int rc = block_tab[slot].grow(L.blocks.size())) return rc;
-        SG_CUDA(cudaMemcpyAsync(stream_buf[slot].p, L.bytes.data(), L.bytes.size(), cudaMemcpyHostToDevice, s));
-        SG_CUDA(cudaMemcpyAsync(block_tab[slot].p, L.blocks.data(), L.blocks.size() * sizeof(psb_codec_block),
+        const uint64_t bytes = psb::store_length(store, int(g));
+        if (bytes == 0) return PSB_OK;
+        if (host_stream.size() < bytes) host_stream.resize(bytes);
+        psb::store_rewind(store, int(g));
+        uint64_t got = 0;
+        if (int rc = psb::store_read(store, int(g), host_stream.data(), bytes, &got)) return rc;
+        if (got != bytes) return psb_set_error(PSB_ERR_IO, "segmented search: a layer came back short");
+        uint32_t nb = 0;
+        if (int rc = psb_frontier_index(host_stream.data(), bytes, nullptr, 0, &nb)) return rc;
+        blocks.resize(nb);
+        if (int rc = psb_frontier_index(host_stream.data(), bytes, blocks.data(), nb, &nb)) return rc;
+        if (int rc = stream_buf[slot].grow(bytes)) return rc;
+        if (int rc = block_tab[slot].grow(nb)) return rc;
+        // Pageable sources: both copies have left host memory when the calls return.
+        SG_CUDA(cudaMemcpyAsync(stream_buf[slot].p, host_stream.data(), bytes, cudaMemcpyHostToDevice, s));
+        SG_CUDA(cudaMemcpyAsync(block_tab[slot].p, blocks.data(), nb * sizeof(psb_codec_block),
                                 cudaMemcpyHostToDevice, s));
-        st.h2d_bytes += L.bytes.size();
-        return psb::frontier_decode_async(stream_buf[slot].p, block_tab[slot].p, uint32_t(L.blocks.size()), bits,
-                                          states_in(g), scalars.p + 3, s);
+        st.h2d_bytes += bytes;
+        return psb::frontier_decode_async(stream_buf[slot].p, block_tab[slot].p, nb, bits, states_in(g),
+                                          scalars.p + 3, s);
     }
 
-    // Encodes a segment bitmap holding `count` states into a layer.
-    int encode(const uint64_t* bits, uint64_t g, uint64_t count, Layer* L) {
-        L->bytes.clear();
-        L->blocks.clear();
-        L->count = count;
+    // Encodes a segment bitmap holding `count` states as segment g's layer in `store`.
+    int encode(const uint64_t* bits, uint64_t g, uint64_t count, psb::StoreImpl& store) {
         if (count == 0) return PSB_OK;
         uint64_t bytes = 0, n = 0;
         if (int rc = psb::encoder_plan(enc, bits, states_in(g), s, false, &bytes, &n)) return rc;
         if (n != count) return psb_set_error(PSB_ERR_DEVICE, "segmented search: layer count mismatch");
         if (int rc = stream_buf[0].grow(bytes)) return rc;
         if (int rc = psb::encoder_write(enc, stream_buf[0].p, s)) return rc;
-        L->bytes.resize(bytes);
-        SG_CUDA(cudaMemcpyAsync(L->bytes.data(), stream_buf[0].p, bytes, cudaMemcpyDeviceToHost, s));
+        if (host_stream.size() < bytes) host_stream.resize(bytes);
+        SG_CUDA(cudaMemcpyAsync(host_stream.data(), stream_buf[0].p, bytes, cudaMemcpyDeviceToHost, s));
         SG_CUDA(cudaStreamSynchronize(s));
-        // The block table, for the decoder: read back from the stream's own headers.
-        uint32_t nb = 0;
-        if (int rc = psb_frontier_index(L->bytes.data(), bytes, nullptr, 0, &nb)) return rc;
-        L->blocks.resize(nb);
-        if (int rc = psb_frontier_index(L->bytes.data(), bytes, L->blocks.data(), nb, &nb)) return rc;
         st.d2h_bytes += bytes;
-        return PSB_OK;
+        return psb::store_write(store, int(g), host_stream.data(), bytes);
     }
 
-    // ORs the offsets a segment received into `bits`.
-    int receive(const std::vector<uint32_t>& list, uint64_t* bits) {
-        for (uint64_t at = 0; at < list.size(); at += offs.cap) {
-            const uint64_t n = std::min<uint64_t>(offs.cap, list.size() - at);
-            SG_CUDA(cudaMemcpyAsync(offs.p, list.data() + at, n * 4, cudaMemcpyHostToDevice, s));
-            st.h2d_bytes += n * 4;
-            psb::seg_set_offsets<<<unsigned(std::min<uint64_t>((n + psb::kThreads - 1) / psb::kThreads, 148 * 16)),
-                                   psb::kThreads, 0, s>>>(bits, offs.p, n);
-            SG_CUDA(cudaGetLastError());
-            SG_CUDA(cudaStreamSynchronize(s));  // the staging buffer is reused
+    // ORs the offsets segment g received (its chunks in `store`) into `bits`,
+    // then drops them from the store.
+    int receive(psb::StoreImpl& store, uint64_t g, uint64_t* bits) {
+        const uint64_t bytes = psb::store_length(store, int(g));
+        if (bytes == 0) return PSB_OK;
+        if (host_offs.size() < bytes / 4) host_offs.resize(bytes / 4);
+        psb::store_rewind(store, int(g));
+        uint64_t n = 0;
+        for (;;) {
+            uint64_t got = 0;
+            if (int rc = psb::store_read(store, int(g), host_offs.data() + n, bytes - n * 4, &got)) return rc;
+            if (got == 0) break;
+            n += got / 4;
+        }
+        if (int rc = offs.grow(n)) return rc;
+        SG_CUDA(cudaMemcpyAsync(offs.p, host_offs.data(), n * 4, cudaMemcpyHostToDevice, s));
+        st.h2d_bytes += n * 4;
+        psb::seg_set_offsets<<<unsigned(std::min<uint64_t>((n + psb::kThreads - 1) / psb::kThreads, 148 * 16)),
+                               psb::kThreads, 0, s>>>(bits, offs.p, n);
+        SG_CUDA(cudaGetLastError());
+        return psb::store_erase(store, int(g));
+    }
+
+    // Appends offsets for target segment t to its staging, writing full
+    // stages to `store` (Multiplexor::Add, Common/Multiplexor.cpp:10-19).
+    int stage_add(psb::StoreImpl& store, uint64_t t, const uint32_t* v, uint64_t n) {
+        uint32_t* buf = stage.data() + t * stage_cap;
+        while (n) {
+            const uint64_t k = std::min<uint64_t>(n, stage_cap - stage_len[t]);
+            std::memcpy(buf + stage_len[t], v, k * 4);
+            stage_len[t] += uint32_t(k);
+            v += k;
+            n -= k;
+            if (stage_len[t] == stage_cap) {
+                if (int rc = psb::store_write(store, int(t), buf, stage_cap * 4)) return rc;
+                stage_len[t] = 0;
+            }
+        }
+        return PSB_OK;
+    }
+    int stage_flush(psb::StoreImpl& store) {  // Multiplexor::FlushAllSegments
+        for (uint64_t t = 0; t < n_segments; t++) {
+            if (!stage_len[t]) continue;
+            if (int rc = psb::store_write(store, int(t), stage.data() + t * stage_cap, uint64_t(stage_len[t]) * 4))
+                return rc;
+            stage_len[t] = 0;
         }
         return PSB_OK;
     }
 
-    // Expands the states of `bits` (segment g) chunk by chunk: cross == 0
-    // marks the children inside g in `next`; cross == 1 appends the offsets
-    // of the children outside g to their target segments' lists.
-    int expand(const uint64_t* bits, uint64_t g, int cross, std::vector<std::vector<uint32_t>>* lists) {
+    // Expands the states of `bits` (segment g) chunk by chunk: with no store
+    // it marks the children inside g in `next`; with one it stages the
+    // offsets of the children outside g for their target segments.
+    int expand(const uint64_t* bits, uint64_t g, psb::StoreImpl* cross_store) {
+        const int cross = cross_store != nullptr;
         psb::SegExpandArgs a{};
         a.bits = bits;
         a.seg_base = g * seg_states;
@@ -203,6 +250,7 @@ struct Run {
         a.cross = cross;
         a.pz = P->pz;
         a.err = scalars.p + 2;
+        std::vector<unsigned int> h(cross ? n_segments : 0), start(cross ? n_segments : 0);
         for (uint64_t w = 0; w < seg_words; w += chunk_words) {
             a.word_lo = w;
             a.word_hi = std::min(seg_words, w + chunk_words);
@@ -220,37 +268,26 @@ struct Run {
             SG_CUDA(cudaMemsetAsync(hist.p, 0, n_segments * 4, s));
             const unsigned pg = unsigned(std::min<uint64_t>((n + psb::kThreads - 1) / psb::kThreads, 148 * 16));
             psb::seg_histogram<<<pg, psb::kThreads, 0, s>>>(kids.p, n, sb, hist.p);
-            std::vector<unsigned int> h(n_segments);
             SG_CUDA(cudaMemcpyAsync(h.data(), hist.p, n_segments * 4, cudaMemcpyDeviceToHost, s));
             SG_CUDA(cudaStreamSynchronize(s));
-            std::vector<unsigned int> start(n_segments);
             unsigned int acc = 0;
             for (uint64_t t = 0; t < n_segments; t++) { start[t] = acc; acc += h[t]; }
             SG_CUDA(cudaMemcpyAsync(hist.p, start.data(), n_segments * 4, cudaMemcpyHostToDevice, s));
             if (int rc = offs.grow(n)) return rc;
             psb::seg_scatter<<<pg, psb::kThreads, 0, s>>>(kids.p, n, sb, hist.p, offs.p);
             SG_CUDA(cudaGetLastError());
-            std::vector<uint32_t> host(n);
-            SG_CUDA(cudaMemcpyAsync(host.data(), offs.p, n * 4, cudaMemcpyDeviceToHost, s));
+            if (host_offs.size() < n) host_offs.resize(n);
+            SG_CUDA(cudaMemcpyAsync(host_offs.data(), offs.p, n * 4, cudaMemcpyDeviceToHost, s));
             SG_CUDA(cudaStreamSynchronize(s));
             st.d2h_bytes += n * 4;
             for (uint64_t t = 0; t < n_segments; t++)
-                if (h[t]) (*lists)[t].insert((*lists)[t].end(), host.begin() + start[t], host.begin() + start[t] + h[t]);
+                if (h[t])
+                    if (int rc = stage_add(*cross_store, t, host_offs.data() + start[t], h[t])) return rc;
         }
         SG_CUDA(cudaStreamSynchronize(s));
         return PSB_OK;
     }
 };
-
-uint64_t host_bytes(const std::vector<Layer>& a, const std::vector<Layer>& b, const std::vector<Layer>& c,
-                    const std::vector<std::vector<uint32_t>>& x, const std::vector<std::vector<uint32_t>>& y) {
-    uint64_t n = 0;
-    for (auto* v : {&a, &b, &c})
-        for (const Layer& L : *v) n += L.bytes.size();
-    for (auto* v : {&x, &y})
-        for (const auto& l : *v) n += l.size() * 4;
-    return n;
-}
 
 }  // namespace
 
@@ -262,6 +299,15 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
     if (initial >= p->n_states) return psb_set_error(PSB_ERR_ARG, "initial index >= IndexesCount()");
     const int sb = opts && opts->segment_bits ? opts->segment_bits : 32;
     if (sb < 10 || sb > 32) return psb_set_error(PSB_ERR_ARG, "segment_bits outside 10..32");
+    std::vector<std::string> dirs;
+    if (opts && opts->n_directories > 0) {
+        if (!opts->directories) return psb_set_error(PSB_ERR_ARG, "directories is NULL");
+        for (int i = 0; i < opts->n_directories; i++) {
+            if (!opts->directories[i] || !*opts->directories[i]) return psb_set_error(PSB_ERR_ARG, "empty directory");
+            dirs.emplace_back(opts->directories[i]);
+        }
+    }
+    const int files_per_path = opts && opts->files_per_path >= 0 ? opts->files_per_path : 5;
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
         return psb_set_error(PSB_ERR_NO_DEVICE, "no CUDA device visible");
@@ -278,6 +324,30 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
     // Expansion chunk: its children fit the child buffer even if every state is set.
     R.chunk_words = std::min<uint64_t>(R.seg_words, opts && opts->chunk_states ? std::max<uint64_t>(1, opts->chunk_states / 64)
                                                                                  : uint64_t(1) << 16);
+    const uint64_t S = R.n_segments;
+    R.stage_cap = std::max<uint64_t>(64, std::min<uint64_t>(kStageMax, kStageBudget / 4 / S));
+    R.stage.assign(S * R.stage_cap, 0);
+    R.stage_len.assign(S, 0);
+    R.files = !dirs.empty();
+
+    // The segment stores: three frontier layers (old, cur, new, rotating) and
+    // the cross-segment children received for this depth and the next
+    // (the reference's DiskBasedOptThreeBitBFS keeps the same five sets,
+    // Common/DiskBasedOptThreeBitBFS.cpp:20-33).
+    psb::StorePtr layer[3], xseg[2];
+    for (int i = 0; i < 3; i++)
+        if (int rc = psb::store_create(int(S), "layer" + std::to_string(i), dirs, files_per_path, &layer[i])) return rc;
+    for (int i = 0; i < 2; i++)
+        if (int rc = psb::store_create(int(S), "xseg" + std::to_string(i), dirs, files_per_path, &xseg[i])) return rc;
+    std::vector<uint64_t> cnt_old(S, 0), cnt_cur(S, 0), cnt_new(S, 0);
+    psb::StoreImpl *old_s = layer[0].get(), *cur_s = layer[1].get(), *new_s = layer[2].get();
+    psb::StoreImpl *recv_s = xseg[0].get(), *next_s = xseg[1].get();
+    auto store_bytes = [&]() {
+        uint64_t n = 0;
+        for (auto* x : {old_s, cur_s, new_s, recv_s, next_s}) n += psb::store_total(*x);
+        return n;
+    };
+
     SG_CUDA(cudaStreamCreateWithFlags(&R.s, cudaStreamNonBlocking));
     struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); } } guard{R.s};
     for (auto* b : {&R.next, &R.cur, &R.old})
@@ -291,10 +361,6 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
     if (!(R.enc = psb::encoder_create())) return psb_set_error(PSB_ERR_NOMEM, "segmented search: encoder");
     SG_CUDA(cudaMemsetAsync(R.scalars.p, 0, 4 * 8, R.s));
 
-    const uint64_t S = R.n_segments;
-    std::vector<Layer> old_l(S), cur_l(S), new_l(S);
-    std::vector<std::vector<uint32_t>> recv(S), recv_next(S);
-
     // Depth 0: the initial state is segment g0's layer; its children in the
     // other segments are collected at once (SetInitialNode,
     // DiskBasedOptThreeBitBFS.cpp:34-53).
@@ -304,8 +370,10 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
         const uint64_t off = initial - g0 * R.seg_states;
         const uint64_t word = uint64_t(1) << (off & 63);
         SG_CUDA(cudaMemcpyAsync(R.next.p + off / 64, &word, 8, cudaMemcpyHostToDevice, R.s));
-        if (int rc = R.encode(R.next.p, g0, 1, &cur_l[g0])) return rc;
-        if (int rc = R.expand(R.next.p, g0, 1, &recv)) return rc;
+        if (int rc = R.encode(R.next.p, g0, 1, *cur_s)) return rc;
+        cnt_cur[g0] = 1;
+        if (int rc = R.expand(R.next.p, g0, recv_s)) return rc;
+        if (int rc = R.stage_flush(*recv_s)) return rc;
     }
     std::vector<uint64_t> res{1};
     const uint32_t max_depth = opts ? opts->max_depth : 0;
@@ -314,17 +382,17 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
         if (max_depth && res.size() >= size_t(max_depth) + 1) break;
         uint64_t total = 0;
         for (uint64_t g = 0; g < S; g++) {
-            if (cur_l[g].count == 0 && recv[g].empty()) {  // no state of depth d+1 can be in g
-                new_l[g] = Layer();
+            cnt_new[g] = 0;
+            if (cnt_cur[g] == 0 && psb::store_length(*recv_s, int(g)) == 0) {  // no state of depth d+1 can be in g
+                if (int rc = psb::store_erase(*old_s, int(g))) return rc;
                 continue;
             }
             SG_CUDA(cudaMemsetAsync(R.next.p, 0, R.seg_words * 8, R.s));
-            if (int rc = R.receive(recv[g], R.next.p)) return rc;
-            std::vector<uint32_t>().swap(recv[g]);
-            if (int rc = R.decode(cur_l[g], R.cur.p, g, 0)) return rc;
-            if (cur_l[g].count)
-                if (int rc = R.expand(R.cur.p, g, 0, nullptr)) return rc;
-            if (int rc = R.decode(old_l[g], R.old.p, g, 1)) return rc;
+            if (int rc = R.receive(*recv_s, g, R.next.p)) return rc;
+            if (int rc = R.decode(*cur_s, R.cur.p, g, 0)) return rc;
+            if (cnt_cur[g])
+                if (int rc = R.expand(R.cur.p, g, nullptr)) return rc;
+            if (int rc = R.decode(*old_s, R.old.p, g, 1)) return rc;
             SG_CUDA(cudaMemsetAsync(R.scalars.p, 0, 8, R.s));
             psb::seg_finish<<<148 * 8, psb::kThreads, 0, R.s>>>(R.next.p, R.old.p, R.cur.p, R.seg_words, odd ? 1 : 0,
                                                                R.scalars.p);
@@ -332,12 +400,18 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
             unsigned long long c = 0;
             SG_CUDA(cudaMemcpyAsync(&c, R.scalars.p, 8, cudaMemcpyDeviceToHost, R.s));
             SG_CUDA(cudaStreamSynchronize(R.s));
+            // g's depth d-1 layer is no longer needed (DeleteSegment of the old layer)
+            if (int rc = psb::store_erase(*old_s, int(g))) return rc;
             total += c;
-            if (int rc = R.encode(R.next.p, g, c, &new_l[g])) return rc;
+            cnt_new[g] = c;
+            if (int rc = R.encode(R.next.p, g, c, *new_s)) return rc;
             if (c)
-                if (int rc = R.expand(R.next.p, g, 1, &recv_next)) return rc;
-            R.st.peak_host_bytes = std::max(R.st.peak_host_bytes, host_bytes(old_l, cur_l, new_l, recv, recv_next));
+                if (int rc = R.expand(R.next.p, g, next_s)) return rc;
+            const uint64_t held = store_bytes();
+            (R.files ? R.st.peak_disk_bytes : R.st.peak_host_bytes) =
+                std::max(R.files ? R.st.peak_disk_bytes : R.st.peak_host_bytes, held);
         }
+        if (int rc = R.stage_flush(*next_s)) return rc;
         unsigned long long err[2] = {0, 0};
         SG_CUDA(cudaMemcpyAsync(err, R.scalars.p + 2, 16, cudaMemcpyDeviceToHost, R.s));
         SG_CUDA(cudaStreamSynchronize(R.s));
@@ -346,11 +420,13 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
         if (total == 0) break;
         if (res.size() >= cap) return psb_set_error(PSB_ERR_CAPACITY, "more depths than counts_cap");
         res.push_back(total);
-        // layers: old <- cur <- new; received children: the next step's
-        old_l.swap(cur_l);
-        cur_l.swap(new_l);
-        recv.swap(recv_next);
-        for (auto& l : recv_next) std::vector<uint32_t>().swap(l);
+        // layers: old <- cur <- new (the emptied old store takes the next layer);
+        // received children: the next step's
+        std::swap(old_s, cur_s);
+        std::swap(cur_s, new_s);
+        cnt_old.swap(cnt_cur);
+        cnt_cur.swap(cnt_new);
+        std::swap(recv_s, next_s);
     }
     std::copy(res.begin(), res.end(), counts);
     *n_depths = uint32_t(res.size());
@@ -359,6 +435,7 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
         R.st.segments = S;
         R.st.device_bytes = (R.next.cap + R.cur.cap + R.old.cap + R.kids.cap) * 8 + R.offs.cap * 4 +
                             R.stream_buf[0].cap + R.stream_buf[1].cap;
+        R.st.peak_host_bytes += R.stage.size() * 4;
         R.st.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         *stats = R.st;
     }

@@ -58,3 +58,26 @@ def test_small_chunks_and_bad_arguments():
     with pytest.raises(psb.PsbError) as e:
         psb.bfs_segmented(p, 0, segment_bits=9)
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("fpp", [0, 1, 5])
+def test_segment_files(tmp_path, fpp):
+    """StoreOptions: the layers and cross-segment children go to files in two
+    directories (filesPerPath 0, 1 and the reference's default 5); the counts
+    equal the in-memory search's, and no file is left afterwards."""
+    import os
+    p = psb.SlidingTilePuzzleSimple(4, 3)
+    dirs = [str(tmp_path / "disk0"), str(tmp_path / "disk1")]
+    r = psb.bfs_segmented(p, 0, segment_bits=24, directories=dirs, files_per_path=fpp)
+    assert r["counts"] == psb.bfs(p, "two_bit", 0)["counts"]
+    assert r["stats"]["peak_disk_bytes"] > 0
+    assert r["stats"]["peak_host_bytes"] < r["stats"]["peak_disk_bytes"]
+    assert all(os.listdir(d) == [] for d in dirs)
+
+
+def test_segment_files_unwritable(tmp_path):
+    f = tmp_path / "plain"
+    f.write_text("x")
+    with pytest.raises(psb.PsbError) as e:
+        psb.bfs_segmented(psb.PancakeSimple(8), 0, segment_bits=10, directories=[str(f)])
+    assert e.value.code == -9
