@@ -68,16 +68,25 @@ def test_searches_bit_exact(w, h, algo):
         assert r["counts"] == counts and r["final"] == fin, (spec, algo, direction)
 
 
-def test_4x3_golden_and_segmented(golden):
-    """The 4x3 golden vector (SlidingPuzzleTests/TestFrontierSearch.cpp:70-72)
-    over the optimized index (319,334,400 indexes); the reference's
-    DiskBasedOpt* bodies on SlidingTilePuzzleOptimized<5, 2>
+def test_legacy_golden_and_segmented(golden):
+    """The reference's sliding-tile vectors over the optimized index: every
+    full vector of SlidingPuzzleTests/TestFrontierSearch.cpp:19-72 up to 12
+    cells (4x3: 319,334,400 indexes), the first 33 depths of 7x2 (:74-76);
+    and the reference's DiskBasedOpt* bodies on SlidingTilePuzzleOptimized<5, 2>
     (PuzzleSearchTests.cpp:294-333, segmentBits 19 and 22) give ST5x2."""
-    v = [x for x in golden["search"] if x["puzzle"] == ["sliding", 4, 3] and x["full"]][0]
-    p = psb.SlidingTilePuzzleOptimized(4, 3)
-    start = p.Parse(v["start"] or " ".join(str(i) for i in range(12)))
-    for algo in ("two_bit", "three_bit"):
-        assert psb.bfs(p, algo, start)["counts"] == v["counts"], algo
+    ran = 0
+    for v in golden["legacy_sliding"]:
+        w, h = v["puzzle"][1:]
+        if w * h < 4 or w * h > 14 or (not v["full"] and w * h != 14):
+            continue
+        p = psb.SlidingTilePuzzleOptimized(w, h)
+        start = p.Parse(v["start"])
+        depth = 0 if v["full"] else len(v["counts"]) - 1
+        for algo in ("two_bit", "three_bit") if w * h <= 12 else ("two_bit",):
+            assert psb.bfs(p, algo, start, max_depth=depth)["counts"] == v["counts"], (v["source"], algo)
+        ran += 1
+    assert ran >= 10
+    psb.lib().psb_release_cached_memory(0)
     st5x2 = [x for x in golden["search"] if x["puzzle"] == ["sliding", 5, 2] and x["full"]][0]["counts"]
     p = psb.SlidingTilePuzzleOptimized(5, 2)
     for sb in (19, 22):
