@@ -1149,17 +1149,54 @@ struct SegEmitter {
     }
 };
 
+// Position of the k-th (0-based) set bit of v (k < popc(v)).
+__device__ __forceinline__ uint32_t select_bit(uint64_t v, uint32_t k) {
+    uint32_t pos = 0, w = uint32_t(v), c = __popc(w);
+    if (k >= c) { k -= c; w = uint32_t(v >> 32); pos = 32; }
+    c = __popc(w & 0xFFFFu); if (k >= c) { k -= c; w >>= 16; pos += 16; }
+    c = __popc(w & 0xFFu);   if (k >= c) { k -= c; w >>= 8;  pos += 8; }
+    c = __popc(w & 0xFu);    if (k >= c) { k -= c; w >>= 4;  pos += 4; }
+    c = __popc(w & 0x3u);    if (k >= c) { k -= c; w >>= 2;  pos += 2; }
+    return pos + ((k >= (w & 1u)) ? 1u : 0u);
+}
+
+// Each warp takes 32 consecutive words of the segment bitmap and expands
+// their set bits 32 at a time, one state per lane: the lanes of a dense word
+// share its states instead of one thread walking all 64.
 template <class PZ>
 __global__ void __launch_bounds__(kThreads) segment_expand_kernel(SegExpandArgs a) {
     SegEmitter em{&a};
-    for (uint64_t w = a.word_lo + blockIdx.x * uint64_t(kThreads) + threadIdx.x; w < a.word_hi;
-         w += uint64_t(gridDim.x) * kThreads) {
-        uint64_t v = a.bits[w];
-        while (v) {
-            const int b = __ffsll((long long)v) - 1;
-            v &= v - 1;
-            const uint64_t i = w * 64 + uint64_t(b);
-            if (i < a.seg_states) PZ::template expand<false>(a.seg_base + i, 0u, a.pz, em);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = (uint64_t(blockIdx.x) * kThreads + threadIdx.x) >> 5;
+    const uint64_t warps = (uint64_t(gridDim.x) * kThreads) >> 5;
+    for (uint64_t w0 = a.word_lo + warp * 32; w0 < a.word_hi; w0 += warps * 32) {
+        const uint64_t w = w0 + lane;
+        const uint64_t v = w < a.word_hi ? a.bits[w] : 0;
+        const uint32_t c = __popcll(v);
+        uint32_t incl = c;  // inclusive prefix of the lanes' set bits
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= uint32_t(o)) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        for (uint32_t base = 0; base < total; base += 32) {
+            const uint32_t k = base + lane;
+            // source lane: the first whose inclusive prefix exceeds k
+            uint32_t lo = 0, hi = 31;
+#pragma unroll
+            for (int step = 0; step < 5; ++step) {
+                const uint32_t mid = (lo + hi) >> 1;
+                const uint32_t im = __shfl_sync(0xFFFFFFFFu, incl, int(mid));
+                if (im > k) hi = mid;
+                else lo = mid + 1;
+            }
+            const uint32_t before = __shfl_sync(0xFFFFFFFFu, incl - c, int(lo));
+            const uint64_t word = __shfl_sync(0xFFFFFFFFu, v, int(lo));
+            if (k < total) {
+                const uint64_t i = (w0 + lo) * 64 + select_bit(word, k - before);
+                if (i < a.seg_states) PZ::template expand<false>(a.seg_base + i, 0u, a.pz, em);
+            }
         }
     }
     if (em.bad) atomicOr(a.err, 1ull);

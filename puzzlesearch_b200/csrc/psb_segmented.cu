@@ -255,8 +255,9 @@ struct Run {
             a.word_lo = w;
             a.word_hi = std::min(seg_words, w + chunk_words);
             SG_CUDA(cudaMemsetAsync(scalars.p + 1, 0, 8, s));
-            const unsigned grid = unsigned(std::min<uint64_t>((a.word_hi - w + psb::kThreads - 1) / psb::kThreads,
-                                                              148 * 8));
+            // one warp per 32 words
+            const uint64_t warps = (a.word_hi - w + 31) / 32;
+            const unsigned grid = unsigned(std::min<uint64_t>((warps * 32 + psb::kThreads - 1) / psb::kThreads, 148 * 8));
             SG_CUDA(P->k.segment_expand(a, grid, s));
             if (!cross) continue;
             unsigned long long n = 0;
