@@ -22,6 +22,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "../../include/psb200.h"
@@ -434,10 +435,11 @@ __global__ void k_write_bitmap(const uint64_t* bits, uint64_t n_words, uint64_t 
 // Decode: one warp per block; StreamVInt blocks are walked by lane 0 (the
 // tuple chain is sequential), bitmap blocks are spread over the lanes.
 __global__ void k_decode(const uint8_t* in, const psb_codec_block* blocks, uint32_t nb, uint64_t* bits,
-                         uint64_t n_bits, unsigned long long* err) {
+                         uint64_t n_bits, unsigned long long* err, int bitmaps_only = 0) {
     const uint32_t b = blockIdx.x;
     if (b >= nb) return;
     const psb_codec_block bk = blocks[b];
+    if (bitmaps_only && !bk.is_bitmap) return;
     const uint8_t* p = in + bk.offset;
     auto put = [&](uint64_t v) {
         if (v >= n_bits) { atomicOr(err, 1ull); return; }
@@ -446,6 +448,10 @@ __global__ void k_decode(const uint8_t* in, const psb_codec_block* blocks, uint3
     if (bk.is_bitmap) {
         const uint64_t words = (uint64_t(p[0]) | (uint64_t(p[1]) << 8) | (uint64_t(p[2]) << 16) | (uint64_t(p[3] & 0x7F) << 24));
         const uint32_t first = uint32_t(p[4]) | (uint32_t(p[5]) << 8) | (uint32_t(p[6]) << 16) | (uint32_t(p[7]) << 24);
+        if (8 + 8 * words > bk.bytes) {  // a stream shorter than its block table
+            if (threadIdx.x == 0) atomicOr(err, 1ull);
+            return;
+        }
         if (threadIdx.x == 0) put(first);
         for (uint64_t i = threadIdx.x; i < words; i += 32) {
             uint64_t w = 0;
@@ -472,6 +478,82 @@ __global__ void k_decode(const uint8_t* in, const psb_codec_block* blocks, uint3
             cur += x;  // DecodeIndexesAndDiff (StreamVInt.cpp:132-145)
             if (k < count) put(cur);
         }
+    }
+}
+
+// Parallel StreamVInt decode.  A block's tuples form a chain (each
+// descriptor byte gives the tuple's length), so the chain is cut into chunks
+// of kSviChunk tuples whose first byte offsets are found by one walk over
+// the descriptors (on the host when it has the stream, else k_svi_walk);
+// then one thread per chunk sums its deltas (pass 1), an exclusive scan over
+// the chunks gives each chunk's first value, and one thread per chunk
+// decodes again and sets the bits (pass 2).  The values are those of
+// DecodeIndexesAndDiff (StreamVInt.cpp:132-145): a running sum of the
+// deltas, mod 2^32, from 0 at each block.
+constexpr uint32_t kSviChunk = 8;
+struct SviChunk {
+    uint64_t off;     // stream offset of the chunk's first descriptor
+    uint32_t block;   // its block
+    uint32_t tuple0;  // index of its first tuple in the block
+};
+
+__device__ __forceinline__ uint32_t svi_tuple_bytes(uint8_t d) {
+    return 5u + (d & 3u) + ((d >> 2) & 3u) + ((d >> 4) & 3u) + ((d >> 6) & 3u);
+}
+
+// One thread per block: the chunk offsets of the StreamVInt blocks.
+__global__ void k_svi_walk(const uint8_t* in, const psb_codec_block* blocks, uint32_t nb,
+                           const unsigned long long* chunk_first, SviChunk* chunks) {
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const psb_codec_block bk = blocks[b];
+        if (bk.is_bitmap) continue;
+        const uint32_t tuples = (bk.count + 7) / 8 * 2;
+        const uint64_t end = bk.offset + bk.bytes;
+        uint64_t pos = bk.offset + 4, c = chunk_first[b];
+        for (uint32_t t = 0; t < tuples; ++t) {
+            if (t % kSviChunk == 0) chunks[c++] = SviChunk{pos, b, t};
+            if (pos < end) pos += svi_tuple_bytes(in[pos]);  // a short block is caught by k_svi_chunks
+        }
+    }
+}
+
+// Pass 1 (kFinal false): sums[c] = the sum of chunk c's deltas.  Pass 2:
+// sums holds the exclusive scan over all chunks; chunk c's first value is
+// sums[c] - sums[first chunk of its block].
+template <bool kFinal>
+__global__ void k_svi_chunks(const uint8_t* in, const psb_codec_block* blocks, const SviChunk* chunks,
+                             uint64_t n_chunks, const unsigned long long* chunk_first, unsigned long long* sums,
+                             uint64_t* bits, uint64_t n_bits, unsigned long long* err) {
+    for (uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < n_chunks;
+         c += uint64_t(gridDim.x) * blockDim.x) {
+        const SviChunk ck = chunks[c];
+        const psb_codec_block bk = blocks[ck.block];
+        const uint32_t count = bk.count;
+        const uint32_t tuples = (count + 7) / 8 * 2;
+        const uint32_t t_end = ck.tuple0 + kSviChunk < tuples ? ck.tuple0 + kSviChunk : tuples;
+        const uint64_t end = bk.offset + bk.bytes;
+        uint32_t cur = kFinal ? uint32_t(sums[c] - sums[chunk_first[ck.block]]) : 0u;
+        uint64_t pos = ck.off;
+        uint32_t k = 4 * ck.tuple0;
+        for (uint32_t t = ck.tuple0; t < t_end; ++t) {
+            if (pos >= end || pos + svi_tuple_bytes(in[pos]) > end) {  // a stream shorter than its block table
+                atomicOr(err, 1ull);
+                break;
+            }
+            const uint8_t d = in[pos++];
+            for (int q = 0; q < 4; ++q, ++k) {
+                const uint32_t nbytes = 1u + ((d >> (2 * q)) & 3u);
+                uint32_t x = 0;
+                for (uint32_t i = 0; i < nbytes; ++i) x |= uint32_t(in[pos + i]) << (8 * i);
+                pos += nbytes;
+                cur += x;
+                if (kFinal && k < count) {
+                    if (cur >= n_bits) atomicOr(err, 1ull);
+                    else atomicOr(reinterpret_cast<unsigned long long*>(bits) + (cur >> 6), 1ull << (cur & 63));
+                }
+            }
+        }
+        if (!kFinal) sums[c] = cur;
     }
 }
 
@@ -903,10 +985,69 @@ extern "C" int psb_frontier_index(const uint8_t* in, uint64_t in_bytes, psb_code
 }
 
 namespace psb {
-int frontier_decode_async(const uint8_t* d_in, const psb_codec_block* d_blocks, uint32_t n_blocks, uint64_t* d_bits,
-                          uint64_t n_bits, unsigned long long* d_err, cudaStream_t s) {
+
+struct DecodeScratch {
+    SviChunk* chunks = nullptr;
+    unsigned long long *sums = nullptr, *first = nullptr, *gsum = nullptr, *tot = nullptr;
+    size_t cap_chunks = 0, cap_sums = 0, cap_first = 0, cap_gsum = 0, cap_tot = 0;
+    std::vector<SviChunk> h_chunks;
+    std::vector<unsigned long long> h_first;
+    ~DecodeScratch() { cudaFree(chunks); cudaFree(sums); cudaFree(first); cudaFree(gsum); cudaFree(tot); }
+};
+DecodeScratch* decoder_create() { return new (std::nothrow) DecodeScratch(); }
+void decoder_destroy(DecodeScratch* d) { delete d; }
+
+int frontier_decode_async(const uint8_t* d_in, const uint8_t* h_in, const psb_codec_block* h_blocks,
+                          const psb_codec_block* d_blocks, uint32_t n_blocks, uint64_t* d_bits, uint64_t n_bits,
+                          unsigned long long* d_err, DecodeScratch* x, cudaStream_t s) {
     if (n_blocks == 0) return PSB_OK;
-    k_decode<<<n_blocks, 32, 0, s>>>(d_in, d_blocks, n_blocks, d_bits, n_bits, d_err);
+    // Chunks per StreamVInt block, and where each block's chunks start.
+    x->h_first.assign(size_t(n_blocks) + 1, 0);
+    uint64_t n_chunks = 0;
+    bool any_bitmap = false;
+    for (uint32_t b = 0; b < n_blocks; ++b) {
+        x->h_first[b] = n_chunks;
+        if (h_blocks[b].is_bitmap) { any_bitmap = true; continue; }
+        const uint64_t tuples = (uint64_t(h_blocks[b].count) + 7) / 8 * 2;
+        n_chunks += (tuples + kSviChunk - 1) / kSviChunk;
+    }
+    x->h_first[n_blocks] = n_chunks;
+    if (any_bitmap) {
+        k_decode<<<n_blocks, 32, 0, s>>>(d_in, d_blocks, n_blocks, d_bits, n_bits, d_err, 1);
+        CD_CUDA(cudaGetLastError());
+    }
+    if (n_chunks == 0) return PSB_OK;
+    if (int rc = grow(&x->chunks, &x->cap_chunks, n_chunks * sizeof(SviChunk))) return rc;
+    if (int rc = grow(&x->sums, &x->cap_sums, n_chunks * 8)) return rc;
+    if (int rc = grow(&x->first, &x->cap_first, (size_t(n_blocks) + 1) * 8)) return rc;
+    const uint64_t groups = (n_chunks + kT * 16 - 1) / (kT * 16);
+    if (int rc = grow(&x->gsum, &x->cap_gsum, (groups + 1) * 8)) return rc;
+    if (int rc = grow(&x->tot, &x->cap_tot, 8)) return rc;
+    CD_CUDA(cudaMemcpyAsync(x->first, x->h_first.data(), (size_t(n_blocks) + 1) * 8, cudaMemcpyHostToDevice, s));
+    if (h_in) {  // the host walks the descriptors
+        x->h_chunks.resize(n_chunks);
+        for (uint32_t b = 0; b < n_blocks; ++b) {
+            if (h_blocks[b].is_bitmap) continue;
+            const uint32_t tuples = (h_blocks[b].count + 7) / 8 * 2;
+            uint64_t pos = h_blocks[b].offset + 4, c = x->h_first[b];
+            for (uint32_t t = 0; t < tuples; ++t) {
+                if (t % kSviChunk == 0) x->h_chunks[c++] = SviChunk{pos, b, t};
+                const uint8_t d = h_in[pos];
+                pos += 5u + (d & 3u) + ((d >> 2) & 3u) + ((d >> 4) & 3u) + ((d >> 6) & 3u);
+            }
+        }
+        CD_CUDA(cudaMemcpyAsync(x->chunks, x->h_chunks.data(), n_chunks * sizeof(SviChunk), cudaMemcpyHostToDevice, s));
+    } else {
+        k_svi_walk<<<(n_blocks + 127) / 128, 128, 0, s>>>(d_in, d_blocks, n_blocks, x->first, x->chunks);
+    }
+    const unsigned grid = unsigned(std::min<uint64_t>((n_chunks + kT - 1) / kT, 148 * 16));
+    k_svi_chunks<false><<<grid, kT, 0, s>>>(d_in, d_blocks, x->chunks, n_chunks, x->first, x->sums, d_bits, n_bits,
+                                           d_err);
+    k_group_sums<<<unsigned(groups), kT, 0, s>>>(x->sums, n_chunks, x->gsum);
+    k_scan_small<<<1, kScanT, 0, s>>>(x->gsum, groups, x->tot);
+    k_group_scan<<<unsigned(groups), kT, 0, s>>>(x->sums, n_chunks, x->gsum);
+    k_svi_chunks<true><<<grid, kT, 0, s>>>(d_in, d_blocks, x->chunks, n_chunks, x->first, x->sums, d_bits, n_bits,
+                                          d_err);
     CD_CUDA(cudaGetLastError());
     return PSB_OK;
 }
@@ -923,18 +1064,21 @@ extern "C" int psb_frontier_decode(const uint8_t* d_in, const psb_codec_block* b
     CD_CUDA(cudaMalloc(&d_blocks, size_t(n_blocks) * sizeof(psb_codec_block)));
     cudaError_t e = cudaMalloc(&d_err, 8);
     if (e != cudaSuccess) { cudaFree(d_blocks); CD_CUDA(e); }
+    std::unique_ptr<psb::DecodeScratch> x(psb::decoder_create());
     unsigned long long err = 0;
+    int rc = x ? PSB_OK : psb_set_error(PSB_ERR_NOMEM, "decoder scratch");
     e = cudaMemcpyAsync(d_blocks, blocks, size_t(n_blocks) * sizeof(psb_codec_block), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, 8, s);
-    if (e == cudaSuccess) {
-        k_decode<<<n_blocks, 32, 0, s>>>(d_in, d_blocks, n_blocks, d_bits + first_bit / 64, n_bits, d_err);
-        e = cudaGetLastError();
-    }
+    if (e == cudaSuccess && rc == PSB_OK)
+        rc = psb::frontier_decode_async(d_in, nullptr, blocks, d_blocks, n_blocks, d_bits + first_bit / 64, n_bits,
+                                        d_err, x.get(), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&err, d_err, 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    x.reset();
     cudaFree(d_blocks);
     cudaFree(d_err);
     CD_CUDA(e);
+    if (rc) return rc;
     if (err) return psb_set_error(PSB_ERR_ARG, "a decoded offset lies outside the segment");
     return PSB_OK;
 }

@@ -81,11 +81,18 @@ int store_read(StoreImpl& s, int segment, void* buf, uint64_t cap, uint64_t* got
 int store_erase(StoreImpl& s, int segment);
 int store_erase_all(StoreImpl& s);
 
-// Decodes a segment stream (block table `d_blocks` in device memory) into
-// the cleared bitmap d_bits[0, n_bits) on stream s, without allocating or
-// synchronising; an offset outside the segment sets *d_err.
-int frontier_decode_async(const uint8_t* d_in, const psb_codec_block* d_blocks, uint32_t n_blocks, uint64_t* d_bits,
-                          uint64_t n_bits, unsigned long long* d_err, cudaStream_t s);
+// Decodes a segment stream (block table on the host, `h_blocks`, and on the
+// device, `d_blocks`) into the cleared bitmap d_bits[0, n_bits) on stream s,
+// without synchronising; an offset outside the segment sets *d_err.  The
+// StreamVInt blocks are decoded in parallel chunks; `h_in`, the stream in
+// host memory if the caller has it (else NULL), lets the host find the
+// chunks.  The scratch grows on demand and is kept for the next call.
+struct DecodeScratch;
+DecodeScratch* decoder_create();
+void decoder_destroy(DecodeScratch* d);
+int frontier_decode_async(const uint8_t* d_in, const uint8_t* h_in, const psb_codec_block* h_blocks,
+                          const psb_codec_block* d_blocks, uint32_t n_blocks, uint64_t* d_bits, uint64_t n_bits,
+                          unsigned long long* d_err, DecodeScratch* scratch, cudaStream_t s);
 // One-bit frontier bitmaps (ceil(n_states/64) words at out; first_state a
 // multiple of 64) of a two-bit array (states with code `code`) and of a
 // frontier-search array (states with an operator bit set, less `excl`),

@@ -126,6 +126,7 @@ struct Run {
     DevBuf<unsigned int> hist;
     DevBuf<unsigned long long> scalars;  // [0] count, [1] children appended, [2] error flag, [3] decode error
     psb::SegmentEncoder* enc = nullptr;  // device scratch kept from segment to segment
+    psb::DecodeScratch* dec = nullptr;
     std::vector<uint8_t> host_stream;    // one layer between the store and the device
     std::vector<psb_codec_block> blocks;
     std::vector<uint32_t> host_offs;     // cross-segment children between the device and the staging
@@ -136,7 +137,10 @@ struct Run {
     bool files = false;                  // the stores are files (else host memory)
     psb_segmented_stats st{};
 
-    ~Run() { if (enc) psb::encoder_destroy(enc); }
+    ~Run() {
+        if (enc) psb::encoder_destroy(enc);
+        if (dec) psb::decoder_destroy(dec);
+    }
 
     uint64_t states_in(uint64_t g) const { return std::min(seg_states, P->n_states - g * seg_states); }
 
@@ -164,8 +168,8 @@ struct Run {
         SG_CUDA(cudaMemcpyAsync(block_tab[slot].p, blocks.data(), nb * sizeof(psb_codec_block),
                                 cudaMemcpyHostToDevice, s));
         st.h2d_bytes += bytes;
-        return psb::frontier_decode_async(stream_buf[slot].p, block_tab[slot].p, nb, bits, states_in(g),
-                                          scalars.p + 3, s);
+        return psb::frontier_decode_async(stream_buf[slot].p, host_stream.data(), blocks.data(), block_tab[slot].p,
+                                          nb, bits, states_in(g), scalars.p + 3, dec, s);
     }
 
     // Encodes a segment bitmap holding `count` states as segment g's layer in `store`.
@@ -360,6 +364,7 @@ extern "C" int psb_bfs_segmented(const psb_puzzle* p, uint64_t initial, const ps
     if (int rc = R.scalars.grow(4)) return rc;
     if (int rc = R.stream_buf[0].grow(uint64_t(1) << 20)) return rc;
     if (!(R.enc = psb::encoder_create())) return psb_set_error(PSB_ERR_NOMEM, "segmented search: encoder");
+    if (!(R.dec = psb::decoder_create())) return psb_set_error(PSB_ERR_NOMEM, "segmented search: decoder");
     SG_CUDA(cudaMemsetAsync(R.scalars.p, 0, 4 * 8, R.s));
 
     // Depth 0: the initial state is segment g0's layer; its children in the
