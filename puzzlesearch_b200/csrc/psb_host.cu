@@ -783,11 +783,9 @@ int session_pool(int device, cudaMemPool_t* out) {
 // Frontier spill resources: the segment encoder (its device scratch), one
 // segment's extracted bitmap, an arena holding one depth's encoded segments
 // back to back, a copy stream and two pinned host slots.  A depth is encoded
-// into the arena before its level runs; a dense two-bit depth is instead
-// extracted whole into `front` and encoded on the side stream while its
-// level runs.  While the level kernel runs, the calling thread moves the
-// segments through the host slots (copy on the copy stream, then the
-// callback) in order.  They are kept per device between
+// into the arena before its level runs; while the level kernel runs, the
+// calling thread moves the segments through the host slots (copy on the copy
+// stream, then the callback) in order.  They are kept per device between
 // searches (a search allocates them on first use);
 // psb_release_cached_memory frees them.
 struct SpillSeg {
@@ -814,15 +812,6 @@ struct SpillRes {
     SpillSlot slot[2];  // segment i goes through slot i % 2
     cudaStream_t copy = nullptr;
     cudaEvent_t encoded = nullptr;
-    // Dense two-bit depths: the whole frontier extracted into `front` before
-    // the level, then encoded on `side` while the level runs.
-    uint64_t* front = nullptr;
-    uint64_t front_cap = 0;  // bytes
-    unsigned long long* front_sums = nullptr;
-    uint64_t front_sums_cap = 0;  // bytes
-    bool front_failed = false;    // no room for it on this device: encode before the level instead
-    cudaStream_t side = nullptr;
-    cudaEvent_t extracted = nullptr;
 
     ~SpillRes() {
         if (copy) cudaStreamSynchronize(copy);
@@ -831,22 +820,16 @@ struct SpillRes {
             if (sl.start) cudaEventDestroy(sl.start);
             if (sl.done) cudaEventDestroy(sl.done);
         }
-        if (side) cudaStreamSynchronize(side);
         cudaFree(bits);
         cudaFree(arena);
-        cudaFree(front);
-        cudaFree(front_sums);
         if (enc) psb::encoder_destroy(enc);
         if (encoded) cudaEventDestroy(encoded);
-        if (extracted) cudaEventDestroy(extracted);
         if (copy) cudaStreamDestroy(copy);
-        if (side) cudaStreamDestroy(side);
     }
 
     // Waits for copies in flight and drops their segments (a search that
     // failed part-way leaves them behind).
     void reset() {
-        if (side) cudaStreamSynchronize(side);
         if (copy) cudaStreamSynchronize(copy);
         segs.clear();
         issued = delivered = 0;
@@ -869,9 +852,7 @@ int spill_acquire(int device, SpillRes** out) {
     if (!R || !(R->enc = psb::encoder_create())) return fail(PSB_ERR_NOMEM, "spill resources");
     R->device = device;
     PSB_CUDA(cudaStreamCreateWithFlags(&R->copy, cudaStreamNonBlocking));
-    PSB_CUDA(cudaStreamCreateWithFlags(&R->side, cudaStreamNonBlocking));
     PSB_CUDA(cudaEventCreateWithFlags(&R->encoded, cudaEventDisableTiming));
-    PSB_CUDA(cudaEventCreateWithFlags(&R->extracted, cudaEventDisableTiming));
     for (auto& sl : R->slot) {
         PSB_CUDA(cudaEventCreate(&sl.start));
         PSB_CUDA(cudaEventCreate(&sl.done));
@@ -1104,17 +1085,17 @@ int spill_drain(SpillRes* R, const psb_bfs_opts* o, SpillTotals* t) {
     return PSB_OK;
 }
 
-// Encodes the states at `depth` into the arena on stream s, segment by
-// segment (the segment's frontier bitmap is the array itself, a whole-array
-// extraction, or one extracted into the spill scratch), and starts the first
-// copies.  The previous depth must be drained.  This takes SegmentWriter's place (Common/CompressedFrontier.cpp:
+// Encodes the states at `depth` into the arena, segment by segment (the
+// segment's frontier bitmap is the array itself, or one extracted into the
+// spill scratch), and starts the first copies.  The previous depth must be
+// drained.  This takes SegmentWriter's place (Common/CompressedFrontier.cpp:
 // 103-140 writes the same stream per segment).  The arrays may change as
 // soon as this returns: the arena holds everything still to be copied.
-int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const SpillSource& src, SpillTotals* t,
-                cudaStream_t s) {
+int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const SpillSource& src, SpillTotals* t) {
     const auto t0 = std::chrono::steady_clock::now();
     const uint64_t N = S->p.n_states;
     const uint64_t seg = uint64_t(1) << (o->segment_bits ? o->segment_bits : 32);
+    cudaStream_t s = S->stream;
     SpillRes* R = S->spill;
     R->segs.clear();
     R->issued = R->delivered = 0;
@@ -1183,45 +1164,6 @@ int spill_depth(psb_bfs_session* S, const psb_bfs_opts* o, uint32_t depth, const
     if (int rc = spill_issue(R)) return rc;
     t->encode_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return PSB_OK;
-}
-
-// Dense two-bit depths: extracts the whole frontier (the states with code
-// `code`) into R->front on the search stream and records R->extracted, so
-// that the depth can be encoded from R->front on R->side while its level
-// runs and changes the codes.  False (nothing enqueued) when the buffer
-// cannot be had on this device; the depth is then encoded before its level.
-bool spill_front_extract(psb_bfs_session* S, const uint64_t* codes, uint32_t code, cudaStream_t s, int* rc) {
-    SpillRes* R = S->spill;
-    *rc = PSB_OK;
-    if (R->front_failed) return false;
-    const uint64_t N = S->p.n_states;
-    const uint64_t words = words_for(N);
-    const uint64_t bytes = padded(words) * 8, sum_bytes = ((words + 4095) / 4096 + 1) * 8;
-    if (R->front_cap < bytes || R->front_sums_cap < sum_bytes) {
-        cudaFree(R->front);
-        cudaFree(R->front_sums);
-        R->front = nullptr;
-        R->front_sums = nullptr;
-        R->front_cap = R->front_sums_cap = 0;
-        if (cudaMalloc(reinterpret_cast<void**>(&R->front), bytes) != cudaSuccess ||
-            cudaMalloc(reinterpret_cast<void**>(&R->front_sums), sum_bytes) != cudaSuccess) {
-            cudaGetLastError();  // clear the allocation failure
-            cudaFree(R->front);
-            R->front = nullptr;
-            R->front_failed = true;
-            return false;
-        }
-        R->front_cap = bytes;
-        R->front_sums_cap = sum_bytes;
-    }
-    // The previous depth's encode has read the buffer (its copies are drained, too).
-    if (cudaStreamWaitEvent(s, R->encoded, 0) != cudaSuccess ||
-        psb::frontier_bits_two_bit(codes, 0, N, code, R->front, R->front_sums, nullptr, 0, 0, s) != PSB_OK ||
-        cudaEventRecord(R->extracted, s) != cudaSuccess) {
-        *rc = fail(PSB_ERR_CUDA, "frontier extraction: %s", cudaGetErrorString(cudaGetLastError()));
-        return false;
-    }
-    return true;
 }
 
 int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, uint64_t* counts, uint32_t cap,
@@ -1328,15 +1270,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
     uint32_t iteration = 0;
     for (;;) {
         if (max_depth && res.size() >= size_t(max_depth) + 1) break;
-        // A dense two-bit depth is extracted now and encoded on the side
-        // stream once its level is on the GPU; any other depth is encoded here.
-        bool side_spill = false;
-        if (spill && S->algo == PSB_TWO_BIT && flags_valid < 0 && !first) {
-            int rc = PSB_OK;
-            side_spill = spill_front_extract(S, codes, cur_code, s, &rc);
-            if (rc) return rc;
-        }
-        if (spill && !side_spill) {  // the states at depth `iteration`, before its level changes the arrays
+        if (spill) {  // the states at depth `iteration`, before its level changes the arrays
             SpillSource src;
             switch (S->algo) {
             case PSB_THREE_BIT: src.bitmap = cur; break;
@@ -1353,7 +1287,7 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
                 src.window_bits = S->window_bits;
                 src.n_windows = S->n_windows;
             }
-            if (int rc = spill_depth(S, opts, iteration, src, &spilled, s)) return rc;
+            if (int rc = spill_depth(S, opts, iteration, src, &spilled)) return rc;
             spilled_depths = iteration + 1;
         }
         PSB_CUDA(cudaMemsetAsync(S->d_stats, 0, 8 * sizeof(unsigned long long), s));
@@ -1463,13 +1397,6 @@ int session_run(psb_bfs_session* S, uint64_t initial, const psb_bfs_opts* opts, 
             others++;
         }
         PSB_CUDA(cudaEventRecord(S->ev[3], s));
-        if (side_spill) {  // the depth this level expands, from its extracted frontier
-            SpillSource src;
-            src.bitmap = S->spill->front;
-            PSB_CUDA(cudaStreamWaitEvent(S->spill->side, S->spill->extracted, 0));
-            if (int rc = spill_depth(S, opts, iteration, src, &spilled, S->spill->side)) return rc;
-            spilled_depths = iteration + 1;
-        }
         if (spill) if (int rc = spill_drain(S->spill, opts, &spilled)) return rc;  // overlaps this level
         PSB_CUDA(cudaMemcpyAsync(S->h_stats, S->d_stats, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         PSB_CUDA(cudaStreamSynchronize(s));
@@ -1539,7 +1466,7 @@ done:
         // last depth, which no level expanded, in cur / open.
         SpillSource src;
         src.bitmap = S->algo == PSB_THREE_BIT ? cur : open;
-        if (int rc = spill_depth(S, opts, spilled_depths, src, &spilled, s)) return rc;
+        if (int rc = spill_depth(S, opts, spilled_depths, src, &spilled)) return rc;
     }
     if (spill) if (int rc = spill_drain(S->spill, opts, &spilled)) return rc;
     PSB_CUDA(cudaEventRecord(S->ev[3], s));
