@@ -451,7 +451,7 @@ def main():
     ap.add_argument("--no-spill", action="store_true", help="no frontier spill, whatever the workload")
     ap.add_argument("--threads", type=int, default=0, choices=[0, 128, 256, 512],
                     help="threads per block of the top-down two-bit / three-bit level kernels (0 = 128 for two-bit"
-                         " pancake and Hanoi searches of 2^36 states or more, else 256)")
+                         " pancake and Hanoi searches of 2^32 states or more, else 256)")
     ap.add_argument("--far-marks", default="auto", choices=["auto", "none", "near", "all"],
                     help="two-bit long-range marks (PSB_FAR_*); --autotune picks it for two-bit workloads")
     ap.add_argument("--e2e-calls", type=int, default=5,

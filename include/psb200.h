@@ -161,7 +161,7 @@ typedef struct {
                               PuzzleOptions::segmentBits, Common/DiskBasedBFS.h:11) */
     int32_t far_marks;     /* PSB_TWO_BIT top-down levels: where long-range marks go (PSB_FAR_*) */
     int32_t threads;       /* threads per block of the top-down two-bit and three-bit level kernels: 128, 256 or
-                              512 (0 = 128 for two-bit pancake and Hanoi searches of 2^36 states or more, else
+                              512 (0 = 128 for two-bit pancake and Hanoi searches of 2^32 states or more, else
                               256); the other kernels use 256 */
     uint64_t* restored_counts; /* optional, counts_cap entries; 4-peg Hanoi with symmetry and PSB_TWO_BIT only:
                               the counts HanoiSearch reports (HanoiTowers/HanoiSearch.cpp:247-262), i.e. each

@@ -429,7 +429,7 @@ def bfs(puzzle, algo, initial=0, max_depth=0, window_bits=0, final=False, levels
     SPILL_FN is passed through as is (it sees the pinned buffer itself).
     far_marks: two-bit long-range marks, "auto", "none", "near" or "all" (PSB_FAR_*).
     threads: threads per block of the top-down two-bit / three-bit level kernels (128, 256, 512; 0 = 128 for
-        two-bit pancake and Hanoi searches of 2^36 states or more, else 256).
+        two-bit pancake and Hanoi searches of 2^32 states or more, else 256).
     restored: 4-peg Hanoi with symmetry, two-bit: also return "restored", the
     per-depth counts weighted by each canonical state's class size
     (HanoiSearch's result)."""

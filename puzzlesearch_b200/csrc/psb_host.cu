@@ -977,15 +977,14 @@ size_t smem_bytes(int mode, int wb, int threads = 0) {
 }
 
 // Shape variant of the top-down level kernel for psb_bfs_opts.threads.  With
-// threads = 0, two-bit pancake and Hanoi searches of 2^36 states or more take
-// 128-thread blocks with 128 registers a thread (B200 sweeps, whole search:
-// 14-pancake 4.15 s at 128 threads vs 4.40 s at 256, far marks NEAR;
-// 18-disk Hanoi 1.58 vs 1.77 s).  Smaller ones keep 256 (13-pancake two-bit
-// 219 vs 225 ms), as do three-bit (13-pancake 193 vs 195 ms) and the
-// sliding-tile puzzles (3x4 two-bit 40 vs 45 ms).
+// threads = 0, two-bit pancake and Hanoi searches of 2^32 states or more take
+// 128-thread blocks, five per SM (B200 sweeps, whole search, far marks NEAR:
+// 14-pancake 4.06 s at 128 threads vs 4.40 s at 256; 13-pancake 213 vs
+// 219 ms; 18-disk Hanoi 1.58 vs 1.77 s).  Three-bit (13-pancake 195 vs
+// 193 ms) and the sliding-tile puzzles (3x4 two-bit 45 vs 40 ms) keep 256.
 int shape_variant(const psb_puzzle* p, int mode, int threads) {
     if (mode != psb::kTwoBit && mode != psb::kThreeBit) return 0;
-    if (threads == 0 && mode == psb::kTwoBit && p->n_states >= (uint64_t(1) << 36) &&
+    if (threads == 0 && mode == psb::kTwoBit && p->n_states >= (uint64_t(1) << 32) &&
         (p->kind == PSB_PANCAKE || p->kind == PSB_PANCAKE_OPT || p->kind == PSB_HANOI4 || p->kind == PSB_HANOI4_OPT))
         return 2;
     return threads == 512 ? 1 : threads == 128 ? 2 : 0;

@@ -49,14 +49,17 @@ enum Mode : int { kThreeBit = 0, kClassic = 1, kTwoBit = 2, kFrontier = 3 };
 // Variants 1 and 2 of the top-down two-bit and three-bit kernels (the
 // autotuner's threads-per-block dimension, psb_bfs_opts.threads): 512 and
 // 128 threads per block.  For two-bit they also trade resident warps for
-// registers (up to 128 per thread, 512 resident threads per SM): the
-// 13- and 14-pancake kernels issue their far reads early and keep them in
-// flight across the near children, which needs registers rather than warps.
+// registers: 128 per thread at 512 threads (one block per SM), 102 at 128
+// threads (five blocks per SM; B200, whole searches: 13-pancake 213 ms
+// against 226 ms with four blocks of 128 registers, 14-pancake 4.06 s
+// against 4.15 s).  The 13- and 14-pancake kernels issue their far reads
+// early and keep them in flight across the near children, which needs
+// registers rather than warps (at 64 registers they spill).
 template <int MODE, bool BU = false, int V = 0>
 struct Shape {
     static constexpr int threads = V == 1 ? 512 : V == 2 ? 128 : 256;
     static constexpr int min_blocks = BU ? 4
-                                    : MODE == kTwoBit ? (V == 1 ? 1 : 4)
+                                    : MODE == kTwoBit ? (V == 1 ? 1 : V == 2 ? 5 : 4)
                                     : MODE == kFrontier ? 2
                                     : (V == 2 ? 2 : 1);
 };

@@ -33,15 +33,15 @@ def test_pancake13_three_bit():
 
 
 def test_pancake13_two_bit_shapes():
-    """The default two-bit search (far marks NEAR, 256 threads per block at
-    this size), the 128-thread shape with the far bitmap for every long-range
+    """The default two-bit search (far marks NEAR, 128 threads per block at
+    this size), the 256-thread shape with the far bitmap for every long-range
     mark, and read-first far marks."""
     want = fixture("pancake13")
     p = psb.PancakeSimple(13)
     r = psb.bfs(p, "two_bit", 0)
-    assert r["counts"] == want and r["stats"]["threads"] == 256
-    r = psb.bfs(p, "two_bit", 0, threads=128, far_marks="all")
     assert r["counts"] == want and r["stats"]["threads"] == 128
+    r = psb.bfs(p, "two_bit", 0, threads=256, far_marks="all")
+    assert r["counts"] == want and r["stats"]["threads"] == 256
     r = psb.bfs(p, "two_bit", 0, far_marks="none")
     assert r["counts"] == want
     psb.lib().psb_release_cached_memory(0)
