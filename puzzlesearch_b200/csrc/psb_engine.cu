@@ -449,7 +449,6 @@ int psb_engine_create(const psb_engine_opts* opts, psb_engine** out) {
         return psb_set_error(PSB_ERR_ARG, "window_bits_offset outside -6..6");
     e->wb_offset = opts->window_bits_offset;
     EN_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
-    EN_CUDA(psb::ensure_flip_deltas());  // this module's pancake table, before any graph capture
     EN_CUDA(cudaMalloc(&e->pool, e->pool_words * 8));
     e->free_space[0] = e->pool_words;
     EN_CUDA(cudaMalloc(&e->d.slots, sizeof(psb::EngineSlot) * e->n_slots));

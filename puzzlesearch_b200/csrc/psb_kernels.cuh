@@ -1233,9 +1233,6 @@ cudaError_t launch_segment_expand(const SegExpandArgs& a, unsigned grid, cudaStr
 
 template <class PZ, int MODE, bool BU = false, int V = 0>
 cudaError_t launch_level(const LevelArgs& a, unsigned grid, size_t smem, cudaStream_t s) {
-    if constexpr (PZ::kChunkPrefix) {  // the chunk-prefixed pancake path reads the flip-delta table
-        if (cudaError_t e = ensure_flip_deltas()) return e;
-    }
     cudaError_t e = cudaFuncSetAttribute(level_kernel<PZ, MODE, BU, V>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;

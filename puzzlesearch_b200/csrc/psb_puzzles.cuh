@@ -15,7 +15,6 @@
 // stay in registers.
 #pragma once
 
-#include <atomic>
 #include <cstdint>
 #include <type_traits>
 
@@ -118,77 +117,6 @@ __device__ __forceinline__ uint64_t perm_rank_packed(uint64_t p) {
 #pragma unroll
     for (int i = 0; i < N; ++i) v[i] = uint32_t(p >> (4 * i)) & 15u;
     return perm_rank<N>(v);
-}
-
-// Flips of the last m <= 7 values change only the last m Lehmer digits, which
-// encode the relative order of the last m values; so with r = index mod 7!
-// (the relative order of the last 7 values), flip m maps index to
-// index + delta_m(r).  One entry per r holds delta_4 .. delta_7 as signed
-// 16-bit fields (|delta| < 7!), computed at compile time by ranking the
-// reversed arrangement (PermutationMap.cpp:39-58 on 7 values).
-struct FlipDeltas {
-    uint64_t v[5040];
-};
-constexpr int flip7_rank(const int (&w)[7]) {
-    int x = 0;
-    for (int i = 0; i < 7; ++i) {
-        int c = 0;  // values to the right that are smaller
-        for (int j = i + 1; j < 7; ++j) c += w[j] < w[i];
-        x = x * (7 - i) + c;
-    }
-    return x;
-}
-constexpr FlipDeltas make_flip_deltas() {
-    FlipDeltas t{};
-    for (int r = 0; r < 5040; ++r) {
-        int d[7] = {}, v[7] = {};
-        int x = r;
-        for (int i = 6; i >= 0; --i) {
-            d[i] = x % (7 - i);
-            x /= 7 - i;
-        }
-        bool used[7] = {};
-        for (int i = 0; i < 7; ++i) {  // digit d picks the d-th unused value
-            int k = d[i], val = 0;
-            for (;; ++val) {
-                if (used[val]) continue;
-                if (k-- == 0) break;
-            }
-            v[i] = val;
-            used[val] = true;
-        }
-        uint64_t packed = 0;
-        for (int m = 4; m <= 7; ++m) {
-            int w[7] = {};
-            for (int i = 0; i < 7; ++i) w[i] = v[i];
-            for (int a = 7 - m, b = 6; a < b; ++a, --b) {
-                const int t2 = w[a];
-                w[a] = w[b];
-                w[b] = t2;
-            }
-            const int delta = flip7_rank(w) - r;
-            packed |= uint64_t(uint16_t(int16_t(delta))) << (16 * (m - 4));
-        }
-        t.v[r] = packed;
-    }
-    return t;
-}
-// The table in device memory, one copy per translation unit that launches
-// pancake level kernels (internal linkage), filled from the host by
-// ensure_flip_deltas before the first launch on each device.
-static __device__ uint64_t g_flip_deltas[5040];
-
-static inline cudaError_t ensure_flip_deltas() {
-    static std::atomic<uint64_t> ready{0};  // one bit per device
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    const uint64_t bit = dev < 64 ? uint64_t(1) << dev : 0;
-    if (bit && (ready.load() & bit)) return cudaSuccess;
-    static const FlipDeltas host = make_flip_deltas();
-    e = cudaMemcpyToSymbol(g_flip_deltas, host.v, sizeof(host.v));
-    if (e == cudaSuccess) ready.fetch_or(bit);
-    return e;
 }
 
 // --------------------------------------------------------------------------
@@ -307,7 +235,7 @@ struct Pancake {
                                                            uint32_t opbits, int first, int last, Emit& emit) {
         uint32_t d[N], pre[N], pb[N];
         unrank_suffix(P, r, d, pre, pb);
-        children<kOpBits, (N >= 8)>(index, d, pre, pb, opbits, first, last, emit, r);
+        children<kOpBits>(index, d, pre, pb, opbits, first, last, emit);
     }
 
     // Rank of the child of flip m: with pre = the values left of the suffix
@@ -315,11 +243,10 @@ struct Pancake {
     // smaller than v[j], the count above is popc(pb[j] & ~pre).  For m <= 12
     // every quantity is below 12! < 2^31, so the child is passed to emitters
     // that take it (EmitRel) as the parent plus a 32-bit signed delta.
-    // kR7: r7 = index mod 7!, and the flips of 4..7 values come from kFlipDeltas.
-    template <bool kOpBits, bool kR7 = false, class Emit>
+    template <bool kOpBits, class Emit>
     __device__ __forceinline__ static void children(uint64_t index, const uint32_t (&d)[N], const uint32_t (&pre)[N],
                                                     const uint32_t (&pb)[N], uint32_t opbits, int first, int last,
-                                                    Emit& emit, uint32_t r7 = 0) {
+                                                    Emit& emit) {
         // Far children first, for emitters that take them in two steps.
         constexpr bool kSplit = EmitSplitFar<Emit>::value && (N > 12);
         constexpr int kFarN = N > 12 ? N - 12 : 1;
@@ -351,10 +278,6 @@ struct Pancake {
         }
         uint32_t low32 = 0;  // low_m for m <= 12 (d[n-1] is always 0)
         uint64_t low64 = 0;  // low_m for m > 12
-        uint64_t flip_deltas = 0;
-        if constexpr (kR7) {
-            if (first < 6 && last > 2) flip_deltas = __ldg(&g_flip_deltas[r7]);
-        }
 #pragma unroll
         for (int m = 2; m <= N; ++m) {
             if (kSplit && m > 12) break;
@@ -363,12 +286,6 @@ struct Pancake {
             const int op = m - 2;
             if (op >= last) break;
             if (op < first || (kOpBits && (opbits >> op) & 1u)) continue;
-            if (kR7 && m >= 4 && m <= 7) {  // from the table
-                const int32_t delta = int32_t(int16_t(uint16_t(flip_deltas >> (16 * (m - 4)))));
-                if constexpr (EmitRel<Emit>::value) emit.rel(index, delta, uint32_t(op));
-                else emit(index + int64_t(delta), uint32_t(op));
-                continue;
-            }
             const uint32_t excl = pre[N - m];
             if (m <= 12) {  // m is a compile-time constant after unrolling
                 uint32_t s32 = 0;
