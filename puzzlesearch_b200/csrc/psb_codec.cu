@@ -196,8 +196,12 @@ struct SviRef {
 // Writes the ascending offsets of the set bits that fall in StreamVInt
 // blocks, at their rank (offset list position = rank; bitmap blocks need no
 // list: their words are copied from the bitmap).  One CTA per chunk of
-// kT * 16 words; thread t takes the chunk's words 16 t .. 16 t + 15, so one
-// block scan of the per-thread counts ranks them all.
+// kT * 16 words; warp w takes the chunk's words 512 w .. 512 w + 511, 32 at a
+// time, lane l word 32 i + l, so every load is coalesced.  A first pass
+// counts each warp's offsets (one CTA scan of the 8 warp totals gives the
+// warps' first ranks); the second pass reloads the words (from L1) and ranks
+// each lane's offsets by a warp scan, so neighbouring lanes store
+// neighbouring ranks.
 __global__ void __launch_bounds__(kT) k_compact(const uint64_t* bits, uint64_t n_words, uint64_t n_bits,
                                                 const unsigned long long* bsum, uint64_t nbs, uint64_t count,
                                                 const BlockInfo* blocks, uint32_t* idx) {
@@ -210,27 +214,40 @@ __global__ void __launch_bounds__(kT) k_compact(const uint64_t* bits, uint64_t n
     bool all_bitmap = true;
     for (uint64_t b = r_lo / kBlock; b <= (r_hi - 1) / kBlock; ++b) all_bitmap = all_bitmap && blocks[b].is_bitmap;
     if (all_bitmap) return;
-    const uint64_t w0 = uint64_t(blockIdx.x) * kT * 16 + uint64_t(threadIdx.x) * 16;
-    uint64_t v[16];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint64_t w0 = uint64_t(blockIdx.x) * kT * 16 + uint64_t(warp) * 512 + lane;
     uint32_t c = 0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        v[k] = w0 + k < n_words ? masked_word(bits, w0 + k, n_words, n_bits) : 0;
-        c += __popcll(v[k]);
+#pragma unroll 4
+    for (int i = 0; i < 16; ++i) {
+        const uint64_t w = w0 + 32u * i;
+        if (w < n_words) c += __popcll(masked_word(bits, w, n_words, n_bits));
     }
-    const uint32_t inc = block_inclusive_scan(c, warp_tot);
-    if (c == 0) return;
-    unsigned long long r = bsum[blockIdx.x] + inc - c;
-    // c <= 1024 < kBlock: the thread's offsets lie in at most two blocks
-    if (blocks[r / kBlock].is_bitmap && blocks[(r + c - 1) / kBlock].is_bitmap) return;
-    for (int k = 0; k < 16; ++k) {
-        uint64_t m = v[k];
+    // The CTA's ranks, warp by warp (warp order is word order).
+    const uint32_t wsum = __reduce_add_sync(0xFFFFFFFFu, c);
+    if (lane == 0) warp_tot[warp] = wsum;
+    __syncthreads();
+    unsigned long long r = r_lo;
+    for (uint32_t k = 0; k < warp; ++k) r += warp_tot[k];
+    if (wsum == 0) return;
+    for (int i = 0; i < 16; ++i) {
+        const uint64_t w = w0 + 32u * i;
+        uint64_t m = w < n_words ? masked_word(bits, w, n_words, n_bits) : 0;
+        const uint32_t cnt = __popcll(m);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= uint32_t(o)) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        unsigned long long rr = r + incl - cnt;
         while (m) {
             const uint32_t j = __ffsll((long long)m) - 1;
             m &= m - 1;
-            if (!blocks[r / kBlock].is_bitmap) idx[r] = uint32_t((w0 + k) * 64 + j);
-            r++;
+            if (!blocks[rr / kBlock].is_bitmap) idx[rr] = uint32_t(w * 64 + j);
+            rr++;
         }
+        r += total;
     }
 }
 
