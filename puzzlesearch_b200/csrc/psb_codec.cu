@@ -240,12 +240,24 @@ __global__ void __launch_bounds__(kT) k_compact(const uint64_t* bits, uint64_t n
             if (lane >= uint32_t(o)) incl += y;
         }
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        unsigned long long rr = r + incl - cnt;
-        while (m) {
-            const uint32_t j = __ffsll((long long)m) - 1;
-            m &= m - 1;
-            if (!blocks[rr / kBlock].is_bitmap) idx[rr] = uint32_t(w * 64 + j);
-            rr++;
+        // The 32 words' offsets in rank order, 32 at a time: lane l stores
+        // rank r + k, k = base + l, so a warp's stores are contiguous.
+        for (uint32_t base = 0; base < total; base += 32) {
+            const uint32_t k = base + lane;
+            uint32_t lo = 0, hi = 31;  // source lane: the first whose inclusive count exceeds k
+#pragma unroll
+            for (int step = 0; step < 5; ++step) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__shfl_sync(0xFFFFFFFFu, incl, int(mid)) > k) hi = mid;
+                else lo = mid + 1;
+            }
+            const uint32_t before = __shfl_sync(0xFFFFFFFFu, incl - cnt, int(lo));
+            const uint64_t word = __shfl_sync(0xFFFFFFFFu, m, int(lo));
+            if (k < total) {
+                const unsigned long long rank = r + k;
+                if (!blocks[rank / kBlock].is_bitmap)
+                    idx[rank] = uint32_t((w0 + 32u * i - lane + lo) * 64 + psb::select_bit(word, k - before));
+            }
         }
         r += total;
     }
