@@ -55,6 +55,15 @@ WORKLOADS = {
     "sliding4x3-frontier": ("sliding", 4, 3, "frontier", "4x3 sliding-tile in-memory frontier search, full solve"),
 }
 SPILL_BY_DEFAULT = {"pancake14-2bit", "hanoi18-2bit"}
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the level
+# kernels over one full search, from a one-pass ncu capture of the same search
+# without spill (the level launches are the same with it); ncu cannot run
+# inside the bench.  Used for roofline.traffic when the run has the same
+# launches (same level count, window and shape defaults).
+LEVEL_TRAFFIC = {
+    "pancake14-2bit": {"bytes": 11978881712384, "launches": 17, "window_bits": 16, "threads": 128,
+                       "profile": "profiles/level_kernel_pancake14_2bit_traffic.md"},
+}
 REF_SAMPLE = ("pancake", 11, 0, "two_bit")      # cpu_baseline: one reference InMemoryTwoBitBFS, one core
 REF_ARM_SAMPLE = ("pancake", 10, 0, "two_bit")  # --impl reference: one search per host core per step
 
@@ -606,6 +615,16 @@ def main():
     expand_ms = sum(s.expand_ms for s in stats) / len(stats)
     achieved = alg_bytes / (expand_ms / 1000.0) / 1e9
     peak, peak_kind = load_peaks()
+    traffic = None
+    tr = LEVEL_TRAFFIC.get(args.workload)
+    if tr and st.levels == tr["launches"] and st.window_bits == tr["window_bits"] and st.threads == tr["threads"]:
+        traffic = {"per_launch": tr["bytes"] / tr["launches"], "per_search": tr["bytes"],
+                   "vs_algorithmic": tr["bytes"] / alg_bytes,
+                   # the captured bytes over this run's level time: the DRAM throughput the kernels sustain
+                   "dram_gbs": tr["bytes"] / (expand_ms / 1000.0) / 1e9,
+                   "dram_frac": tr["bytes"] / (expand_ms / 1000.0) / 1e9 / peak,
+                   "source": "ncu one-pass capture, dram__bytes_read.sum + dram__bytes_write.sum over the search's"
+                             " level launches (" + tr["profile"] + ")"}
     # level kernels + one finalize per level (three-bit, classic) or one
     # CUR -> OLD pass per bottom-up level (two-bit)
     launches_per_step = st.levels + st.other_launches + st.spill_launches
@@ -626,11 +645,12 @@ def main():
                 "call_s": [round(c, 4) for c in calls]},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": traffic["per_launch"] if traffic else None,
                      "note": f"level kernel (top-down and bottom-up launches), {peak_kind} peak; algorithmic bytes"
                              f" per level = {'N/8' if algo != 'two_bit' else '2 x 2N/8'} sweep + 8 B per child"
-                             " generated or probe issued; traffic is not measured in this run (ncu is not run"
-                             " inside the bench)"},
+                             " generated or probe issued; traffic (bytes per launch) from the capture named in"
+                             " traffic_detail, null where no capture covers this workload",
+                     "traffic_detail": traffic},
         "kernel_ms_per_step": {"level": expand_ms, "finalize": sum(s.finalize_ms for s in stats) / len(stats)},
         "children_per_step": st.children, "local_child_fraction": st.local_children / max(st.children, 1),
         "direction": {"mode": args.direction, "bottom_up_levels": st.bottom_up_levels, "levels": st.levels},
