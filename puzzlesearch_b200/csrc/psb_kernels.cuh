@@ -269,6 +269,8 @@ struct LevelArgs {
     uint32_t* far;              // two-bit top-down, optional: 1 bit per state for long-range marks (see Emitter)
     int far_all;                // far != NULL: the far-reaching marks (Emitter::far) use it too
     int sym_mult;               // Hanoi with symmetry: add each frontier state's class size to stats[7]
+    int flag_bits;              // non-zero: wflag_next has one byte per 2^flag_bits states (a bottom-up level's
+                                // windows are larger than the top-down windows its flags serve); 0: window_bits
 };
 
 constexpr uint64_t kEven = 0x5555555555555555ull;
@@ -976,7 +978,13 @@ __device__ __forceinline__ void level_window(const LevelArgs& a, uint64_t window
     // Flush the window's shared-memory marks (only if it had frontier states).
     uint32_t fresh = 0;  // two-bit: states this flush moves from UNVISITED to NEXT
     if (sh.any) {
-        if (a.wflag_next && tid == 0) a.wflag_next[window] = 1;
+        if (a.wflag_next && tid == 0) {
+            if (a.flag_bits) {  // every flag window this window overlaps (base + span <= n_states)
+                for (uint64_t f = base >> a.flag_bits; f <= (base + span - 1) >> a.flag_bits; ++f) a.wflag_next[f] = 1;
+            } else {
+                a.wflag_next[window] = 1;
+            }
+        }
         if constexpr (MODE == kTwoBit) {
             const uint32_t next_pat = em.next_pat;
             unsigned long long* codes = reinterpret_cast<unsigned long long*>(a.marks) + (base >> 5);
