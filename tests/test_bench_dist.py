@@ -53,3 +53,14 @@ def test_single_process_needs_no_group(monkeypatch):
     assert bench.max_over_ranks(3.5, None) == 3.5
     with pytest.raises(SystemExit):
         bench.dist_setup(2)
+
+
+def test_level_traffic_matches_its_profile():
+    """The DRAM bytes bench.py reports as roofline.traffic come from a
+    committed ncu summary; the constant and the summary agree."""
+    for workload, tr in bench.LEVEL_TRAFFIC.items():
+        assert workload in bench.WORKLOADS
+        path = os.path.join(bench.REPO, tr["profile"])
+        text = open(path).read()
+        assert f"{tr['bytes']:,} bytes" in text, (workload, path)
+        assert tr["launches"] > 0 and tr["window_bits"] >= 10 and tr["threads"] in (128, 256, 512)
