@@ -74,6 +74,7 @@ enum {
 
 typedef struct psb_puzzle psb_puzzle;
 
+/* Library version string (static storage, never NULL). */
 const char* psb_version(void);
 /* Copies the calling thread's last error message (NUL-terminated). */
 int psb_last_error(char* buf, int cap);
